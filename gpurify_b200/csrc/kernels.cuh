@@ -1,0 +1,58 @@
+// Device-side view of a plan and the launch wrappers of the FP64 kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gpx_common.h"
+
+namespace gpx {
+
+// Device pointers of one uploaded plan (all arrays in leaf-sorted order).
+struct DevPlan {
+    int n, n3, L;
+    int64_t N;
+    int32_t nleaf, nbox, leaf_box0;
+    const double* verts;      // 12 per panel
+    const double* cent;       // 3 per panel
+    const double* area;
+    const int32_t* cond;
+    const double* w1d;        // 3*n per panel
+    const int64_t* leaf_begin;
+    const int32_t* near_off;
+    const int32_t* near_src;
+    const int32_t* near_S;
+    const int64_t* nval_off;
+    const int32_t* box_parent;
+    const int32_t* box_octant;
+    const int64_t* m2l_off;
+    const int32_t* m2l_src;
+    const int32_t* m2l_slot;
+    const double* m2m1d;      // 24 n x n
+    const double* m2l_K;      // 343 n3 x n3 (FP64 table)
+};
+
+// Wilton near-field block assembly: P (nnz doubles), one CTA per target leaf.
+void launch_near_assemble(Ctx& c, const DevPlan& p, int64_t nnz, double* P, double coef);
+// inv_diag[i] = 1 / P_ii (|P_ii| > 1e-30 else 1), the reference's DiagJacobi.
+void launch_diag_inv(Ctx& c, const DevPlan& p, const double* P, double* inv_diag);
+// Y = P_near X (overwrite), X/Y are N x R row-major.
+void launch_near_apply(Ctx& c, const DevPlan& p, int64_t nnz, const double* P, const double* X, double* Y, int R);
+// Host-side level table plus device child ranges used to sequence the far field.
+struct FarLaunch {
+    const int32_t* lvl_off;      // host, L+2 entries
+    const double* lvl_half;      // host, L+1 entries
+    const int32_t* child_first;  // device, per box
+    const int32_t* child_count;  // device, per box
+    const int32_t* leaf_of;      // device, per sorted panel
+    const int64_t* m2l_off;      // host, per box (pair counts per level)
+};
+// Far field, added to Y: P2M, M2M, M2L, L2L, L2P (bbfmm.rs:209-448), scaled by
+// coef; M and Lc are nbox x n3 x R scratch.
+void launch_far_apply(Ctx& c, const DevPlan& p, const FarLaunch& f, const double* X, double* Y, int R, double* M,
+                      double* Lc, double coef);
+// Dense all-pairs block for arbitrary target points.
+void launch_potential_matrix(Ctx& c, const double* src_verts, int64_t ns, const double* pts, int64_t nt, double* out,
+                             double coef);
+
+}  // namespace gpx

@@ -1,0 +1,306 @@
+// Multi-RHS restarted GMRES building blocks (FP64).  Vectors are N x R
+// row-major (panel-major, one column per right-hand side) so a row of R values
+// is one coalesced load.  All reductions are two-stage with a fixed block
+// partition and a fixed summation order, so results are bit-reproducible.
+#include <algorithm>
+
+#include "gpx_common.h"
+#include "krylov.cuh"
+
+namespace gpx {
+
+namespace {
+
+constexpr int kRedThreads = 256;
+
+// partial[b][i][r] = sum over rows of block b of A_i[n][r] * B[n][r].
+__global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restrict__ A, int64_t strideA, int ni,
+                                                          const double* __restrict__ B, int64_t N, int R,
+                                                          double* __restrict__ partial) {
+    const int nsub = kRedThreads / R;
+    const int r = threadIdx.x % R, sub = threadIdx.x / R;
+    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
+    const int64_t n0 = (int64_t)blockIdx.x * per, n1 = min(N, n0 + per);
+    __shared__ double red[kRedThreads];
+    for (int i = 0; i < ni; ++i) {
+        const double* Ai = A + i * strideA;
+        double acc = 0.0;
+        if (sub < nsub)
+            for (int64_t n = n0 + sub; n < n1; n += nsub) acc += Ai[n * R + r] * B[n * R + r];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        if (sub == 0) {
+            double s = red[r];
+            for (int k = 1; k < nsub; ++k) s += red[k * R + r];
+            partial[((int64_t)blockIdx.x * ni + i) * R + r] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// out[i][r] (+)= sum_b partial[b][i][r]; one thread per (i, r).
+__global__ void k_reduce_blocks(const double* __restrict__ partial, int nblk, int ni, int R, double* __restrict__ out,
+                                int accumulate) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= ni * R) return;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += partial[(int64_t)b * ni * R + o];
+    out[o] = accumulate ? out[o] + s : s;
+}
+
+// W[n][r] -= sum_{i<ni} h[i][r] * V_i[n][r]
+__global__ void k_multi_axpy(const double* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ h,
+                             double* __restrict__ W, int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= N * R) return;
+    const int r = (int)(o % R);
+    double w = W[o];
+    for (int i = 0; i < ni; ++i) w -= h[i * R + r] * V[i * strideV + o];
+    W[o] = w;
+}
+
+// dst[n][r] = src[n][r] / s[r] when s[r] > thresh, else src (Arnoldi
+// normalisation with the reference's happy-breakdown rule, krylov.rs:111-115).
+__global__ void k_scale_cols(const double* __restrict__ src, const double* __restrict__ s, double thresh,
+                             double* __restrict__ dst, int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= N * R) return;
+    const double d = s[o % R];
+    dst[o] = d > thresh ? src[o] / d : src[o];
+}
+
+__global__ void k_sqrt(double* v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = sqrt(v[i]);
+}
+
+// Z[n][r] = inv_diag[n] * V[n][r]
+__global__ void k_diag_scale(const double* __restrict__ V, const double* __restrict__ d, double* __restrict__ Z,
+                             int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= N * R) return;
+    Z[o] = V[o] * d[o / R];
+}
+
+// Res[n][r] = b[n][r] - AX[n][r], b the unit-conductor right-hand side
+// (cap/solver.rs:55-63): 1 on the panels of conductor rhs_cond[r].
+__global__ void k_residual(const int32_t* __restrict__ cond, const int32_t* __restrict__ rhs_cond,
+                           const double* __restrict__ AX, double* __restrict__ Res, int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= N * R) return;
+    const double b = cond[o / R] == rhs_cond[o % R] ? 1.0 : 0.0;
+    Res[o] = AX ? b - AX[o] : b;
+}
+
+// Per-column Hessenberg column k update, Givens rotation (krylov.rs:118-142,
+// :195-207), residual estimate and freeze of converged columns.
+__global__ void k_givens(GmresDev g, int k) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.R) return;
+    const int m = g.m, R = g.R;
+    if (!g.act[r]) return;
+    double* H = g.H;  // H[(i*m + k)*R + r]
+    auto h = [&](int i) -> double& { return H[((int64_t)i * m + k) * R + r]; };
+    for (int i = 0; i <= k; ++i) h(i) = g.h1[i * R + r] + g.h2[i * R + r];
+    h(k + 1) = g.hnorm[r];
+    for (int i = 0; i < k; ++i) {
+        const double cs = g.cs[i * R + r], sn = g.sn[i * R + r];
+        const double t = cs * h(i) + sn * h(i + 1);
+        h(i + 1) = -sn * h(i) + cs * h(i + 1);
+        h(i) = t;
+    }
+    const double a = h(k), b = h(k + 1);
+    double c, s;
+    if (b == 0.0) {
+        c = 1.0;
+        s = 0.0;
+    } else if (fabs(b) > fabs(a)) {
+        const double t = a / b;
+        s = 1.0 / sqrt(1.0 + t * t);
+        c = t * s;
+    } else {
+        const double t = b / a;
+        c = 1.0 / sqrt(1.0 + t * t);
+        s = t * c;
+    }
+    g.cs[k * R + r] = c;
+    g.sn[k * R + r] = s;
+    h(k) = c * a + s * b;
+    h(k + 1) = 0.0;
+    const double gk = g.g[k * R + r], gk1 = g.g[(k + 1) * R + r];
+    g.g[k * R + r] = c * gk + s * gk1;
+    g.g[(k + 1) * R + r] = -s * gk + c * gk1;
+    g.kused[r] = k + 1;
+    const double est = fabs(g.g[(k + 1) * R + r]) / g.bnorm[r];
+    g.est[r] = est;
+    if (est <= g.tol) g.act[r] = 0;
+}
+
+// Back substitution H y = g per column (krylov.rs:144-152); y[i][r].
+__global__ void k_trisolve(GmresDev g) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.R) return;
+    const int m = g.m, R = g.R, ku = g.done[r] ? 0 : g.kused[r];
+    for (int i = 0; i < m; ++i) g.y[i * R + r] = 0.0;
+    for (int i = ku - 1; i >= 0; --i) {
+        double sum = g.g[i * R + r];
+        for (int j = i + 1; j < ku; ++j) sum -= g.H[((int64_t)i * m + j) * R + r] * g.y[j * R + r];
+        g.y[i * R + r] = sum / g.H[((int64_t)i * m + i) * R + r];
+    }
+}
+
+// X[n][r] += inv_diag[n] * sum_i y[i][r] V_i[n][r]  (krylov.rs:154-168)
+__global__ void k_combine(const double* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ y,
+                          const double* __restrict__ d, double* __restrict__ X, int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= N * R) return;
+    const int r = (int)(o % R);
+    double s = 0.0;
+    for (int i = 0; i < ni; ++i) s += y[i * R + r] * V[i * strideV + o];
+    X[o] += d[o / R] * s;
+}
+
+// Start of a cycle: beta = ||res||, converged-at-start test, V_0 = res/beta,
+// g = (beta, 0, ...), activity flags.
+__global__ void k_cycle_start(GmresDev g, const double* __restrict__ beta) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.R) return;
+    const double b = beta[r];
+    const double rel = b / g.bnorm[r];
+    g.resid[r] = rel;
+    if (rel <= g.tol) g.done[r] = 1;
+    g.act[r] = g.done[r] ? 0 : 1;
+    g.kused[r] = 0;
+    for (int i = 0; i <= g.m; ++i) g.g[i * g.R + r] = 0.0;
+    g.g[r] = b;
+    g.bcur[r] = g.done[r] ? 0.0 : b;
+}
+
+// End of a cycle: true residual check of columns whose estimate is within
+// 10x of the tolerance (krylov.rs:170-181).
+__global__ void k_cycle_end(GmresDev g, const double* __restrict__ rnorm) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.R) return;
+    if (g.done[r]) return;
+    const double rel = rnorm[r] / g.bnorm[r];
+    g.resid[r] = rel;
+    const int ku = g.kused[r];
+    const double est = ku > 0 ? fabs(g.g[ku * g.R + r]) / g.bnorm[r] : rel;
+    if (est <= g.tol * 10.0 && rel <= g.tol) g.done[r] = 1;
+}
+
+__global__ void k_count_active(const int32_t* act, int R, int32_t* out) {
+    int c = 0;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) c += act[r] != 0;
+    __shared__ int red[256];
+    red[threadIdx.x] = c;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+int reduce_blocks_for(int64_t N) { return (int)std::min<int64_t>(296, std::max<int64_t>(1, N / 64)); }
+
+void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
+                     double* partial, int nblk, double* out, int accumulate, int tag) {
+    {
+        KTimer t(c, tag, 8.0 * (ni + 1) * (double)N * R, 2.0 * ni * (double)N * R);
+        k_multidot<<<nblk, kRedThreads, 0, c.stream>>>(A, strideA, ni, B, N, R, partial);
+        GPX_LAUNCH_CHECK();
+    }
+    {
+        KTimer t(c, K_SMALL);
+        k_reduce_blocks<<<blocks_for((int64_t)ni * R, 128), 128, 0, c.stream>>>(partial, nblk, ni, R, out, accumulate);
+        GPX_LAUNCH_CHECK();
+    }
+    c.launches += 2;
+}
+
+void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, int nblk, double* out) {
+    launch_multidot(c, A, 0, 1, A, N, R, partial, nblk, out, 0, K_VEC);
+    KTimer t(c, K_SMALL);
+    k_sqrt<<<blocks_for(R, 128), 128, 0, c.stream>>>(out, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R) {
+    KTimer t(c, K_GS_AXPY, 8.0 * (ni + 2) * (double)N * R, 2.0 * ni * (double)N * R);
+    k_multi_axpy<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, h, W, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R) {
+    KTimer t(c, K_VEC, 16.0 * (double)N * R, (double)N * R);
+    k_scale_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(src, sc, thresh, dst, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R) {
+    KTimer t(c, K_VEC, 16.0 * (double)N * R + 8.0 * N, (double)N * R);
+    k_diag_scale<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, d, Z, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_residual(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const double* AX, double* Res, int64_t N,
+                     int R) {
+    KTimer t(c, K_VEC, (AX ? 16.0 : 8.0) * (double)N * R + 4.0 * N, (double)N * R);
+    k_residual<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(cond, rhs_cond, AX, Res, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_givens(Ctx& c, const GmresDev& g, int k) {
+    KTimer t(c, K_SMALL);
+    k_givens<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g, k);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_trisolve(Ctx& c, const GmresDev& g) {
+    KTimer t(c, K_SMALL);
+    k_trisolve<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_combine(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, const double* d, double* X,
+                    int64_t N, int R) {
+    KTimer t(c, K_VEC, 8.0 * (ni + 2) * (double)N * R, 2.0 * ni * (double)N * R);
+    k_combine<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, y, d, X, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_cycle_start(Ctx& c, const GmresDev& g, const double* beta) {
+    KTimer t(c, K_SMALL);
+    k_cycle_start<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g, beta);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_cycle_end(Ctx& c, const GmresDev& g, const double* rnorm) {
+    KTimer t(c, K_SMALL);
+    k_cycle_end<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g, rnorm);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_count_active(Ctx& c, const int32_t* act, int R, int32_t* out) {
+    KTimer t(c, K_SMALL);
+    k_count_active<<<1, 256, 0, c.stream>>>(act, R, out);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+}  // namespace gpx

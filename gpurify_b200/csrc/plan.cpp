@@ -1,0 +1,409 @@
+// Host plan builder: bit-exact panel centroids/areas, the uniform octree of
+// the reference (fmm/tree.rs:41-210), near-field blocks (bbfmm.rs:192-206),
+// interaction lists and the M2L operator table (bbfmm.rs:132-174).
+// Compiled with -ffp-contract=off: centroids, leaf cells and Chebyshev
+// weights use the reference's operation order.
+#include "plan.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <numeric>
+#include <thread>
+#include <unordered_map>
+
+namespace gpx {
+
+namespace {
+
+struct P3 {
+    double x, y, z;
+};
+inline P3 sub(P3 a, P3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline P3 add(P3 a, P3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline P3 scl(P3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline P3 crs(P3 a, P3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double len(P3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+// Area-weighted fan centroid and area of a quad whose 4th vertex may repeat
+// the 3rd (integrals/panel.rs:29-67).
+void panel_centroid_area(const double* v, double* c, double* a) {
+    P3 q[4];
+    for (int i = 0; i < 4; ++i) q[i] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    int nv = (q[3].x == q[2].x && q[3].y == q[2].y && q[3].z == q[2].z) ? 3 : 4;
+    double asum = 0.0;
+    P3 acc{0.0, 0.0, 0.0};
+    for (int i = 1; i < nv - 1; ++i) {
+        double t = len(crs(sub(q[i], q[0]), sub(q[i + 1], q[0]))) * 0.5;
+        P3 tc = scl(add(add(q[0], q[i]), q[i + 1]), 1.0 / 3.0);
+        acc = add(acc, scl(tc, t));
+        asum += t;
+    }
+    P3 r = asum == 0.0 ? q[0] : scl(acc, 1.0 / asum);
+    c[0] = r.x;
+    c[1] = r.y;
+    c[2] = r.z;
+    *a = asum;
+}
+
+inline uint64_t spread3(uint32_t v) {
+    uint64_t x = v & 0x1fffff;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+inline uint64_t morton(uint32_t x, uint32_t y, uint32_t z) { return spread3(x) << 2 | spread3(y) << 1 | spread3(z); }
+inline uint64_t cell_key(int64_t x, int64_t y, int64_t z) { return ((uint64_t)x << 42) | ((uint64_t)y << 21) | (uint64_t)z; }
+
+// compiler-rt's repeated-squaring power, which Rust's f64::powi lowers to.
+double powi_sq(double a, int b) {
+    bool recip = b < 0;
+    double r = 1.0;
+    for (;;) {
+        if (b & 1) r *= a;
+        b /= 2;
+        if (b == 0) break;
+        a *= a;
+    }
+    return recip ? 1.0 / r : r;
+}
+
+// Column-pivoted modified Gram-Schmidt truncation of the m x m kernel matrix
+// g (linalg.rs:277-381), returning the product Q_k * R_k (P^T applied):
+// the operator the reference applies as U * (V^T x).
+void qr_truncate_product(const std::vector<double>& g, int m, double eps, double* out, int32_t* rank) {
+    std::vector<double> q(g), r((size_t)m * m, 0.0), nrm(m);
+    std::vector<int> perm(m);
+    std::iota(perm.begin(), perm.end(), 0);
+    for (int j = 0; j < m; ++j) {
+        double s = -0.0;
+        for (int i = 0; i < m; ++i) s += g[(size_t)i * m + j] * g[(size_t)i * m + j];
+        nrm[j] = s;
+    }
+    double big = 0.0;
+    for (double v : nrm) big = std::fmax(big, v);
+    const double thr = eps * big;
+    int k = 0;
+    for (int st = 0; st < m; ++st) {
+        int piv = st;
+        for (int j = st + 1; j < m; ++j)
+            if (nrm[j] > nrm[piv]) piv = j;
+        if (nrm[piv] < thr) break;
+        if (piv != st) {
+            std::swap(perm[st], perm[piv]);
+            std::swap(nrm[st], nrm[piv]);
+            for (int i = 0; i < m; ++i) std::swap(q[(size_t)i * m + st], q[(size_t)i * m + piv]);
+            for (int row = 0; row < st; ++row) std::swap(r[(size_t)row * m + st], r[(size_t)row * m + piv]);
+        }
+        double cn = 0.0;
+        for (int i = 0; i < m; ++i) cn += q[(size_t)i * m + st] * q[(size_t)i * m + st];
+        cn = std::sqrt(cn);
+        if (cn < 1e-15) break;
+        r[(size_t)st * m + st] = cn;
+        const double inv = 1.0 / cn;
+        for (int i = 0; i < m; ++i) q[(size_t)i * m + st] *= inv;
+        for (int j = st + 1; j < m; ++j) {
+            double d = 0.0;
+            for (int i = 0; i < m; ++i) d += q[(size_t)i * m + st] * q[(size_t)i * m + j];
+            r[(size_t)st * m + j] = d;
+            for (int i = 0; i < m; ++i) q[(size_t)i * m + j] -= d * q[(size_t)i * m + st];
+            nrm[j] -= d * d;
+            if (nrm[j] < 0.0) nrm[j] = 0.0;
+        }
+        k = st + 1;
+    }
+    // V^T[i][perm[j]] = R[i][j]; product U * V^T.
+    std::vector<double> vt((size_t)k * m);
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < m; ++j) vt[(size_t)i * m + perm[j]] = r[(size_t)i * m + j];
+    for (int a = 0; a < m; ++a)
+        for (int b = 0; b < m; ++b) {
+            double s = 0.0;
+            for (int i = 0; i < k; ++i) s += q[(size_t)a * m + i] * vt[(size_t)i * m + b];
+            out[(size_t)a * m + b] = s;
+        }
+    *rank = k;
+}
+
+}  // namespace
+
+std::vector<double> cheb_roots(int n) {
+    std::vector<double> v(n);
+    for (int m = 0; m < n; ++m) v[m] = std::cos((2.0 * m + 1.0) * kPi / (2.0 * n));
+    return v;
+}
+
+// S_n(x, x_m) = 1/n + 2/n sum_{k=1}^{n-1} T_k(x_m) T_k(x), by recurrence.
+void cheb_weights(double x, int n, const double* roots, double* out) {
+    double tx[32];
+    tx[0] = 1.0;
+    if (n > 1) {
+        tx[1] = x;
+        for (int k = 2; k < n; ++k) tx[k] = 2.0 * x * tx[k - 1] - tx[k - 2];
+    }
+    const double inv_n = 1.0 / n;
+    for (int m = 0; m < n; ++m) {
+        const double xm = roots[m];
+        double sum = 0.5, prev = 1.0, cur = xm;
+        for (int k = 1; k < n; ++k) {
+            double tk;
+            if (k == 1) {
+                tk = xm;
+            } else {
+                tk = 2.0 * xm * cur - prev;
+                prev = cur;
+                cur = tk;
+            }
+            sum += tk * tx[k];
+        }
+        out[m] = 2.0 * inv_n * sum;
+    }
+}
+
+void build_m2l_table(M2LTable& t, int n, int mode) {
+    const int n3 = n * n * n;
+    t.n = n;
+    t.mode = mode;
+    t.K.assign((size_t)343 * n3 * n3, 0.0);
+    t.rank.assign(343, -1);
+    std::vector<double> roots = cheb_roots(n);
+    std::vector<double> ref((size_t)n3 * 3);
+    for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b)
+            for (int c = 0; c < n; ++c) {
+                int m = (a * n + b) * n + c;
+                ref[3 * m] = roots[a];
+                ref[3 * m + 1] = roots[b];
+                ref[3 * m + 2] = roots[c];
+            }
+    const double eps = std::fmax(1e-3 * powi_sq(0.1, n), 1e-14);
+    std::vector<int> slots;
+    for (int s = 0; s < 343; ++s) {
+        int ox = s / 49 - 3, oy = (s / 7) % 7 - 3, oz = s % 7 - 3;
+        if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) >= 2) slots.push_back(s);
+    }
+    auto work = [&](size_t lo, size_t hi) {
+        std::vector<double> g((size_t)n3 * n3);
+        for (size_t si = lo; si < hi; ++si) {
+            int s = slots[si];
+            double sh[3] = {2.0 * (s / 49 - 3), 2.0 * ((s / 7) % 7 - 3), 2.0 * (s % 7 - 3)};
+            for (int m = 0; m < n3; ++m)
+                for (int l = 0; l < n3; ++l) {
+                    double dx = ref[3 * m] - ref[3 * l] - sh[0];
+                    double dy = ref[3 * m + 1] - ref[3 * l + 1] - sh[1];
+                    double dz = ref[3 * m + 2] - ref[3 * l + 2] - sh[2];
+                    double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+                    g[(size_t)m * n3 + l] = r > 0.0 ? 1.0 / r : 0.0;
+                }
+            double* dst = &t.K[(size_t)s * n3 * n3];
+            if (mode == GPX_M2L_EXACT) {
+                std::copy(g.begin(), g.end(), dst);
+                t.rank[s] = n3;
+            } else {
+                qr_truncate_product(g, n3, eps, dst, &t.rank[s]);
+            }
+        }
+    };
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    size_t per = (slots.size() + nt - 1) / nt;
+    for (unsigned i = 0; i < nt; ++i) {
+        size_t lo = i * per, hi = std::min(slots.size(), lo + per);
+        if (lo < hi) th.emplace_back(work, lo, hi);
+    }
+    for (auto& x : th) x.join();
+}
+
+void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, int ncond, int order, int depth) {
+    p.n = order;
+    p.n3 = order * order * order;
+    p.L = depth;
+    p.N = N;
+    p.ncond = ncond;
+    p.far = depth >= 2;
+    // centroids / areas in caller order
+    std::vector<double> c0((size_t)N * 3), a0(N);
+    for (int64_t i = 0; i < N; ++i) panel_centroid_area(verts + 12 * i, &c0[3 * i], &a0[i]);
+    // cubic bounding box (fmm/tree.rs:43-62)
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = 0; i < N; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::fmin(lo[d], c0[3 * i + d]);
+            hi[d] = std::fmax(hi[d], c0[3 * i + d]);
+        }
+    double half = 0.0, center[3];
+    for (int d = 0; d < 3; ++d) {
+        center[d] = 0.5 * (lo[d] + hi[d]);
+        half = std::fmax(half, 0.5 * (hi[d] - lo[d]));
+    }
+    half *= 1.0 + 1e-6;
+    if (half == 0.0) half = 1.0;
+    const uint32_t ncell = 1u << depth;
+    const double leaf_size = 2.0 * half / (double)ncell;
+    const double origin[3] = {center[0] - half, center[1] - half, center[2] - half};
+    // leaf cell per panel (fmm/tree.rs:86-95)
+    std::vector<uint32_t> cell((size_t)N * 3);
+    std::vector<uint64_t> key(N);
+    for (int64_t i = 0; i < N; ++i) {
+        for (int d = 0; d < 3; ++d) {
+            long long idx = (long long)std::floor((c0[3 * i + d] - origin[d]) / leaf_size);
+            idx = std::max(0ll, std::min((long long)ncell - 1, idx));
+            cell[3 * i + d] = (uint32_t)idx;
+        }
+        key[i] = morton(cell[3 * i], cell[3 * i + 1], cell[3 * i + 2]);
+    }
+    p.perm.resize(N);
+    std::iota(p.perm.begin(), p.perm.end(), 0);
+    std::stable_sort(p.perm.begin(), p.perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    p.verts.resize((size_t)N * 12);
+    p.cent.resize((size_t)N * 3);
+    p.area.resize(N);
+    p.cond.resize(N);
+    for (int64_t s = 0; s < N; ++s) {
+        int64_t i = p.perm[s];
+        std::copy(verts + 12 * i, verts + 12 * i + 12, &p.verts[12 * s]);
+        std::copy(&c0[3 * i], &c0[3 * i] + 3, &p.cent[3 * s]);
+        p.area[s] = a0[i];
+        p.cond[s] = cond ? cond[i] : 0;
+    }
+    // levels: leaf boxes in Morton order, then parents
+    std::vector<std::vector<std::array<uint32_t, 3>>> cells(depth + 1);
+    p.leaf_begin.clear();
+    for (int64_t s = 0; s < N; ++s) {
+        int64_t i = p.perm[s];
+        std::array<uint32_t, 3> c = {cell[3 * i], cell[3 * i + 1], cell[3 * i + 2]};
+        if (cells[depth].empty() || cells[depth].back() != c) {
+            cells[depth].push_back(c);
+            p.leaf_begin.push_back(s);
+        }
+    }
+    p.leaf_begin.push_back(N);
+    p.max_leaf = 0;
+    for (size_t k = 0; k + 1 < p.leaf_begin.size(); ++k)
+        p.max_leaf = std::max<int32_t>(p.max_leaf, (int32_t)(p.leaf_begin[k + 1] - p.leaf_begin[k]));
+    for (int l = depth - 1; l >= 0; --l)
+        for (auto& c : cells[l + 1]) {
+            std::array<uint32_t, 3> pc = {c[0] / 2, c[1] / 2, c[2] / 2};
+            if (cells[l].empty() || cells[l].back() != pc) cells[l].push_back(pc);
+        }
+    p.lvl_off.assign(depth + 2, 0);
+    for (int l = 0; l <= depth; ++l) p.lvl_off[l + 1] = p.lvl_off[l] + (int32_t)cells[l].size();
+    const int64_t nb = p.lvl_off[depth + 1];
+    p.box_cell.resize(nb * 3);
+    p.box_parent.assign(nb, -1);
+    p.box_octant.assign(nb, 0);
+    p.lvl_half.resize(depth + 1);
+    std::vector<std::unordered_map<uint64_t, int32_t>> idx(depth + 1);
+    for (int l = 0; l <= depth; ++l) {
+        p.lvl_half[l] = half / (double)(1u << l);
+        for (size_t k = 0; k < cells[l].size(); ++k) {
+            int32_t b = p.lvl_off[l] + (int32_t)k;
+            for (int d = 0; d < 3; ++d) p.box_cell[3 * b + d] = (int32_t)cells[l][k][d];
+            idx[l][cell_key(cells[l][k][0], cells[l][k][1], cells[l][k][2])] = b;
+        }
+    }
+    p.child_first.assign(nb, 0);
+    p.child_count.assign(nb, 0);
+    for (int l = 1; l <= depth; ++l)
+        for (int32_t b = p.lvl_off[l]; b < p.lvl_off[l + 1]; ++b) {
+            const int32_t* c = &p.box_cell[3 * b];
+            const int32_t par = idx[l - 1].at(cell_key(c[0] / 2, c[1] / 2, c[2] / 2));
+            p.box_parent[b] = par;
+            p.box_octant[b] = (c[0] & 1) + 2 * (c[1] & 1) + 4 * (c[2] & 1);
+            if (p.child_count[par] == 0) p.child_first[par] = b;
+            p.child_count[par] += 1;
+        }
+    p.leaf_of.resize(N);
+    for (int64_t k = 0; k + 1 < (int64_t)p.leaf_begin.size(); ++k)
+        for (int64_t s = p.leaf_begin[k]; s < p.leaf_begin[k + 1]; ++s) p.leaf_of[s] = (int32_t)k;
+    // 1-D Chebyshev weights of each panel in its leaf (bbfmm.rs:53-59).
+    std::vector<double> roots = cheb_roots(order);
+    p.w1d.resize((size_t)N * 3 * order);
+    const double hl = p.lvl_half[depth];
+    for (int64_t k = 0; k + 1 < (int64_t)p.leaf_begin.size(); ++k) {
+        int32_t b = p.lvl_off[depth] + (int32_t)k;
+        double ctr[3];
+        for (int d = 0; d < 3; ++d) ctr[d] = origin[d] + ((double)p.box_cell[3 * b + d] + 0.5) * 2.0 * hl;
+        for (int64_t s = p.leaf_begin[k]; s < p.leaf_begin[k + 1]; ++s)
+            for (int d = 0; d < 3; ++d)
+                cheb_weights((p.cent[3 * s + d] - ctr[d]) / hl, order, roots.data(), &p.w1d[(s * 3 + d) * order]);
+    }
+    // near blocks: self leaf first, then neighbours in dx,dy,dz order
+    const int64_t nl = p.nleaf();
+    p.near_off.assign(nl + 1, 0);
+    p.near_src.clear();
+    p.near_S.assign(nl, 0);
+    p.nval_off.assign(nl + 1, 0);
+    p.max_S = 0;
+    const int64_t ncl = 1ll << depth;
+    for (int64_t k = 0; k < nl; ++k) {
+        int32_t b = p.lvl_off[depth] + (int32_t)k;
+        const int32_t* c = &p.box_cell[3 * b];
+        p.near_src.push_back((int32_t)k);
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dz = -1; dz <= 1; ++dz) {
+                    if (!dx && !dy && !dz) continue;
+                    int64_t x = c[0] + dx, y = c[1] + dy, z = c[2] + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= ncl || y >= ncl || z >= ncl) continue;
+                    auto it = idx[depth].find(cell_key(x, y, z));
+                    if (it != idx[depth].end()) p.near_src.push_back(it->second - p.lvl_off[depth]);
+                }
+        p.near_off[k + 1] = (int32_t)p.near_src.size();
+        int64_t S = 0;
+        for (int32_t e = p.near_off[k]; e < p.near_off[k + 1]; ++e)
+            S += p.leaf_begin[p.near_src[e] + 1] - p.leaf_begin[p.near_src[e]];
+        p.near_S[k] = (int32_t)S;
+        p.max_S = std::max<int32_t>(p.max_S, (int32_t)S);
+        p.nval_off[k + 1] = p.nval_off[k] + (p.leaf_begin[k + 1] - p.leaf_begin[k]) * S;
+    }
+    // interaction lists (fmm/tree.rs:188-209): children of the parent's
+    // neighbourhood that are not neighbours of the box.
+    p.m2l_off.assign(nb + 1, 0);
+    p.m2l_src.clear();
+    p.m2l_slot.clear();
+    for (int64_t b = 0; b < nb; ++b) {
+        int l = 0;
+        while (b >= p.lvl_off[l + 1]) ++l;
+        if (l >= 2) {
+            const int32_t* c = &p.box_cell[3 * b];
+            int64_t pc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
+            const int64_t npc = 1ll << (l - 1);
+            for (int dx = -1; dx <= 1; ++dx)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dz = -1; dz <= 1; ++dz) {
+                        int64_t q[3] = {pc[0] + dx, pc[1] + dy, pc[2] + dz};
+                        if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= npc || q[1] >= npc || q[2] >= npc) continue;
+                        if (!idx[l - 1].count(cell_key(q[0], q[1], q[2]))) continue;
+                        for (int o = 0; o < 8; ++o) {
+                            int64_t ch[3] = {2 * q[0] + (o & 1), 2 * q[1] + ((o >> 1) & 1), 2 * q[2] + ((o >> 2) & 1)};
+                            auto it = idx[l].find(cell_key(ch[0], ch[1], ch[2]));
+                            if (it == idx[l].end()) continue;
+                            int64_t ox = ch[0] - c[0], oy = ch[1] - c[1], oz = ch[2] - c[2];
+                            if (std::max(std::llabs(ox), std::max(std::llabs(oy), std::llabs(oz))) <= 1) continue;
+                            p.m2l_src.push_back(it->second);
+                            p.m2l_slot.push_back((int32_t)(((ox + 3) * 7 + oy + 3) * 7 + oz + 3));
+                        }
+                    }
+        }
+        p.m2l_off[b + 1] = (int64_t)p.m2l_src.size();
+    }
+    // tensor-product M2M operators (bbfmm.rs:89-112)
+    p.m2m1d.assign((size_t)24 * order * order, 0.0);
+    std::vector<double> w(order);
+    for (int o = 0; o < 8; ++o) {
+        const int ob[3] = {o & 1, (o >> 1) & 1, (o >> 2) & 1};
+        for (int axis = 0; axis < 3; ++axis) {
+            const double cc = (2.0 * ob[axis] - 1.0) * 0.5;
+            for (int k = 0; k < order; ++k) {
+                cheb_weights(cc + 0.5 * roots[k], order, roots.data(), w.data());
+                for (int m = 0; m < order; ++m) p.m2m1d[((size_t)(o * 3 + axis) * order + m) * order + k] = w[m];
+            }
+        }
+    }
+}
+
+}  // namespace gpx

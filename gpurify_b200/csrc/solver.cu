@@ -1,0 +1,458 @@
+// Capacitance solve on one GPU: plan upload, Wilton near-field assembly, the
+// precorrected FMM operator, multi-RHS restarted GMRES with one right-hand
+// side per conductor, and the Maxwell-matrix accumulation.
+//
+// Reference path: crates/pex/src/quasistatic/cap/fmm_solver.rs:147-172
+// (FmmCapOperator + DiagJacobi + gmres per conductor) and cap/solver.rs:55-71
+// (unit-conductor right-hand sides, C[i][j] += sigma_k * a_k).  Differences
+// by design: all conductors are solved together (one operator apply per
+// Arnoldi step serves every right-hand side) and the Arnoldi step uses
+// classical Gram-Schmidt with one re-orthogonalisation pass (CGS2) instead of
+// modified Gram-Schmidt, which turns k+1 dependent reductions into two.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+
+#include "kernels.cuh"
+#include "krylov.cuh"
+#include "solver.h"
+
+namespace gpx {
+
+struct DevM2L {
+    int n = 0, mode = 0;
+    DBuf<double> K;
+    std::vector<int32_t> rank;
+};
+
+namespace {
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
+    for (auto& t : ctx.m2l_cache)
+        if (t->n == n && t->mode == mode) return t;
+    M2LTable host;
+    build_m2l_table(host, n, mode);
+    auto d = std::make_shared<DevM2L>();
+    d->n = n;
+    d->mode = mode;
+    d->rank = host.rank;
+    d->K.upload(host.K, ctx.stream);
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+    ctx.m2l_cache.push_back(d);
+    return d;
+}
+
+struct DevPlanBufs {
+    DBuf<double> verts, cent, area, w1d, m2m1d;
+    DBuf<int32_t> cond, near_off, near_src, near_S, box_parent, box_octant, m2l_src, m2l_slot, child_first,
+        child_count, leaf_of;
+    DBuf<int64_t> leaf_begin, nval_off, m2l_off;
+    DevPlan v{};
+    FarLaunch far{};
+};
+
+void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
+    cudaStream_t s = ctx.stream;
+    d.verts.upload(p.verts, s);
+    d.cent.upload(p.cent, s);
+    d.area.upload(p.area, s);
+    d.w1d.upload(p.w1d, s);
+    d.m2m1d.upload(p.m2m1d, s);
+    d.cond.upload(p.cond, s);
+    d.near_off.upload(p.near_off, s);
+    d.near_src.upload(p.near_src, s);
+    d.near_S.upload(p.near_S, s);
+    d.box_parent.upload(p.box_parent, s);
+    d.box_octant.upload(p.box_octant, s);
+    d.m2l_src.upload(p.m2l_src, s);
+    d.m2l_slot.upload(p.m2l_slot, s);
+    d.child_first.upload(p.child_first, s);
+    d.child_count.upload(p.child_count, s);
+    d.leaf_of.upload(p.leaf_of, s);
+    d.leaf_begin.upload(p.leaf_begin, s);
+    d.nval_off.upload(p.nval_off, s);
+    d.m2l_off.upload(p.m2l_off, s);
+    DevPlan& v = d.v;
+    v.n = p.n;
+    v.n3 = p.n3;
+    v.L = p.L;
+    v.N = p.N;
+    v.nleaf = (int32_t)p.nleaf();
+    v.nbox = (int32_t)p.nbox();
+    v.leaf_box0 = p.lvl_off[p.L];
+    v.verts = d.verts.p;
+    v.cent = d.cent.p;
+    v.area = d.area.p;
+    v.cond = d.cond.p;
+    v.w1d = d.w1d.p;
+    v.leaf_begin = d.leaf_begin.p;
+    v.near_off = d.near_off.p;
+    v.near_src = d.near_src.p;
+    v.near_S = d.near_S.p;
+    v.nval_off = d.nval_off.p;
+    v.box_parent = d.box_parent.p;
+    v.box_octant = d.box_octant.p;
+    v.m2l_off = d.m2l_off.p;
+    v.m2l_src = d.m2l_src.p;
+    v.m2l_slot = d.m2l_slot.p;
+    v.m2m1d = d.m2m1d.p;
+    v.m2l_K = m2l ? m2l->K.p : nullptr;
+    d.far.lvl_off = p.lvl_off.data();
+    d.far.lvl_half = p.lvl_half.data();
+    d.far.child_first = d.child_first.p;
+    d.far.child_count = d.child_count.p;
+    d.far.leaf_of = d.leaf_of.p;
+    d.far.m2l_off = p.m2l_off.data();
+}
+
+// The precorrected potential operator of one plan for R right-hand sides.
+struct Operator {
+    Ctx& ctx;
+    const Plan& pl;
+    DevPlanBufs& d;
+    int R;
+    DBuf<double> P, inv_diag, M, Lc;
+    double t_assembly_s = 0.0;
+    int64_t applies = 0;
+
+    Operator(Ctx& c, const Plan& p, DevPlanBufs& dd, int r) : ctx(c), pl(p), d(dd), R(r) {}
+
+    bool has_far() const { return pl.far && pl.m2l_pairs() > 0; }
+
+    void assemble() {
+        cudaStream_t s = ctx.stream;
+        P.alloc((size_t)pl.nnz(), s);
+        inv_diag.alloc((size_t)pl.N, s);
+        cudaEvent_t e0, e1;
+        GPX_CUDA(cudaEventCreate(&e0));
+        GPX_CUDA(cudaEventCreate(&e1));
+        GPX_CUDA(cudaEventRecord(e0, s));
+        launch_near_assemble(ctx, d.v, pl.nnz(), P.p, kCoulomb);
+        GPX_CUDA(cudaEventRecord(e1, s));
+        launch_diag_inv(ctx, d.v, P.p, inv_diag.p);
+        GPX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        GPX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t_assembly_s = ms * 1e-3;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (has_far()) {
+            M.alloc((size_t)pl.nbox() * pl.n3 * R, s);
+            Lc.alloc((size_t)pl.nbox() * pl.n3 * R, s);
+        }
+    }
+
+    // Y = A X (X, Y: N x R, leaf-sorted panel order).
+    void apply(const double* X, double* Y) {
+        launch_near_apply(ctx, d.v, pl.nnz(), P.p, X, Y, R);
+        if (has_far()) launch_far_apply(ctx, d.v, d.far, X, Y, R, M.p, Lc.p, kCoulomb);
+        applies += 1;
+    }
+};
+
+__global__ void k_accum_c(const int32_t* __restrict__ cond, const double* __restrict__ area,
+                          const double* __restrict__ X, int64_t N, int R, double* __restrict__ C) {
+    const int i = blockIdx.x;
+    const int nsub = 256 / R;
+    const int r = threadIdx.x % R, sub = threadIdx.x / R;
+    double acc = 0.0;
+    if (sub < nsub)
+        for (int64_t n = sub; n < N; n += nsub)
+            if (cond[n] == i) acc += X[n * R + r] * area[n];
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    if (sub == 0) {
+        double s = red[r];
+        for (int k = 1; k < nsub; ++k) s += red[k * R + r];
+        C[(int64_t)i * R + r] = s;
+    }
+}
+
+__global__ void k_clamp_min(double* v, int n, double lo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = fmax(v[i], lo);
+}
+
+struct SolveStats {
+    int iterations = 0;
+    int cycles = 0;
+    double max_resid = 0.0;
+    bool converged = false;
+};
+
+// Restarted right-preconditioned GMRES(m) on all R columns at once
+// (krylov.rs:50-191 per column); X (N x R) receives the solution.
+void gmres_multi(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d_rhs_cond, int R, int64_t N,
+                 double tol, int m, int max_restarts, DBuf<double>& X, SolveStats& st) {
+    cudaStream_t s = ctx.stream;
+    const int64_t NR = N * R;
+    DBuf<double> V, W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
+    DBuf<int32_t> act, done, kused, cnt;
+    V.alloc((size_t)(m + 1) * NR, s);
+    W.alloc(NR, s);
+    Z.alloc(NR, s);
+    Res.alloc(NR, s);
+    H.alloc((size_t)(m + 1) * m * R, s);
+    cs.alloc((size_t)m * R, s);
+    sn.alloc((size_t)m * R, s);
+    g.alloc((size_t)(m + 1) * R, s);
+    y.alloc((size_t)m * R, s);
+    h1.alloc((size_t)(m + 1) * R, s);
+    h2.alloc((size_t)(m + 1) * R, s);
+    for (auto* b : {&hnorm, &bnorm, &bcur, &est, &resid, &beta}) b->alloc(R, s);
+    act.alloc(R, s);
+    done.alloc(R, s);
+    kused.alloc(R, s);
+    cnt.alloc(1, s);
+    const int nblk = reduce_blocks_for(N);
+    partial.alloc((size_t)nblk * (m + 1) * R, s);
+    X.alloc(NR, s);
+    X.zero();
+    done.zero();
+    kused.zero();
+    GmresDev gd{m, R, tol, H.p, cs.p, sn.p, g.p, y.p, h1.p, h2.p, hnorm.p, bnorm.p, bcur.p, est.p, resid.p,
+                act.p, done.p, kused.p};
+    int32_t* hcount = nullptr;
+    GPX_CUDA(cudaMallocHost((void**)&hcount, sizeof(int32_t)));
+    struct HostFree {
+        int32_t* p;
+        ~HostFree() { cudaFreeHost(p); }
+    } hf{hcount};
+    auto read_count = [&](const int32_t* flags, bool count_zero) -> int {
+        launch_count_active(ctx, flags, R, cnt.p);
+        GPX_CUDA(cudaMemcpyAsync(hcount, cnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        GPX_CUDA(cudaStreamSynchronize(s));
+        return count_zero ? R - *hcount : *hcount;
+    };
+    // ||b|| (krylov.rs:58, clamped to the smallest positive normal)
+    launch_residual(ctx, d_cond, d_rhs_cond, nullptr, Res.p, N, R);
+    launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, bnorm.p);
+    {
+        KTimer kt(ctx, K_SMALL);
+        k_clamp_min<<<(R + 63) / 64, 64, 0, s>>>(bnorm.p, R, 2.2250738585072014e-308);
+        GPX_LAUNCH_CHECK();
+        ctx.launches += 1;
+    }
+    st = SolveStats();
+    for (int cycle = 0; cycle < max_restarts; ++cycle) {
+        st.cycles = cycle + 1;
+        launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, beta.p);
+        launch_cycle_start(ctx, gd, beta.p);
+        launch_scale_cols(ctx, Res.p, beta.p, 0.0, V.p, N, R);
+        if (read_count(act.p, false) == 0) break;
+        int kmax = 0;
+        for (int k = 0; k < m; ++k) {
+            const double* Vk = V.p + (int64_t)k * NR;
+            launch_diag_scale(ctx, Vk, op.inv_diag.p, Z.p, N, R);
+            op.apply(Z.p, W.p);
+            launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h1.p, 0);
+            launch_multi_axpy(ctx, V.p, NR, k + 1, h1.p, W.p, N, R);
+            launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h2.p, 0);
+            launch_multi_axpy(ctx, V.p, NR, k + 1, h2.p, W.p, N, R);
+            launch_colnorm(ctx, W.p, N, R, partial.p, nblk, hnorm.p);
+            launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, V.p + (int64_t)(k + 1) * NR, N, R);
+            launch_givens(ctx, gd, k);
+            st.iterations += 1;
+            kmax = k + 1;
+            if (read_count(act.p, false) == 0) break;
+        }
+        launch_trisolve(ctx, gd);
+        launch_combine(ctx, V.p, NR, kmax, y.p, op.inv_diag.p, X.p, N, R);
+        op.apply(X.p, W.p);
+        launch_residual(ctx, d_cond, d_rhs_cond, W.p, Res.p, N, R);
+        launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, beta.p);
+        launch_cycle_end(ctx, gd, beta.p);
+        if (read_count(done.p, true) == 0) break;
+    }
+    std::vector<double> hres(R);
+    std::vector<int32_t> hdone(R);
+    resid.download(hres.data(), R);
+    done.download(hdone.data(), R);
+    GPX_CUDA(cudaStreamSynchronize(s));
+    st.converged = true;
+    for (int r = 0; r < R; ++r) {
+        st.max_resid = std::max(st.max_resid, hres[r]);
+        if (!hdone[r]) st.converged = false;
+    }
+}
+
+}  // namespace
+
+Opts normalize(const gpx_solve_opts* o) {
+    Opts r;
+    if (!o) return r;
+    r.precision = o->precision;
+    r.order = o->order > 0 ? o->order : 4;
+    r.max_level = o->max_level != 0 ? o->max_level : 4;
+    r.m2l_mode = o->m2l_mode;
+    r.tol = o->tol > 0.0 ? o->tol : 1e-8;
+    r.restart = o->restart > 0 ? o->restart : 200;
+    r.max_restarts = o->max_restarts > 0 ? o->max_restarts : 50;
+    r.dense_below = o->dense_below == 0 ? 500 : o->dense_below;
+    r.precond = o->precond;
+    r.solve_ground_rhs = o->solve_ground_rhs;
+    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 5;
+    r.mesh_max_edge = o->mesh_max_edge_m;
+    r.max_panels = o->max_panels;
+    return r;
+}
+
+int choose_depth(const Opts& o, int64_t n) {
+    if (o.dense_below > 0 && n < o.dense_below) return 1;
+    if (o.max_level > 0) return o.max_level;
+    // auto: about 32 panels per occupied leaf for surface meshes (~n^(1/2) leaves per level step)
+    int d = 2;
+    while (d < 10 && (double)n / std::pow(4.0, d) > 32.0) ++d;
+    return d;
+}
+
+static void check_problem(int64_t n, const double* verts, const int32_t* cond, int ncond, int order) {
+    if (n <= 0 || !verts) throw Error(GPX_ERR_CAPACITANCE, "no panels in geometry");
+    if (ncond <= 0 || ncond > 4096) throw Error(GPX_ERR_INVALID_ARG, "n_conductors must be in [1, 4096]");
+    if (order < 2 || order > 8) throw Error(GPX_ERR_INVALID_ARG, "Chebyshev order must be in [2, 8]");
+    for (int64_t i = 0; i < n; ++i) {
+        if (cond && (cond[i] < 0 || cond[i] >= ncond))
+            throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
+        for (int k = 0; k < 12; ++k)
+            if (!std::isfinite(verts[12 * i + k]))
+                throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has a non-finite vertex");
+    }
+}
+
+void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, double* C,
+               gpx_solve_report* rep) {
+    const double t0 = now_s();
+    const int64_t l0 = ctx.launches;
+    check_problem(n, verts, cond, ncond, o.order);
+    if (o.precision != GPX_PREC_FP64)
+        throw Error(GPX_ERR_INVALID_ARG, "mixed precision is not available in this build");
+    const int depth = choose_depth(o, n);
+    const bool dense = depth == 1;
+    const int R = (o.solve_ground_rhs || ncond == 1) ? ncond : ncond - 1;
+    if (R > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
+    Plan plan;
+    build_plan(plan, n, verts, cond, ncond, o.order, depth);
+    std::shared_ptr<DevM2L> m2l;
+    if (plan.far && plan.m2l_pairs() > 0) m2l = get_m2l(ctx, o.order, o.m2l_mode);
+    DevPlanBufs dp;
+    upload_plan(ctx, plan, m2l.get(), dp);
+    Operator op(ctx, plan, dp, R);
+    op.assemble();
+    std::vector<int32_t> rhs_cond(R);
+    for (int r = 0; r < R; ++r) rhs_cond[r] = r;
+    DBuf<int32_t> d_rhs;
+    d_rhs.upload(rhs_cond, ctx.stream);
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+    const double t1 = now_s();
+    DBuf<double> X;
+    SolveStats st;
+    // The all-pairs path stands in for the reference's dense LU (cap/solver.rs:114-117):
+    // solve it to a tighter tolerance so it matches a direct solve.
+    const double tol = dense ? std::min(o.tol, 1e-12) : o.tol;
+    gmres_multi(ctx, op, dp.cond.p, d_rhs.p, R, n, tol, o.restart, o.max_restarts, X, st);
+    DBuf<double> dC;
+    dC.alloc((size_t)ncond * R, ctx.stream);
+    {
+        KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
+        k_accum_c<<<ncond, 256, 0, ctx.stream>>>(dp.cond.p, dp.area.p, X.p, n, R, dC.p);
+        GPX_LAUNCH_CHECK();
+        ctx.launches += 1;
+    }
+    std::vector<double> hc((size_t)ncond * R);
+    dC.download(hc.data(), hc.size());
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+    const double t2 = now_s();
+    for (int i = 0; i < ncond; ++i)
+        for (int j = 0; j < ncond; ++j) {
+            double v;
+            if (j < R)
+                v = hc[(size_t)i * R + j];
+            else if (i < R)
+                v = hc[(size_t)j * R + i];  // substrate column by symmetry
+            else
+                v = std::nan("");
+            C[(size_t)i * ncond + j] = v;
+        }
+    if (rep) {
+        gpx_solve_report& r = *rep;
+        r.n_panels = n;
+        r.n_conductors = ncond;
+        r.n_rhs = R;
+        r.order = o.order;
+        r.max_level = depth;
+        r.n_boxes = plan.nbox();
+        r.n_leaves = plan.nleaf();
+        r.nnz_near = plan.nnz();
+        r.m2l_pairs = plan.m2l_pairs();
+        r.iterations = st.iterations;
+        r.outer_iterations = 0;
+        r.operator_applies = op.applies;
+        r.max_rel_residual = st.max_resid;
+        r.converged = st.converged ? 1 : 0;
+        r.dense = dense ? 1 : 0;
+        r.t_setup_s = t1 - t0;
+        r.t_solve_s = t2 - t1;
+        r.t_total_s = t2 - t0;
+        r.t_near_assembly_s = op.t_assembly_s;
+        r.kernel_launches = ctx.launches - l0;
+    }
+    if (!st.converged)
+        throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge: max relative residual " +
+                                             std::to_string(st.max_resid) + " after " + std::to_string(st.iterations) +
+                                             " iterations");
+}
+
+void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int R, const double* sigma, double* y,
+                    gpx_solve_report* rep) {
+    check_problem(n, verts, nullptr, 1, o.order);
+    if (R <= 0 || R > 256) throw Error(GPX_ERR_INVALID_ARG, "nrhs must be in [1, 256]");
+    const int depth = choose_depth(o, n);
+    Plan plan;
+    build_plan(plan, n, verts, nullptr, 1, o.order, depth);
+    std::shared_ptr<DevM2L> m2l;
+    if (plan.far && plan.m2l_pairs() > 0) m2l = get_m2l(ctx, o.order, o.m2l_mode);
+    DevPlanBufs dp;
+    upload_plan(ctx, plan, m2l.get(), dp);
+    Operator op(ctx, plan, dp, R);
+    op.assemble();
+    std::vector<double> xs((size_t)n * R), ys((size_t)n * R);
+    for (int64_t s = 0; s < n; ++s)
+        for (int r = 0; r < R; ++r) xs[(size_t)s * R + r] = sigma[(size_t)plan.perm[s] * R + r];
+    DBuf<double> X, Y;
+    X.upload(xs, ctx.stream);
+    Y.alloc(xs.size(), ctx.stream);
+    op.apply(X.p, Y.p);
+    Y.download(ys.data(), ys.size());
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+    for (int64_t s = 0; s < n; ++s)
+        for (int r = 0; r < R; ++r) y[(size_t)plan.perm[s] * R + r] = ys[(size_t)s * R + r];
+    if (rep) {
+        rep->n_panels = n;
+        rep->max_level = depth;
+        rep->order = o.order;
+        rep->n_boxes = plan.nbox();
+        rep->n_leaves = plan.nleaf();
+        rep->nnz_near = plan.nnz();
+        rep->m2l_pairs = plan.m2l_pairs();
+        rep->dense = depth == 1;
+        rep->t_near_assembly_s = op.t_assembly_s;
+    }
+}
+
+void potential_matrix(Ctx& ctx, int64_t ns, const double* sv, int64_t nt, const double* pts, double* out) {
+    if (ns <= 0 || nt <= 0) return;
+    DBuf<double> a, b, c;
+    a.upload(sv, (size_t)ns * 12, ctx.stream);
+    b.upload(pts, (size_t)nt * 3, ctx.stream);
+    c.alloc((size_t)ns * nt, ctx.stream);
+    launch_potential_matrix(ctx, a.p, ns, b.p, nt, c.p, kCoulomb);
+    c.download(out, (size_t)ns * nt);
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+}  // namespace gpx

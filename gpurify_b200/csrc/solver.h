@@ -1,0 +1,38 @@
+// Capacitance solve orchestration (plan -> device operator -> multi-RHS GMRES).
+#pragma once
+#include "gpx_common.h"
+#include "plan.h"
+
+namespace gpx {
+
+// Options after defaults are applied.
+struct Opts {
+    int precision = GPX_PREC_FP64;
+    int order = 4, max_level = 4, m2l_mode = GPX_M2L_COMPRESSED;
+    double tol = 1e-8;
+    int restart = 200, max_restarts = 50;
+    int dense_below = 500;
+    int precond = 0;
+    int solve_ground_rhs = 1;
+    int inner_tol_exp = 5;
+    double mesh_max_edge = 0.0;
+    int64_t max_panels = 0;
+};
+Opts normalize(const gpx_solve_opts* o);
+
+// Depth the solver uses for n panels under the options (1 = all pairs).
+int choose_depth(const Opts& o, int64_t n);
+
+// Solve the Maxwell matrix of a panel problem (farads, not k-scaled) into C
+// (ncond x ncond row-major).  Columns not solved are filled by symmetry.
+void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, double* C,
+               gpx_solve_report* rep);
+
+// y = P sigma (sigma, y: n x R row-major in caller panel order).
+void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int R, const double* sigma, double* y,
+                    gpx_solve_report* rep);
+
+// Dense Wilton block.
+void potential_matrix(Ctx& ctx, int64_t ns, const double* sv, int64_t nt, const double* pts, double* out);
+
+}  // namespace gpx

@@ -1,0 +1,231 @@
+/*
+ * gpx_pex.h — C ABI of the B200-native field-solver capacitance extractor.
+ *
+ * Drop-in boundary for the reference's `"pex_method": "field_solver"`
+ * capacitance path.  Plain pointers and sizes only; caller-owned outputs; no
+ * callbacks; no exceptions cross the ABI.  Every call returns a gpx_status;
+ * gpx_last_error() gives the message of the last failing call on a context.
+ * A context owns one CUDA stream on one device and is safe to use from one
+ * thread at a time (use one context per thread for concurrency).
+ *
+ * Entry points and the reference interface each one replaces
+ * (paths relative to the reference project root):
+ *
+ *   gpx_extract_quasistatic  crates/pex/src/bridge.rs:73-147 `extract_quasistatic`
+ *                            (capacitance + fixed via R; the FastHenry sheet-R
+ *                            solve, bridge.rs:144,180-299, stays with the caller)
+ *   gpx_cap_solve_groups     crates/pex/src/bridge.rs:307-443 `solve_capacitance`
+ *   gpx_cap_solve            crates/pex/src/quasistatic/cap/fmm_solver.rs:147-172
+ *                            `fmm_solver::solve` and cap/solver.rs:100-134 `solve`
+ *   gpx_cap_solve_batched    (no single reference function: many independent
+ *                            windows; each window is one gpx_cap_solve)
+ *   gpx_operator_apply       crates/pex/src/quasistatic/cap/fmm_solver.rs:109-129
+ *                            `FmmCapOperator::apply`, for R right-hand sides
+ *   gpx_potential_matrix     crates/pex/src/quasistatic/cap/solver.rs:81-97
+ *                            `assemble_p_set` (Wilton integral, panel.rs:147-208)
+ *   gpx_ctx_create/destroy   crates/backend/src/gpu.rs:270-278 (lazily created,
+ *                            error-contained device context)
+ */
+#ifndef GPX_PEX_H
+#define GPX_PEX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GPX_OK = 0,
+    GPX_ERR_INVALID_ARG = 1,
+    GPX_ERR_CUDA = 2,
+    GPX_ERR_NO_DEVICE = 3,
+    /* BridgeError variants (bridge.rs:35-56) */
+    GPX_ERR_INVALID_DBU = 10,          /* InvalidDatabaseUnit */
+    GPX_ERR_INVALID_PROCESS = 11,      /* InvalidProcessValue */
+    GPX_ERR_UNSUPPORTED_GEOMETRY = 12, /* UnsupportedGeometry (polygon index in err_polygon) */
+    GPX_ERR_GRID_CAPACITY = 13,        /* GridCapacity */
+    GPX_ERR_PANEL_CAPACITY = 14,       /* PanelCapacity */
+    GPX_ERR_CAPACITANCE = 15,          /* Capacitance(msg): includes GMRES non-convergence */
+    GPX_ERR_NON_FINITE = 16,           /* NonFiniteResult */
+    GPX_ERR_OUTPUT_CAPACITY = 20,      /* caller's output buffer too small */
+    GPX_ERR_OUT_OF_MEMORY = 21,
+    GPX_ERR_INTERNAL = 22
+} gpx_status;
+
+typedef struct gpx_ctx gpx_ctx;
+
+/* Create a context on CUDA device `device` (one stream, device buffers and
+ * cached M2L tables).  Fails with GPX_ERR_NO_DEVICE when no such device. */
+gpx_status gpx_ctx_create(gpx_ctx** out, int device);
+void gpx_ctx_destroy(gpx_ctx* ctx);
+/* Message of the last failing call on `ctx` (never NULL; "" after success). */
+const char* gpx_last_error(const gpx_ctx* ctx);
+/* Library version string. */
+const char* gpx_version(void);
+
+typedef enum {
+    GPX_PREC_FP64 = 0,  /* plain: every operator apply and all GMRES work in FP64 */
+    GPX_PREC_MIXED = 1  /* FP32 far field (M2L on tensor cores) + FP32 near apply
+                           inside an FP64 iterative-refinement loop */
+} gpx_precision;
+
+typedef enum {
+    GPX_M2L_COMPRESSED = 0, /* QR-compressed operators, as the reference (bbfmm.rs:132-174) */
+    GPX_M2L_EXACT = 1       /* uncompressed Chebyshev M2L operators */
+} gpx_m2l_mode;
+
+typedef struct {
+    int32_t precision;       /* gpx_precision */
+    int32_t order;           /* Chebyshev order n; 0 -> 4 (bridge.rs:403) */
+    int32_t max_level;       /* uniform octree depth; 0 -> 4 (bridge.rs:403); -1 -> auto */
+    int32_t m2l_mode;        /* gpx_m2l_mode */
+    double tol;              /* GMRES relative residual; 0 -> 1e-8 (bridge.rs:403) */
+    int32_t restart;         /* 0 -> 200 (fmm_solver.rs:164) */
+    int32_t max_restarts;    /* 0 -> 50 */
+    int32_t dense_below;     /* all-pairs (no far field) below this many panels;
+                                0 -> 500 (bridge.rs:30), -1 -> never */
+    int32_t precond;         /* 0 diagonal Jacobi (fmm_solver.rs:133-162), 1 leaf block-Jacobi */
+    int32_t solve_ground_rhs;/* 1: also solve the substrate column (reference does) */
+    int32_t inner_tol_exp;   /* mixed: inner solve tolerance 10^-x; 0 -> 5 */
+    double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
+    int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
+    int32_t reserved[8];
+} gpx_solve_opts;
+
+typedef struct {
+    int64_t n_panels;
+    int32_t n_conductors;
+    int32_t n_rhs;
+    int32_t order, max_level;
+    int64_t n_boxes, n_leaves, nnz_near, m2l_pairs;
+    int32_t iterations;        /* max GMRES iterations over RHS (all cycles, inner solves in mixed) */
+    int32_t outer_iterations;  /* mixed: refinement steps */
+    int64_t operator_applies;  /* multi-RHS operator applies (FP64 + FP32) */
+    double max_rel_residual;   /* final true FP64 relative residual, max over RHS */
+    int32_t converged;
+    int32_t dense;             /* 1 when the all-pairs path ran */
+    double t_panelize_s, t_setup_s, t_solve_s, t_total_s;
+    double t_near_assembly_s;  /* device time of the Wilton near-field assembly */
+    int64_t kernel_launches;
+} gpx_solve_report;
+
+/* Pre-built panels: `verts` n x 12 doubles (4 vertices x xyz, metres; a
+ * triangle repeats its third vertex), `conductor` n ints in [0, n_conductors). */
+typedef struct {
+    int64_t n_panels;
+    const double* verts;
+    const int32_t* conductor;
+    int32_t n_conductors;
+} gpx_panel_problem;
+
+/* Maxwell capacitance matrix (farads, no dielectric scaling) of the panel
+ * problem.  maxwell_out: n_conductors x n_conductors row-major, C[i][j] =
+ * charge on i per volt on j.  Columns not solved (substrate when
+ * opts.solve_ground_rhs == 0: the last conductor) are filled by symmetry. */
+gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
+                         double* maxwell_out, gpx_solve_report* report);
+
+/* Many independent problems in one call; maxwell_out[i] per problem. */
+gpx_status gpx_cap_solve_batched(gpx_ctx* ctx, const gpx_panel_problem* problems, int32_t n_problems,
+                                 const gpx_solve_opts* opts, double* const* maxwell_out,
+                                 gpx_solve_report* reports);
+
+/* y = P sigma for `nrhs` columns (sigma, y: n_panels x nrhs row-major, panel
+ * order of `problem`), P the precorrected operator the solver uses. */
+gpx_status gpx_operator_apply(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
+                              int32_t nrhs, const double* sigma, double* y, gpx_solve_report* report);
+
+/* Dense block out[t][s] = (1/(4 pi eps0)) * Wilton integral of panel s at
+ * point t (n_tgt x n_src row-major). */
+gpx_status gpx_potential_matrix(gpx_ctx* ctx, int64_t n_src, const double* src_verts, int64_t n_tgt,
+                                const double* tgt_points, double* out);
+
+/* ---- bridge level ---- */
+typedef struct {
+    uint32_t net;
+    double z0_m, z1_m, dielectric_k;
+    int64_t rect_offset, rect_count; /* into the rects array, 4 x int32 (x0,y0,x1,y1) DBU each */
+} gpx_volume_group;
+
+/* Replaces bridge.rs:307-443 `solve_capacitance`: groups in the caller's
+ * BTreeMap<(net, layer)> order.  Outputs per net (ascending net id) the net id
+ * and C[i][i] in aF (scaled by k), and optionally the full (nets+1)^2 Maxwell
+ * matrix in farads (k-scaled; last row/column = substrate). */
+gpx_status gpx_cap_solve_groups(gpx_ctx* ctx, const gpx_volume_group* groups, int64_t n_groups,
+                                const int32_t* rects, double xy_scale_m, const gpx_solve_opts* opts,
+                                uint32_t* nets_out, double* cap_af_out, int64_t nets_cap, int64_t* n_nets,
+                                double* maxwell_out, gpx_solve_report* report);
+
+typedef struct {
+    const int32_t* verts_x;
+    const int32_t* verts_y;
+    const uint32_t* poly_vert_start;
+    const uint32_t* poly_vert_len;
+    const uint16_t* poly_layer;
+    int64_t n_poly;
+} gpx_geometry_store;
+
+typedef struct { /* io/pdk.rs:520-544 */
+    uint16_t layer;
+    double sheet_res_ohm_sq, area_cap_af_um2, fringe_cap_af_um, coupling_cap_af_um;
+    double interlayer_cap_af_um2, via_res_ohm, thickness_nm, height_nm, dielectric_k;
+} gpx_layer_params;
+
+typedef struct {
+    const gpx_layer_params* layers;
+    int64_t n_layers;
+    double dbu_nm;
+} gpx_deck;
+
+typedef struct { /* analytical/mod.rs:354-357 NetParasitics */
+    uint32_t net;
+    double r_ohm;   /* fixed via/contact resistance only */
+    double cap_af;
+} gpx_net_parasitics;
+
+/* Replaces bridge.rs:73-147 `extract_quasistatic` for C (and fixed via R).
+ * On GPX_ERR_UNSUPPORTED_GEOMETRY *err_polygon is the polygon index (else
+ * UINT32_MAX), as lib.rs:111-123 maps it into the diagnostic. */
+gpx_status gpx_extract_quasistatic(gpx_ctx* ctx, const gpx_geometry_store* store, const gpx_deck* deck,
+                                   const uint32_t* net_of_poly, int64_t n_net_of_poly,
+                                   const gpx_solve_opts* opts, gpx_net_parasitics* out, int64_t out_cap,
+                                   int64_t* n_out, uint32_t* err_polygon, gpx_solve_report* report);
+
+/* Panelise only (bridge.rs:445-652 + ground plate :346-379): for tests and
+ * callers that keep the panels.  Returns counts in *n_panels / *n_nets. */
+gpx_status gpx_bridge_panelize(gpx_ctx* ctx, const gpx_geometry_store* store, const gpx_deck* deck,
+                               const uint32_t* net_of_poly, int64_t n_net_of_poly,
+                               const gpx_solve_opts* opts, double* verts_out, int32_t* cond_out,
+                               double* eps_out, int64_t cap, int64_t* n_panels, uint32_t* nets_out,
+                               int64_t nets_cap, int64_t* n_nets, uint32_t* err_polygon);
+
+/* ---- instrumentation ---- */
+/* Kernel classes of gpx_ctx_kernel_stats. */
+typedef enum {
+    GPX_K_NEAR_ASSEMBLE = 0, GPX_K_NEAR_APPLY = 1, GPX_K_P2M = 2, GPX_K_M2M = 3, GPX_K_M2L = 4, GPX_K_L2L = 5,
+    GPX_K_L2P = 6, GPX_K_GS_DOT = 7, GPX_K_GS_AXPY = 8, GPX_K_VEC = 9, GPX_K_SMALL = 10, GPX_K_COUNT = 11
+} gpx_kernel_class;
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
+void* gpx_ctx_stream(gpx_ctx* ctx);
+/* Per-kernel CUDA-event timing on the context stream (off by default). */
+gpx_status gpx_ctx_set_profiling(gpx_ctx* ctx, int32_t on);
+/* Accumulated launches, device milliseconds and algorithmic bytes / flops
+ * of one kernel class since the last reset; *total_launches counts every
+ * kernel this context launched. */
+gpx_status gpx_ctx_kernel_stats(gpx_ctx* ctx, int32_t kernel_class, int64_t* launches, double* ms, double* bytes,
+                                double* flops, int64_t* total_launches);
+gpx_status gpx_ctx_reset_stats(gpx_ctx* ctx);
+
+/* Host-only self-check of the octree plan the solver would build for these
+ * panels at (order, depth): index bounds, list disjointness and exact pair
+ * coverage (every ordered panel pair is near or in exactly one M2L pair).
+ * stats[0..6] = leaves, boxes, near pairs, M2L box pairs, far panel pairs,
+ * largest leaf, largest near row.  Needs no device. */
+gpx_status gpx_plan_check(int64_t n_panels, const double* verts, int32_t order, int32_t depth, int64_t* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPX_PEX_H */
