@@ -47,7 +47,8 @@ class SolveOpts(C.Structure):
         ("precision", C.c_int32), ("order", C.c_int32), ("max_level", C.c_int32), ("m2l_mode", C.c_int32),
         ("tol", C.c_double), ("restart", C.c_int32), ("max_restarts", C.c_int32), ("dense_below", C.c_int32),
         ("precond", C.c_int32), ("solve_ground_rhs", C.c_int32), ("inner_tol_exp", C.c_int32),
-        ("mesh_max_edge_m", C.c_double), ("max_panels", C.c_int64), ("reserved", C.c_int32 * 8),
+        ("mesh_max_edge_m", C.c_double), ("max_panels", C.c_int64), ("far_quad", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -59,6 +60,7 @@ class SolveReport(C.Structure):
         ("operator_applies", C.c_int64), ("max_rel_residual", C.c_double), ("converged", C.c_int32),
         ("dense", C.c_int32), ("t_panelize_s", C.c_double), ("t_setup_s", C.c_double), ("t_solve_s", C.c_double),
         ("t_total_s", C.c_double), ("t_near_assembly_s", C.c_double), ("kernel_launches", C.c_int64),
+        ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
     ]
 
     def as_dict(self):

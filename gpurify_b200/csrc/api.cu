@@ -23,6 +23,19 @@ gpx_status fail(gpx_ctx* ctx, gpx_status s, const std::string& msg) {
     return s;
 }
 
+// Copies host<->device byte counts of one call into its report.
+struct CopyMeter {
+    gpx_solve_report* r;
+    int64_t h0, d0;
+    explicit CopyMeter(gpx_solve_report* rep) : r(rep), h0(h2d_counter().load()), d0(d2h_counter().load()) {}
+    ~CopyMeter() {
+        if (r) {
+            r->h2d_bytes = h2d_counter().load() - h0;
+            r->d2h_bytes = d2h_counter().load() - d0;
+        }
+    }
+};
+
 template <class F>
 gpx_status guarded(gpx_ctx* ctx, F&& f, uint32_t* err_polygon = nullptr) {
     if (err_polygon) *err_polygon = 0xFFFFFFFFu;
@@ -134,6 +147,7 @@ gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* pb, const gpx_so
                          gpx_solve_report* report) {
     if (!ctx || !pb || !maxwell_out) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
     if (report) std::memset(report, 0, sizeof(*report));
+    CopyMeter meter(report);
     return guarded(ctx, [&] {
         Opts o = normalize(opts);
         cap_solve(ctx->impl, pb->n_panels, pb->verts, pb->conductor, pb->n_conductors, o, maxwell_out, report);
@@ -176,6 +190,7 @@ gpx_status gpx_cap_solve_groups(gpx_ctx* ctx, const gpx_volume_group* groups, in
                                 int64_t nets_cap, int64_t* n_nets, double* maxwell_out, gpx_solve_report* report) {
     if (!ctx || (n_groups > 0 && (!groups || !rects)) || !n_nets) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
     if (report) std::memset(report, 0, sizeof(*report));
+    CopyMeter meter(report);
     return guarded(ctx, [&] {
         Opts o = normalize(opts);
         *n_nets = 0;
@@ -208,6 +223,7 @@ gpx_status gpx_extract_quasistatic(gpx_ctx* ctx, const gpx_geometry_store* store
                                    gpx_solve_report* report) {
     if (!ctx || !store || !deck || !n_out) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
     if (report) std::memset(report, 0, sizeof(*report));
+    CopyMeter meter(report);
     return guarded(
         ctx,
         [&] {

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdint>
 #include <cstdio>
 #include <memory>
@@ -36,6 +38,16 @@ struct Error : std::runtime_error {
                                                                : GPX_ERR_CUDA,                \
                                std::string(#call) + ": " + cudaGetErrorString(e_));           \
     } while (0)
+
+// Host<->device bytes copied by the library (all contexts of the process).
+inline std::atomic<int64_t>& h2d_counter() {
+    static std::atomic<int64_t> c{0};
+    return c;
+}
+inline std::atomic<int64_t>& d2h_counter() {
+    static std::atomic<int64_t> c{0};
+    return c;
+}
 
 // Stream-ordered device buffer (cudaMallocAsync pool of the context stream).
 template <class T>
@@ -74,10 +86,12 @@ struct DBuf {
     void upload(const T* h, size_t count, cudaStream_t stream) {
         alloc(count, stream);
         if (count) GPX_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+        h2d_counter() += (int64_t)(count * sizeof(T));
     }
     void upload(const std::vector<T>& v, cudaStream_t stream) { upload(v.data(), v.size(), stream); }
     void download(T* h, size_t count) const {
         if (count) GPX_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+        d2h_counter() += (int64_t)(count * sizeof(T));
     }
 };
 

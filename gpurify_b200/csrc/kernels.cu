@@ -68,6 +68,14 @@ __device__ __forceinline__ void prep_source(const double* g, SrcPanel& s) {
 
 // Wilton integral of one prepared panel at point p (panel.rs:147-208).  A
 // zero-length edge (the repeated vertex of a triangle) contributes nothing.
+//
+// The log term is evaluated in an algebraically identical, cancellation-free
+// form: with r0^2 = pp^2 + d^2, num = r+ + s+ and den = r- + s- are formed as
+// r0^2 / (r - s) when s < 0, and log(num/den) = log1p((num-den)/den) with
+// num - den = el * (num + den) / (r+ + r-).  Where the reference's direct
+// form rounds num or den to <= 0 it falls back to the asinh difference; the
+// stable form needs no fallback, and a point on the edge line (r0 = 0)
+// contributes 0 exactly as the reference's fallback does.
 __device__ __forceinline__ double wilton(const SrcPanel& s, double px, double py, double pz) {
     const double d = (px - s.v[0][0]) * s.n[0] + (py - s.v[0][1]) * s.n[1] + (pz - s.v[0][2]) * s.n[2];
     const double p0[3] = {px - s.n[0] * d, py - s.n[1] * d, pz - s.n[2] * d};
@@ -86,16 +94,10 @@ __device__ __forceinline__ double wilton(const SrcPanel& s, double px, double py
         const double r0sq = pp * pp + d * d;
         const double rp = sqrt(sp * sp + r0sq);
         const double rm = sqrt(sm * sm + r0sq);
-        const double num = rp + sp, den = rm + sm;
-        double lt;
-        if (num > 0.0 && den > 0.0) {
-            lt = pp * log(num / den);
-        } else if (fabs(den) > 0.0) {
-            const double r0 = sqrt(r0sq);
-            lt = r0 == 0.0 ? 0.0 : pp * (asinh(sp / r0) - asinh(sm / r0));
-        } else {
-            lt = 0.0;
-        }
+        const double num = sp >= 0.0 ? rp + sp : r0sq / (rp - sp);
+        const double den = sm >= 0.0 ? rm + sm : r0sq / (rm - sm);
+        double lt = 0.0;
+        if (num > 0.0 && den > 0.0) lt = pp * log1p(s.el[i] * (num + den) / ((rp + rm) * den));
         double at = 0.0;
         if (ad > 0.0 && pp != 0.0) {
             const double tp = (pp * sp) / (r0sq + ad * rp);
@@ -110,11 +112,13 @@ __device__ __forceinline__ double wilton(const SrcPanel& s, double px, double py
 constexpr int kAsmThreads = 256;
 constexpr int kAsmTile = 64;
 
-// One CTA per target leaf: P block m_t x S_t, row-major.
+// One CTA per work item (target leaf, <= 128 rows): rows of the leaf's
+// P block m_t x S_t, row-major.
 __global__ void __launch_bounds__(kAsmThreads) k_near_assemble(DevPlan p, double* __restrict__ P, double coef) {
-    const int t = blockIdx.x;
+    const int t = p.item_leaf[blockIdx.x];
+    const int r0 = p.item_row0[blockIdx.x];
     const int64_t tb = p.leaf_begin[t];
-    const int m = (int)(p.leaf_begin[t + 1] - tb);
+    const int m = min((int)(p.leaf_begin[t + 1] - tb), r0 + 128);
     const int S = p.near_S[t];
     const int64_t off = p.nval_off[t];
     __shared__ int64_t s_beg[28];
@@ -144,7 +148,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_near_assemble(DevPlan p, double
         for (int j = lane; j < cnt; j += 32) {
             SrcPanel sp;
             prep_source(p.verts + 12 * s_gid[j], sp);
-            for (int row = warp; row < m; row += nw) {
+            for (int row = r0 + warp; row < m; row += nw) {
                 const double* c = p.cent + 3 * (tb + row);
                 P[off + (int64_t)row * S + base + j] = coef * wilton(sp, c[0], c[1], c[2]);
             }
@@ -169,9 +173,10 @@ __global__ void k_diag_inv(DevPlan p, const double* __restrict__ P, double* __re
 constexpr int kNaRPW = 16;  // rows per warp per pass (128 rows per pass)
 __global__ void __launch_bounds__(256) k_near_apply(DevPlan p, const double* __restrict__ P,
                                                      const double* __restrict__ X, double* __restrict__ Y, int R) {
-    const int t = blockIdx.x;
+    const int t = p.item_leaf[blockIdx.x];
+    const int r0 = p.item_row0[blockIdx.x];
     const int64_t tb = p.leaf_begin[t];
-    const int m = (int)(p.leaf_begin[t + 1] - tb);
+    const int m = min((int)(p.leaf_begin[t + 1] - tb), r0 + 8 * kNaRPW);
     const int S = p.near_S[t];
     const int64_t off = p.nval_off[t];
     __shared__ int64_t s_beg[28];
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(256) k_near_apply(DevPlan p, const double* __r
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int rc = 0; rc < R; rc += 64) {
-        for (int rb = 0; rb < m; rb += 8 * kNaRPW) {
+        for (int rb = r0; rb < m; rb += 8 * kNaRPW) {
             double acc0[kNaRPW], acc1[kNaRPW];
 #pragma unroll
             for (int i = 0; i < kNaRPW; ++i) acc0[i] = acc1[i] = 0.0;
@@ -238,19 +243,94 @@ __global__ void __launch_bounds__(256) k_near_apply(DevPlan p, const double* __r
     }
 }
 
+// 1-D Chebyshev interpolation weights S_n(x, x_m) (fmm/chebyshev.rs:41-74).
+__device__ __forceinline__ void cheb_w(double x, int n, const double* roots, double* out) {
+    double tx[8];
+    tx[0] = 1.0;
+    if (n > 1) tx[1] = x;
+    for (int k = 2; k < n; ++k) tx[k] = 2.0 * x * tx[k - 1] - tx[k - 2];
+    const double inv_n = 1.0 / n;
+    for (int m = 0; m < n; ++m) {
+        const double xm = roots[m];
+        double sum = 0.5, prev = 1.0, cur = xm;
+        for (int k = 1; k < n; ++k) {
+            double tk;
+            if (k == 1) {
+                tk = xm;
+            } else {
+                tk = 2.0 * xm * cur - prev;
+                prev = cur;
+                cur = tk;
+            }
+            sum += tk * tx[k];
+        }
+        out[m] = 2.0 * inv_n * sum;
+    }
+}
+
+// One thread per panel: W[j][m] for all n^3 nodes.
+__global__ void k_src_weights(DevPlan p, int quad, double* __restrict__ W) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.N) return;
+    const int n = p.n, n3 = p.n3;
+    const double* ctr = p.leaf_ctr + 3 * p.leaf_of[j];
+    const double ih = 1.0 / p.leaf_half;
+    double* out = W + j * n3;
+    for (int m = 0; m < n3; ++m) out[m] = 0.0;
+    double w[3][8];
+    if (quad == 0) {
+        for (int d = 0; d < 3; ++d) cheb_w((p.cent[3 * j + d] - ctr[d]) * ih, n, p.roots, w[d]);
+        for (int a = 0; a < n; ++a)
+            for (int b = 0; b < n; ++b)
+                for (int c = 0; c < n; ++c) out[(a * n + b) * n + c] = (w[0][a] * w[1][b]) * w[2][c];
+        return;
+    }
+    // 2x2 Gauss rule on the bilinear map of the quad (a triangle is the quad
+    // with a collapsed edge); weights normalised to sum to one.
+    const double* v = p.verts + 12 * j;
+    const double g = 0.57735026918962576451;
+    double jw[4], pts[4][3], jsum = 0.0;
+    for (int q = 0; q < 4; ++q) {
+        const double u = (q & 1) ? g : -g, t = (q & 2) ? g : -g;
+        const double N[4] = {0.25 * (1 - u) * (1 - t), 0.25 * (1 + u) * (1 - t), 0.25 * (1 + u) * (1 + t),
+                             0.25 * (1 - u) * (1 + t)};
+        const double dNu[4] = {-0.25 * (1 - t), 0.25 * (1 - t), 0.25 * (1 + t), -0.25 * (1 + t)};
+        const double dNt[4] = {-0.25 * (1 - u), -0.25 * (1 + u), 0.25 * (1 + u), 0.25 * (1 - u)};
+        double xu[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+        for (int d = 0; d < 3; ++d) {
+            pts[q][d] = 0.0;
+            for (int k = 0; k < 4; ++k) {
+                pts[q][d] += N[k] * v[3 * k + d];
+                xu[d] += dNu[k] * v[3 * k + d];
+                xt[d] += dNt[k] * v[3 * k + d];
+            }
+        }
+        const double cx = xu[1] * xt[2] - xu[2] * xt[1], cy = xu[2] * xt[0] - xu[0] * xt[2],
+                     cz = xu[0] * xt[1] - xu[1] * xt[0];
+        jw[q] = sqrt(cx * cx + cy * cy + cz * cz);
+        jsum += jw[q];
+    }
+    for (int q = 0; q < 4; ++q) {
+        const double wq = jsum > 0.0 ? jw[q] / jsum : 0.25;
+        for (int d = 0; d < 3; ++d) cheb_w((pts[q][d] - ctr[d]) * ih, n, p.roots, w[d]);
+        for (int a = 0; a < n; ++a)
+            for (int b = 0; b < n; ++b) {
+                const double wab = wq * w[0][a] * w[1][b];
+                for (int c = 0; c < n; ++c) out[(a * n + b) * n + c] += wab * w[2][c];
+            }
+    }
+}
+
 // P2M: M[leafbox][m][r] = sum_j W_j[m] * area_j * X[j][r]; one thread per (m, r).
 __global__ void k_p2m(DevPlan p, const double* __restrict__ X, double* __restrict__ M, int R) {
     const int t = blockIdx.x;
     const int o = blockIdx.y * blockDim.x + threadIdx.x;
-    const int n = p.n, n3 = p.n3;
+    const int n3 = p.n3;
     if (o >= n3 * R) return;
     const int mi = o / R, r = o % R;
-    const int a = mi / (n * n), b = (mi / n) % n, c = mi % n;
     double acc = 0.0;
-    for (int64_t j = p.leaf_begin[t]; j < p.leaf_begin[t + 1]; ++j) {
-        const double* w = p.w1d + j * 3 * n;
-        acc += (w[a] * w[n + b]) * w[2 * n + c] * (p.area[j] * X[j * R + r]);
-    }
+    for (int64_t j = p.leaf_begin[t]; j < p.leaf_begin[t + 1]; ++j)
+        acc += p.wsrc[j * n3 + mi] * (p.area[j] * X[j * R + r]);
     M[((int64_t)(p.leaf_box0 + t) * n3 + mi) * R + r] = acc;
 }
 
@@ -406,7 +486,7 @@ __global__ void k_potential_matrix(const double* __restrict__ sv, int64_t ns, co
 void launch_near_assemble(Ctx& c, const DevPlan& p, int64_t nnz, double* P, double coef) {
     if (p.nleaf == 0) return;
     KTimer t(c, K_NEAR_ASSEMBLE, 8.0 * nnz, (double)nnz);
-    k_near_assemble<<<p.nleaf, kAsmThreads, 0, c.stream>>>(p, P, coef);
+    k_near_assemble<<<p.nitems, kAsmThreads, 0, c.stream>>>(p, P, coef);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
@@ -422,7 +502,7 @@ void launch_diag_inv(Ctx& c, const DevPlan& p, const double* P, double* inv) {
 void launch_near_apply(Ctx& c, const DevPlan& p, int64_t nnz, const double* P, const double* X, double* Y, int R) {
     if (p.nleaf == 0) return;
     KTimer t(c, K_NEAR_APPLY, 8.0 * nnz + 16.0 * (double)p.N * R, 2.0 * (double)nnz * R);
-    k_near_apply<<<p.nleaf, 256, 0, c.stream>>>(p, P, X, Y, R);
+    k_near_apply<<<p.nitems, 256, 0, c.stream>>>(p, P, X, Y, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
@@ -473,6 +553,14 @@ void launch_far_apply(Ctx& c, const DevPlan& p, const FarLaunch& f, const double
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
+}
+
+void launch_src_weights(Ctx& c, const DevPlan& p, int quad, double* W) {
+    if (p.N == 0) return;
+    KTimer t(c, K_SMALL);
+    k_src_weights<<<(unsigned)((p.N + 127) / 128), 128, 0, c.stream>>>(p, quad, W);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
 }
 
 void launch_potential_matrix(Ctx& c, const double* sv, int64_t ns, const double* pts, int64_t nt, double* out,

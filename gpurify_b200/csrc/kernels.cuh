@@ -12,7 +12,7 @@ namespace gpx {
 struct DevPlan {
     int n, n3, L;
     int64_t N;
-    int32_t nleaf, nbox, leaf_box0;
+    int32_t nleaf, nbox, leaf_box0, nitems;
     const double* verts;      // 12 per panel
     const double* cent;       // 3 per panel
     const double* area;
@@ -23,6 +23,8 @@ struct DevPlan {
     const int32_t* near_src;
     const int32_t* near_S;
     const int64_t* nval_off;
+    const int32_t* item_leaf;  // near-field work items (leaf, first row), <= 128 rows each
+    const int32_t* item_row0;
     const int32_t* box_parent;
     const int32_t* box_octant;
     const int64_t* m2l_off;
@@ -30,6 +32,11 @@ struct DevPlan {
     const int32_t* m2l_slot;
     const double* m2m1d;      // 24 n x n
     const double* m2l_K;      // 343 n3 x n3 (FP64 table)
+    const double* leaf_ctr;   // 3 per leaf: box centre
+    const int32_t* leaf_of;   // per panel: its leaf
+    double leaf_half;
+    double roots[8];          // Chebyshev roots of order n
+    const double* wsrc;       // N x n3 far-field source weights (P2M), set by launch_src_weights
 };
 
 // Wilton near-field block assembly: P (nnz doubles), one CTA per target leaf.
@@ -51,6 +58,10 @@ struct FarLaunch {
 // coef; M and Lc are nbox x n3 x R scratch.
 void launch_far_apply(Ctx& c, const DevPlan& p, const FarLaunch& f, const double* X, double* Y, int R, double* M,
                       double* Lc, double coef);
+// Far-field source weights W[j][m]: the Chebyshev interpolation weights of
+// panel j's charge in its leaf; quad 0: at the centroid (the reference's
+// point lumping), quad 1: averaged over 2x2 Gauss points of the panel.
+void launch_src_weights(Ctx& c, const DevPlan& p, int quad, double* W);
 // Dense all-pairs block for arbitrary target points.
 void launch_potential_matrix(Ctx& c, const double* src_verts, int64_t ns, const double* pts, int64_t nt, double* out,
                              double coef);

@@ -244,6 +244,7 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
     const uint32_t ncell = 1u << depth;
     const double leaf_size = 2.0 * half / (double)ncell;
     const double origin[3] = {center[0] - half, center[1] - half, center[2] - half};
+    for (int dd = 0; dd < 3; ++dd) p.origin[dd] = origin[dd];
     // leaf cell per panel (fmm/tree.rs:86-95)
     std::vector<uint32_t> cell((size_t)N * 3);
     std::vector<uint64_t> key(N);
@@ -360,6 +361,13 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
         p.max_S = std::max<int32_t>(p.max_S, (int32_t)S);
         p.nval_off[k + 1] = p.nval_off[k] + (p.leaf_begin[k + 1] - p.leaf_begin[k]) * S;
     }
+    p.item_leaf.clear();
+    p.item_row0.clear();
+    for (int64_t k = 0; k < nl; ++k)
+        for (int64_t r = 0; r < p.leaf_begin[k + 1] - p.leaf_begin[k]; r += Plan::kRowsPerItem) {
+            p.item_leaf.push_back((int32_t)k);
+            p.item_row0.push_back((int32_t)r);
+        }
     // interaction lists (fmm/tree.rs:188-209): children of the parent's
     // neighbourhood that are not neighbours of the box.
     p.m2l_off.assign(nb + 1, 0);

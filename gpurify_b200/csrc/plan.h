@@ -31,6 +31,7 @@ struct Plan {
     std::vector<int32_t> box_parent;
     std::vector<int32_t> box_octant;
     std::vector<double> lvl_half;   // per level
+    double origin[3] = {0, 0, 0};    // low corner of the root box
     std::vector<int32_t> child_first, child_count;  // per box: contiguous child range (next level)
 
     // Leaves (level L): leaf k is box lvl_off[L] + k; panels [leaf_begin[k], leaf_begin[k+1]).
@@ -45,6 +46,9 @@ struct Plan {
     std::vector<int32_t> near_S;      // total source panels per target leaf
     std::vector<int64_t> nval_off;    // nleaf+1: value offset of each leaf's m_t x S_t block
     int32_t max_S = 0;
+    // Near-field work items: (target leaf, first row), at most kRowsPerItem rows each.
+    static constexpr int kRowsPerItem = 128;
+    std::vector<int32_t> item_leaf, item_row0;
 
     // M2L: per target box (global box index), sources + operator slot.
     std::vector<int64_t> m2l_off;     // nbox+1

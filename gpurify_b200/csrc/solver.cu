@@ -49,8 +49,9 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
 struct DevPlanBufs {
     DBuf<double> verts, cent, area, w1d, m2m1d;
     DBuf<int32_t> cond, near_off, near_src, near_S, box_parent, box_octant, m2l_src, m2l_slot, child_first,
-        child_count, leaf_of;
+        child_count, leaf_of, item_leaf, item_row0;
     DBuf<int64_t> leaf_begin, nval_off, m2l_off;
+    DBuf<double> leaf_ctr, wsrc;
     DevPlan v{};
     FarLaunch far{};
 };
@@ -76,7 +77,28 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
     d.leaf_begin.upload(p.leaf_begin, s);
     d.nval_off.upload(p.nval_off, s);
     d.m2l_off.upload(p.m2l_off, s);
+    {
+        std::vector<double> ctr((size_t)p.nleaf() * 3);
+        const double hl = p.lvl_half[p.L];
+        for (int64_t k = 0; k < p.nleaf(); ++k)
+            for (int dd = 0; dd < 3; ++dd)
+                ctr[3 * k + dd] =
+                    p.origin[dd] + ((double)p.box_cell[3 * (p.lvl_off[p.L] + k) + dd] + 0.5) * 2.0 * hl;
+        d.leaf_ctr.upload(ctr, s);
+    }
+    d.item_leaf.upload(p.item_leaf, s);
+    d.item_row0.upload(p.item_row0, s);
     DevPlan& v = d.v;
+    v.nitems = (int32_t)p.item_leaf.size();
+    v.item_leaf = d.item_leaf.p;
+    v.leaf_ctr = d.leaf_ctr.p;
+    v.leaf_of = d.leaf_of.p;
+    v.leaf_half = p.lvl_half[p.L];
+    {
+        std::vector<double> roots = cheb_roots(p.n);
+        for (int k = 0; k < p.n && k < 8; ++k) v.roots[k] = roots[k];
+    }
+    v.item_row0 = d.item_row0.p;
     v.n = p.n;
     v.n3 = p.n3;
     v.L = p.L;
@@ -115,11 +137,12 @@ struct Operator {
     const Plan& pl;
     DevPlanBufs& d;
     int R;
+    int far_quad;
     DBuf<double> P, inv_diag, M, Lc;
     double t_assembly_s = 0.0;
     int64_t applies = 0;
 
-    Operator(Ctx& c, const Plan& p, DevPlanBufs& dd, int r) : ctx(c), pl(p), d(dd), R(r) {}
+    Operator(Ctx& c, const Plan& p, DevPlanBufs& dd, int r, int fq) : ctx(c), pl(p), d(dd), R(r), far_quad(fq) {}
 
     bool has_far() const { return pl.far && pl.m2l_pairs() > 0; }
 
@@ -143,6 +166,9 @@ struct Operator {
         if (has_far()) {
             M.alloc((size_t)pl.nbox() * pl.n3 * R, s);
             Lc.alloc((size_t)pl.nbox() * pl.n3 * R, s);
+            d.wsrc.alloc((size_t)pl.N * pl.n3, s);
+            launch_src_weights(ctx, d.v, far_quad, d.wsrc.p);
+            d.v.wsrc = d.wsrc.p;
         }
     }
 
@@ -299,6 +325,7 @@ Opts normalize(const gpx_solve_opts* o) {
     r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 5;
     r.mesh_max_edge = o->mesh_max_edge_m;
     r.max_panels = o->max_panels;
+    r.far_quad = o->far_quad;
     return r;
 }
 
@@ -341,7 +368,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     if (plan.far && plan.m2l_pairs() > 0) m2l = get_m2l(ctx, o.order, o.m2l_mode);
     DevPlanBufs dp;
     upload_plan(ctx, plan, m2l.get(), dp);
-    Operator op(ctx, plan, dp, R);
+    Operator op(ctx, plan, dp, R, o.far_quad);
     op.assemble();
     std::vector<int32_t> rhs_cond(R);
     for (int r = 0; r < R; ++r) rhs_cond[r] = r;
@@ -418,7 +445,7 @@ void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int
     if (plan.far && plan.m2l_pairs() > 0) m2l = get_m2l(ctx, o.order, o.m2l_mode);
     DevPlanBufs dp;
     upload_plan(ctx, plan, m2l.get(), dp);
-    Operator op(ctx, plan, dp, R);
+    Operator op(ctx, plan, dp, R, o.far_quad);
     op.assemble();
     std::vector<double> xs((size_t)n * R), ys((size_t)n * R);
     for (int64_t s = 0; s < n; ++s)

@@ -17,6 +17,7 @@ struct Opts {
     int inner_tol_exp = 5;
     double mesh_max_edge = 0.0;
     int64_t max_panels = 0;
+    int far_quad = 0;
 };
 Opts normalize(const gpx_solve_opts* o);
 

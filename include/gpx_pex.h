@@ -91,7 +91,9 @@ typedef struct {
     int32_t inner_tol_exp;   /* mixed: inner solve tolerance 10^-x; 0 -> 5 */
     double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
-    int32_t reserved[8];
+    int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
+                                (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
+    int32_t reserved[7];
 } gpx_solve_opts;
 
 typedef struct {
@@ -109,6 +111,7 @@ typedef struct {
     double t_panelize_s, t_setup_s, t_solve_s, t_total_s;
     double t_near_assembly_s;  /* device time of the Wilton near-field assembly */
     int64_t kernel_launches;
+    int64_t h2d_bytes, d2h_bytes;  /* host<->device copies made by the call */
 } gpx_solve_report;
 
 /* Pre-built panels: `verts` n x 12 doubles (4 vertices x xyz, metres; a

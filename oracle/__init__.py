@@ -61,6 +61,7 @@ class FmmOpts(C.Structure):
         ("max_restarts", C.c_int32),
         ("tol", C.c_double),
         ("threads", C.c_int32),
+        ("rhs_limit", C.c_int32),
     ]
 
 
@@ -232,11 +233,13 @@ def cap_dense_gmres(verts, cond, ncond) -> np.ndarray:
     return C_
 
 
-def cap_fmm(verts, cond, ncond, order=4, max_level=4, tol=1e-8, restart=200, max_restarts=50, threads=0):
-    """cap::fmm_solver::solve (cap/fmm_solver.rs:147-172). Returns (C, report dict)."""
+def cap_fmm(verts, cond, ncond, order=4, max_level=4, tol=1e-8, restart=200, max_restarts=50, threads=0,
+            rhs_limit=0):
+    """cap::fmm_solver::solve (cap/fmm_solver.rs:147-172). Returns (C, report dict).
+    ``rhs_limit`` > 0 solves only the first conductors (bounded CPU samples)."""
     v, c = _prep(verts, cond)
     C_ = np.zeros((ncond, ncond))
-    o = FmmOpts(order, max_level, restart, max_restarts, tol, threads)
+    o = FmmOpts(order, max_level, restart, max_restarts, tol, threads, rhs_limit)
     r = FmmReport()
     rc = lib().orc_cap_fmm(len(v), v.ctypes.data, c.ctypes.data, ncond, C.byref(o), C_.ctypes.data, C.byref(r))
     if rc != 0:

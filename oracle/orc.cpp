@@ -1534,7 +1534,8 @@ int orc_cap_fmm(int64_t n, const double* verts, const int32_t* cond, int32_t nco
     std::fill(C, C + (size_t)ncond * ncond, 0.0);
     orc_fmm_report r{};
     r.all_converged = 1;
-    for (int j = 0; j < ncond; ++j) {
+    const int nrhs = o->rhs_limit > 0 ? std::min(o->rhs_limit, ncond) : ncond;
+    for (int j = 0; j < nrhs; ++j) {
         std::vector<double> b = rhs_unit(s, j);
         GmresResult g = gmres(op, b.data(), &pc, {o->tol, (size_t)o->restart, (size_t)o->max_restarts});
         accumulate_c(s, g.x, j, ncond, C);

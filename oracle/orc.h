@@ -77,6 +77,7 @@ typedef struct {
     int32_t order, max_level, restart, max_restarts;
     double tol;
     int32_t threads;          /* 0 = OpenMP default */
+    int32_t rhs_limit;        /* > 0: solve only the first rhs_limit conductors */
 } orc_fmm_opts;
 typedef struct {
     int64_t total_iterations;

@@ -79,11 +79,13 @@ def _wilton_mp(vq, p, dps=50):
 
 
 def test_wilton_matrix_matches_oracle(ctx, orc):
-    """Entry-wise Wilton block vs the oracle.  The FP64 closed form itself
-    loses up to ~1e-10 relative on far coplanar pairs (both implementations,
-    measured against a 50-digit evaluation), so the entry bar is 1e-8; the
-    second check pins the GPU to be as close to the 50-digit value as the
-    oracle on the worst entries."""
+    """Entry-wise Wilton block vs the oracle.  The reference's FP64 form of
+    the closed form loses up to ~1e-9 relative on far pairs (its log of a
+    ratio near 1), which the oracle reproduces, so the entry bar against the
+    oracle is 1e-8.  The GPU evaluates an algebraically identical
+    cancellation-free form; on the entries where the two differ most, the
+    GPU value must be within 1e-13 of a 50-digit evaluation and never
+    further from it than the oracle."""
     p = two_wire_panels()
     v, c = orc.icosphere([1e-6, 0.2e-6, 2e-6], 0.3e-6, 1, 0)
     verts = np.vstack([p["verts"], v])
@@ -92,7 +94,7 @@ def test_wilton_matrix_matches_oracle(ctx, orc):
     ref = orc.dense_P(verts)
     err = np.abs(got - ref) / np.abs(ref)
     assert err.max() < 1e-8, err.max()
-    assert np.median(err) < 1e-14
+    assert np.median(err) < 1e-12
     coef = 1.0 / (4.0 * math.pi * 8.854187812800e-12)
     worst = np.argsort(err.ravel())[::-1][:6]
     for k in worst:
@@ -100,7 +102,7 @@ def test_wilton_matrix_matches_oracle(ctx, orc):
         exact = coef * _wilton_mp(verts[j], cent[i])
         e_gpu = abs(got[i, j] - exact) / exact
         e_orc = abs(ref[i, j] - exact) / exact
-        assert e_gpu <= 3.0 * e_orc + 1e-14, (i, j, e_gpu, e_orc)
+        assert e_gpu <= 1e-13 and e_gpu <= e_orc + 1e-15, (i, j, e_gpu, e_orc)
 
 
 @pytest.mark.parametrize("nrhs", [1, 5])
