@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--side", type=float, default=40.0, help="window side in um")
     ap.add_argument("--restart", type=int, default=200, help="GMRES restart length")
     ap.add_argument("--far-quad", type=int, default=0, help="0 centroid lumping (reference), 1 Gauss points")
+    ap.add_argument("--precond", type=int, default=0, help="0 diagonal Jacobi (reference), 1 leaf block-Jacobi")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     return ap.parse_args()
@@ -198,8 +199,8 @@ def main():
 
     ctx = _lib.Context(local)
     prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
-    solve_kw = dict(order=args.order, max_level=args.depth, precision=prec, solve_ground_rhs=0, tol=1e-8,
-                    restart=args.restart, far_quad=args.far_quad)
+    solve_kw = dict(order=args.order, max_level=args.depth, precision=prec, skip_ground_rhs=1, tol=1e-8,
+                    restart=args.restart, far_quad=args.far_quad, precond=args.precond)
 
     lay = workload(rank, args.nets, args.side)
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
@@ -250,7 +251,7 @@ def main():
         res = pex.run_pex_by_net_checked(lay.store, lay.deck, lay.net_of_poly, ctx=ctx, report=e2e_rep,
                                          mesh_max_edge_m=EDGE_M, max_panels=-1, order=args.order,
                                          max_level=args.depth, precision=prec, restart=args.restart,
-                                         far_quad=args.far_quad)
+                                         far_quad=args.far_quad, precond=args.precond)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     if dist:
@@ -292,7 +293,7 @@ def main():
             "config": {"workload": f"routing window {args.nets} nets {args.side:g}x{args.side:g}um 3 layers, 0.25um "
                                    f"panels, {N} panels, {R} RHS, GMRES tol 1e-8",
                        "panels": N, "rhs": R, "precision": args.precision, "order": args.order, "depth": args.depth,
-                       "far_quad": args.far_quad, "restart": args.restart,
+                       "far_quad": args.far_quad, "restart": args.restart, "precond": args.precond,
                        "parallelism": f"replicas x{world}", "l2": "working set (Krylov basis ~7 GB) >> L2"},
             "panel_rhs_per_s": world * N * R / (ms_step * 1e-3),
             "iterations": last["iterations"], "max_rel_residual": last["max_rel_residual"],

@@ -230,7 +230,7 @@ gpx_status gpx_extract_quasistatic(gpx_ctx* ctx, const gpx_geometry_store* store
             Opts o = normalize(opts);
             // The per-net result needs only the nets' diagonal entries: the
             // substrate right-hand side is skipped unless asked for.
-            if (!opts) o.solve_ground_rhs = 0;
+            if (!opts) o.skip_ground_rhs = 1;
             *n_out = 0;
             PanelizeResult pr;
             const double t0 =
@@ -352,7 +352,7 @@ gpx_status gpx_plan_check(int64_t n_panels, const double* verts, int32_t order, 
                 bad("children");
         // every ordered leaf pair is covered exactly once by near blocks or by
         // an M2L pair of some ancestor pair (checked by panel-pair counting)
-        int64_t near_pairs = p.nnz();
+        int64_t near_pairs = p.near_pairs();
         int64_t covered_far = 0;
         std::vector<int64_t> cnt(nb, 0);
         for (int64_t k = 0; k < nl; ++k) cnt[p.lvl_off[p.L] + k] = p.leaf_begin[k + 1] - p.leaf_begin[k];

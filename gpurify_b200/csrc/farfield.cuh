@@ -1,0 +1,39 @@
+// Far-field (Chebyshev FMM) launch interface shared by the FP64 and FP32 paths.
+#pragma once
+#include <functional>
+
+#include "kernels.cuh"
+
+namespace gpx {
+
+// Runs the M2L translations of one level: (level, first box, box count, 1/half).
+template <class T>
+using M2LLevelFn = std::function<void(int, int, int, double)>;
+
+// Y += coef * far-field potential of X (N x R, type T), expansions E and L of
+// type T (nbox x Rb x n3 each with Rb >= R rows per box, zeroed here), M2L
+// supplied per level.
+template <class T>
+void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, double* Y, int R, int Rb, T* E,
+                      T* L, double coef, const M2LLevelFn<T>& m2l);
+
+// FP64 M2L of one level with CUDA-core FMAs.
+void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale);
+
+// Tensor-core (tcgen05, TF32 inputs, FP32 accumulation) M2L work list of one
+// level: pairs of target boxes sharing one offset loop.
+struct TcLevel {
+    int nitems = 0;
+    const int32_t* item_t = nullptr;    // 2 per item: target boxes (second may be -1)
+    const int32_t* item_off = nullptr;  // nitems + 1: entry ranges
+    const int32_t* slot = nullptr;      // per entry: operator slot
+    const int32_t* srcA = nullptr;      // per entry: source box of the first target or -1
+    const int32_t* srcB = nullptr;      // per entry: source box of the second target or -1
+};
+// L[t][r][m] = scale * sum K[m][l] E[s][r][l] for order-4 expansions (64
+// nodes), R a multiple of 64.  err receives a nonzero code if a bounded wait
+// on the tensor-core pipeline expired.
+void launch_m2l_tc(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale,
+                   int* err);
+
+}  // namespace gpx

@@ -7,6 +7,8 @@
 //  * near-field apply: dense leaf blocks times R right-hand sides, source
 //    columns of X staged in shared memory, block rows broadcast by shuffle;
 //  * far field: Chebyshev P2M, M2M, M2L, L2L, L2P (fmm/bbfmm.rs:209-448).
+#include <algorithm>
+
 #include "gpx_common.h"
 #include "kernels.cuh"
 
@@ -112,14 +114,15 @@ __device__ __forceinline__ double wilton(const SrcPanel& s, double px, double py
 constexpr int kAsmThreads = 256;
 constexpr int kAsmTile = 64;
 
-// One CTA per work item (target leaf, <= 128 rows): rows of the leaf's
+// One CTA per work item (target leaf, <= 64 rows): rows of the leaf's
 // P block m_t x S_t, row-major.
 __global__ void __launch_bounds__(kAsmThreads) k_near_assemble(DevPlan p, double* __restrict__ P, double coef) {
     const int t = p.item_leaf[blockIdx.x];
     const int r0 = p.item_row0[blockIdx.x];
     const int64_t tb = p.leaf_begin[t];
-    const int m = min((int)(p.leaf_begin[t + 1] - tb), r0 + 128);
+    const int m = min((int)(p.leaf_begin[t + 1] - tb), r0 + 64);
     const int S = p.near_S[t];
+    const int Sp = (S + 3) & ~3;
     const int64_t off = p.nval_off[t];
     __shared__ int64_t s_beg[28];
     __shared__ int32_t s_pre[29];
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_near_assemble(DevPlan p, double
             prep_source(p.verts + 12 * s_gid[j], sp);
             for (int row = r0 + warp; row < m; row += nw) {
                 const double* c = p.cent + 3 * (tb + row);
-                P[off + (int64_t)row * S + base + j] = coef * wilton(sp, c[0], c[1], c[2]);
+                P[off + (int64_t)row * Sp + base + j] = coef * wilton(sp, c[0], c[1], c[2]);
             }
         }
         __syncthreads();
@@ -161,33 +164,58 @@ __global__ void k_diag_inv(DevPlan p, const double* __restrict__ P, double* __re
     const int t = blockIdx.x;
     const int64_t tb = p.leaf_begin[t];
     const int m = (int)(p.leaf_begin[t + 1] - tb);
-    const int S = p.near_S[t];
+    const int Sp = (p.near_S[t] + 3) & ~3;
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
-        double d = P[p.nval_off[t] + (int64_t)r * S + r];  // self leaf is the first source block
+        double d = P[p.nval_off[t] + (int64_t)r * Sp + r];  // self leaf is the first source block
         inv[tb + r] = fabs(d) > 1e-30 ? 1.0 / d : 1.0;
     }
 }
 
-// Near apply: CTA per target leaf, 8 warps; each lane owns columns lane and
-// lane+32 of a 64-wide RHS chunk, each warp owns rows warp + 8*i.
-constexpr int kNaRPW = 16;  // rows per warp per pass (128 rows per pass)
-__global__ void __launch_bounds__(256) k_near_apply(DevPlan p, const double* __restrict__ P,
-                                                     const double* __restrict__ X, double* __restrict__ Y, int R) {
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Near apply as a register-tiled GEMM per work item (target leaf, <= 64 rows)
+// and 64-wide chunk of right-hand sides:
+//     Y[rows][0:64] = P_t[rows][0:S] X[src(0:S)][0:64],
+// 64 threads, 8 x 8 outputs per thread (rows ty+8i, columns tx+8j: every
+// shared-memory read is a broadcast or conflict-free), the contraction
+// staged 32 source panels at a time with cp.async into a double buffer so the
+// next tile's loads overlap this tile's FMAs.  T = double (plain path) or
+// float (mixed path); rows of P are padded to a multiple of 4 entries and R
+// is a multiple of 4, so every 16-byte copy is aligned.
+template <class T>
+__global__ void __launch_bounds__(64) k_near_apply(DevPlan p, const T* __restrict__ P, const T* __restrict__ X,
+                                                   double* __restrict__ Y, int R) {
+    constexpr int V = 16 / sizeof(T);        // elements per 16-byte copy
+    constexpr int KC = 128 / sizeof(T);      // contraction chunk: 32 floats / 16 doubles
+    constexpr int PP = KC + V;               // Ps row pitch (16-byte multiple, conflict-free)
+    constexpr int XP = 64 + V;               // Xs row pitch
     const int t = p.item_leaf[blockIdx.x];
     const int r0 = p.item_row0[blockIdx.x];
-    const int64_t tb = p.leaf_begin[t];
-    const int m = min((int)(p.leaf_begin[t + 1] - tb), r0 + 8 * kNaRPW);
+    const int rc = blockIdx.y * 64;
+    const int64_t tb = p.leaf_begin[t] + r0;
+    const int m = min((int)(p.leaf_begin[t + 1] - p.leaf_begin[t]) - r0, 64);
     const int S = p.near_S[t];
-    const int64_t off = p.nval_off[t];
+    const int Sp = (S + 3) & ~3;
+    const T* Pi = P + p.nval_off[t] + (int64_t)r0 * Sp;
     __shared__ int64_t s_beg[28];
     __shared__ int32_t s_pre[29];
-    __shared__ int64_t s_gid[32];
-    __shared__ double xs[32][65];
+    __shared__ int64_t s_gid[2][KC];
+    __shared__ __align__(16) T Ps[2][64][PP];  // [row][k]
+    __shared__ __align__(16) T Xs[2][KC][XP];  // [k][col]
+    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
     const int e0 = p.near_off[t], ne = p.near_off[t + 1] - e0;
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         int acc = 0;
         for (int e = 0; e < ne; ++e) {
-            int src = p.near_src[e0 + e];
+            const int src = p.near_src[e0 + e];
             s_beg[e] = p.leaf_begin[src];
             s_pre[e] = acc;
             acc += (int)(p.leaf_begin[src + 1] - p.leaf_begin[src]);
@@ -195,50 +223,75 @@ __global__ void __launch_bounds__(256) k_near_apply(DevPlan p, const double* __r
         s_pre[ne] = acc;
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int rc = 0; rc < R; rc += 64) {
-        for (int rb = r0; rb < m; rb += 8 * kNaRPW) {
-            double acc0[kNaRPW], acc1[kNaRPW];
-#pragma unroll
-            for (int i = 0; i < kNaRPW; ++i) acc0[i] = acc1[i] = 0.0;
-            for (int sb = 0; sb < S; sb += 32) {
-                const int cnt = min(32, S - sb);
-                __syncthreads();
-                if (threadIdx.x < cnt) {
-                    int s = sb + threadIdx.x, e = 0;
-                    while (s_pre[e + 1] <= s) ++e;
-                    s_gid[threadIdx.x] = s_beg[e] + (s - s_pre[e]);
-                }
-                __syncthreads();
-                for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
-                    int j = idx >> 6, c = idx & 63;
-                    xs[j][c] = (j < cnt && rc + c < R) ? X[s_gid[j] * R + rc + c] : 0.0;
-                }
-                __syncthreads();
-                double pr[kNaRPW];
-#pragma unroll
-                for (int i = 0; i < kNaRPW; ++i) {
-                    int row = rb + warp + 8 * i;
-                    pr[i] = (row < m && lane < cnt) ? P[off + (int64_t)row * S + sb + lane] : 0.0;
-                }
-                for (int j = 0; j < cnt; ++j) {
-                    const double x0 = xs[j][lane], x1 = xs[j][lane + 32];
-#pragma unroll
-                    for (int i = 0; i < kNaRPW; ++i) {
-                        double pv = __shfl_sync(0xffffffffu, pr[i], j);
-                        acc0[i] += pv * x0;
-                        acc1[i] += pv * x1;
-                    }
-                }
+    const int nchunk = (Sp + KC - 1) / KC;
+    auto gather_ids = [&](int c) {
+        if (tid < KC) {
+            const int sidx = c * KC + tid;
+            int64_t g = 0;
+            if (sidx < S) {
+                int e = 0;
+                while (s_pre[e + 1] <= sidx) ++e;
+                g = s_beg[e] + (sidx - s_pre[e]);
             }
+            s_gid[c & 1][tid] = g;
+        }
+    };
+    auto issue = [&](int c) {
+        const int k0 = c * KC, buf = c & 1;
 #pragma unroll
-            for (int i = 0; i < kNaRPW; ++i) {
-                int row = rb + warp + 8 * i;
-                if (row < m) {
-                    if (rc + lane < R) Y[(tb + row) * R + rc + lane] = acc0[i];
-                    if (rc + lane + 32 < R) Y[(tb + row) * R + rc + lane + 32] = acc1[i];
-                }
-            }
+        for (int q = 0; q < KC / V; ++q) {  // P tile: 64 rows x KC
+            const int id = tid + 64 * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
+            const bool ok = row < m && k0 + kc < Sp;
+            cp_async16(&Ps[buf][row][kc], ok ? (const void*)(Pi + (int64_t)row * Sp + k0 + kc) : (const void*)P, ok);
+        }
+#pragma unroll
+        for (int q = 0; q < KC / V; ++q) {  // X tile: KC x 64 columns
+            const int id = tid + 64 * q, kk = id / (64 / V), cc = (id % (64 / V)) * V;
+            const bool ok = k0 + kk < S && rc + cc < R;
+            cp_async16(&Xs[buf][kk][cc], ok ? (const void*)(X + s_gid[buf][kk] * R + rc + cc) : (const void*)X, ok);
+        }
+        cp_async_commit();
+    };
+    T acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = (T)0;
+    gather_ids(0);
+    __syncthreads();
+    issue(0);
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) gather_ids(c + 1);
+        __syncthreads();
+        if (c + 1 < nchunk) {
+            issue(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int buf = c & 1;
+#pragma unroll 4
+        for (int kk = 0; kk < KC; ++kk) {
+            T a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = Ps[buf][ty + 8 * i][kk];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Xs[buf][kk][tx + 8 * j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int row = ty + 8 * i;
+        if (row >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int col = rc + tx + 8 * j;
+            if (col < R) Y[(tb + row) * R + col] = (double)acc[i][j];
         }
     }
 }
@@ -321,155 +374,6 @@ __global__ void k_src_weights(DevPlan p, int quad, double* __restrict__ W) {
     }
 }
 
-// P2M: M[leafbox][m][r] = sum_j W_j[m] * area_j * X[j][r]; one thread per (m, r).
-__global__ void k_p2m(DevPlan p, const double* __restrict__ X, double* __restrict__ M, int R) {
-    const int t = blockIdx.x;
-    const int o = blockIdx.y * blockDim.x + threadIdx.x;
-    const int n3 = p.n3;
-    if (o >= n3 * R) return;
-    const int mi = o / R, r = o % R;
-    double acc = 0.0;
-    for (int64_t j = p.leaf_begin[t]; j < p.leaf_begin[t + 1]; ++j)
-        acc += p.wsrc[j * n3 + mi] * (p.area[j] * X[j * R + r]);
-    M[((int64_t)(p.leaf_box0 + t) * n3 + mi) * R + r] = acc;
-}
-
-// M2M into parents of level `lvl` boxes: one thread per (parent, m', r);
-// parent boxes of level lvl-1 are [pb0, pb1), children are contiguous after
-// the Morton sort so each parent scans the child range given by c_first/c_count.
-__global__ void k_m2m(DevPlan p, int cb0, int cb1, const int32_t* __restrict__ child_first,
-                      const int32_t* __restrict__ child_count, int pb0, double* __restrict__ M, int R) {
-    const int pb = pb0 + blockIdx.x;
-    const int o = blockIdx.y * blockDim.x + threadIdx.x;
-    const int n = p.n, n3 = p.n3;
-    if (o >= n3 * R) return;
-    const int mi = o / R, r = o % R;
-    const int ap = mi / (n * n), bp = (mi / n) % n, cp = mi % n;
-    double acc = 0.0;
-    const int cf = child_first[pb], cc = child_count[pb];
-    for (int ch = cf; ch < cf + cc; ++ch) {
-        const int oc = p.box_octant[ch];
-        const double* mx = p.m2m1d + (oc * 3 + 0) * n * n;
-        const double* my = p.m2m1d + (oc * 3 + 1) * n * n;
-        const double* mz = p.m2m1d + (oc * 3 + 2) * n * n;
-        const double* src = M + (int64_t)ch * n3 * R + r;
-        for (int a = 0; a < n; ++a) {
-            double sa = 0.0;
-            for (int b = 0; b < n; ++b) {
-                double sb = 0.0;
-                for (int c = 0; c < n; ++c) sb += mz[cp * n + c] * src[((a * n + b) * n + c) * R];
-                sa += my[bp * n + b] * sb;
-            }
-            acc += mx[ap * n + a] * sa;
-        }
-    }
-    M[((int64_t)pb * n3 + mi) * R + r] += acc;
-    (void)cb0;
-    (void)cb1;
-}
-
-// M2L at one level: CTA per target box, 64 x 64 output tile of (m, r) with a
-// 4 x 4 register tile per thread; operator and source multipole tiles of 32
-// along the contraction staged in shared memory.
-__global__ void __launch_bounds__(256) k_m2l(DevPlan p, int b0, double* __restrict__ Lc,
-                                             const double* __restrict__ M, int R, double scale) {
-    const int tb = b0 + blockIdx.x;
-    const int n3 = p.n3;
-    __shared__ double Ks[32][65];   // [l][m]
-    __shared__ double Ms[32][65];   // [l][r]
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // r-group, m-group
-    const int64_t s0 = p.m2l_off[tb], s1 = p.m2l_off[tb + 1];
-    if (s0 == s1) return;
-    for (int mc = 0; mc < n3; mc += 64) {
-        for (int rcn = 0; rcn < R; rcn += 64) {
-            double acc[4][4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-            for (int64_t e = s0; e < s1; ++e) {
-                const int src = p.m2l_src[e];
-                const double* K = p.m2l_K + (int64_t)p.m2l_slot[e] * n3 * n3;
-                const double* Msrc = M + (int64_t)src * n3 * R;
-                for (int lc = 0; lc < n3; lc += 32) {
-                    __syncthreads();
-                    for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
-                        const int a = idx >> 5, b = idx & 31;  // K row m = mc+a, col l = lc+b
-                        Ks[b][a] = (mc + a < n3 && lc + b < n3) ? K[(int64_t)(mc + a) * n3 + lc + b] : 0.0;
-                        const int l = idx >> 6, c = idx & 63;  // M row l = lc+l, col r = rcn+c
-                        Ms[l][c] = (lc + l < n3 && rcn + c < R) ? Msrc[(int64_t)(lc + l) * R + rcn + c] : 0.0;
-                    }
-                    __syncthreads();
-#pragma unroll 4
-                    for (int l = 0; l < 32; ++l) {
-                        double kv[4], mv[4];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) kv[i] = Ks[l][ty + 16 * i];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) mv[j] = Ms[l][tx + 16 * j];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i)
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) acc[i][j] += kv[i] * mv[j];
-                    }
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    int mm = mc + ty + 16 * i, rr = rcn + tx + 16 * j;
-                    if (mm < n3 && rr < R) Lc[((int64_t)tb * n3 + mm) * R + rr] += scale * acc[i][j];
-                }
-        }
-    }
-}
-
-// L2L to children of level lvl boxes: one thread per (child, m, r).
-__global__ void k_l2l(DevPlan p, int cb0, double* __restrict__ Lc, int R) {
-    const int cb = cb0 + blockIdx.x;
-    const int o = blockIdx.y * blockDim.x + threadIdx.x;
-    const int n = p.n, n3 = p.n3;
-    if (o >= n3 * R) return;
-    const int mi = o / R, r = o % R;
-    const int a = mi / (n * n), b = (mi / n) % n, c = mi % n;
-    const int pb = p.box_parent[cb], oc = p.box_octant[cb];
-    const double* mx = p.m2m1d + (oc * 3 + 0) * n * n;
-    const double* my = p.m2m1d + (oc * 3 + 1) * n * n;
-    const double* mz = p.m2m1d + (oc * 3 + 2) * n * n;
-    const double* src = Lc + (int64_t)pb * n3 * R + r;
-    double acc = 0.0;
-    for (int ap = 0; ap < n; ++ap) {
-        double sa = 0.0;
-        for (int bp = 0; bp < n; ++bp) {
-            double sb = 0.0;
-            for (int cp = 0; cp < n; ++cp) sb += mz[cp * n + c] * src[((ap * n + bp) * n + cp) * R];
-            sa += my[bp * n + b] * sb;
-        }
-        acc += mx[ap * n + a] * sa;
-    }
-    Lc[((int64_t)cb * n3 + mi) * R + r] += acc;
-}
-
-// L2P: Y[j][r] += coef * sum_m W_j[m] L[leafbox][m][r]; one thread per (j, r).
-__global__ void k_l2p(DevPlan p, const double* __restrict__ Lc, double* __restrict__ Y, int R, double coef,
-                      const int32_t* __restrict__ leaf_of) {
-    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= p.N * R) return;
-    const int64_t j = o / R;
-    const int r = (int)(o % R);
-    const int n = p.n, n3 = p.n3;
-    const double* w = p.w1d + j * 3 * n;
-    const double* L = Lc + (int64_t)(p.leaf_box0 + leaf_of[j]) * n3 * R + r;
-    double acc = 0.0;
-    for (int a = 0; a < n; ++a)
-        for (int b = 0; b < n; ++b) {
-            const double wab = w[a] * w[n + b];
-            for (int c = 0; c < n; ++c) acc += (wab * w[2 * n + c]) * L[((a * n + b) * n + c) * R];
-        }
-    Y[o] += coef * acc;
-}
-
 __global__ void k_potential_matrix(const double* __restrict__ sv, int64_t ns, const double* __restrict__ pts,
                                    int64_t nt, double* __restrict__ out, double coef) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -502,57 +406,30 @@ void launch_diag_inv(Ctx& c, const DevPlan& p, const double* P, double* inv) {
 void launch_near_apply(Ctx& c, const DevPlan& p, int64_t nnz, const double* P, const double* X, double* Y, int R) {
     if (p.nleaf == 0) return;
     KTimer t(c, K_NEAR_APPLY, 8.0 * nnz + 16.0 * (double)p.N * R, 2.0 * (double)nnz * R);
-    k_near_apply<<<p.nitems, 256, 0, c.stream>>>(p, P, X, Y, R);
+    k_near_apply<double><<<dim3(p.nitems, (R + 63) / 64), 64, 0, c.stream>>>(p, P, X, Y, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
 
-void launch_far_apply(Ctx& c, const DevPlan& p, const FarLaunch& f, const double* X, double* Y, int R, double* M,
-                      double* Lc, double coef) {
-    cudaStream_t s = c.stream;
-    const int n = p.n, n3 = p.n3, L = p.L;
-    const double box_bytes = 8.0 * n3 * R;
-    GPX_CUDA(cudaMemsetAsync(M, 0, (size_t)p.nbox * n3 * R * sizeof(double), s));
-    GPX_CUDA(cudaMemsetAsync(Lc, 0, (size_t)p.nbox * n3 * R * sizeof(double), s));
-    const unsigned oc = (unsigned)((n3 * R + 255) / 256);
-    {
-        KTimer t(c, K_P2M, (double)p.N * (8.0 * R + 24.0 * n + 8.0) + p.nleaf * box_bytes, 2.0 * (double)p.N * n3 * R);
-        k_p2m<<<dim3(p.nleaf, oc), 256, 0, s>>>(p, X, M, R);
-        GPX_LAUNCH_CHECK();
-        c.launches += 1;
-    }
-    for (int l = L; l >= 3; --l) {  // children at level l -> parents at level l-1
-        const int pb0 = f.lvl_off[l - 1], npb = f.lvl_off[l] - pb0, nch = f.lvl_off[l + 1] - f.lvl_off[l];
-        if (npb == 0) continue;
-        KTimer t(c, K_M2M, (double)(npb + nch) * box_bytes, 2.0 * 3.0 * n * n3 * R * (double)nch);
-        k_m2m<<<dim3(npb, oc), 256, 0, s>>>(p, f.lvl_off[l], f.lvl_off[l + 1], f.child_first, f.child_count, pb0, M, R);
-        GPX_LAUNCH_CHECK();
-        c.launches += 1;
-    }
-    for (int l = 2; l <= L; ++l) {
-        const int b0 = f.lvl_off[l], nb = f.lvl_off[l + 1] - b0;
-        if (nb == 0) continue;
-        const double pairs = (double)(f.m2l_off[b0 + nb] - f.m2l_off[b0]);
-        if (pairs == 0) continue;
-        KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)n3 * n3 * R * pairs);
-        k_m2l<<<nb, 256, 0, s>>>(p, b0, Lc, M, R, 1.0 / f.lvl_half[l]);
-        GPX_LAUNCH_CHECK();
-        c.launches += 1;
-    }
-    for (int l = 2; l < L; ++l) {  // parents at level l -> children at level l+1
-        const int cb0 = f.lvl_off[l + 1], ncb = f.lvl_off[l + 2] - cb0, npb = f.lvl_off[l + 1] - f.lvl_off[l];
-        if (ncb == 0) continue;
-        KTimer t(c, K_L2L, (double)(npb + 2 * ncb) * box_bytes, 2.0 * 3.0 * n * n3 * R * (double)ncb);
-        k_l2l<<<dim3(ncb, oc), 256, 0, s>>>(p, cb0, Lc, R);
-        GPX_LAUNCH_CHECK();
-        c.launches += 1;
-    }
-    {
-        KTimer t(c, K_L2P, (double)p.N * (16.0 * R + 24.0 * n) + p.nleaf * box_bytes, 2.0 * (double)p.N * n3 * R);
-        k_l2p<<<(unsigned)((p.N * R + 255) / 256), 256, 0, s>>>(p, Lc, Y, R, coef, f.leaf_of);
-        GPX_LAUNCH_CHECK();
-        c.launches += 1;
-    }
+void launch_near_apply32(Ctx& c, const DevPlan& p, int64_t nnz, const float* P, const float* X, double* Y, int R) {
+    if (p.nleaf == 0) return;
+    KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 12.0 * (double)p.N * R, 2.0 * (double)nnz * R);
+    k_near_apply<float><<<dim3(p.nitems, (R + 63) / 64), 64, 0, c.stream>>>(p, P, X, Y, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+void launch_to_f32(Ctx& c, const double* a, float* b, int64_t n) {
+    if (n == 0) return;
+    KTimer t(c, K_VEC, 12.0 * n, 0.0);
+    k_to_f32<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, c.stream>>>(a, b, n);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
 }
 
 void launch_src_weights(Ctx& c, const DevPlan& p, int quad, double* W) {

@@ -23,7 +23,7 @@ struct DevPlan {
     const int32_t* near_src;
     const int32_t* near_S;
     const int64_t* nval_off;
-    const int32_t* item_leaf;  // near-field work items (leaf, first row), <= 128 rows each
+    const int32_t* item_leaf;  // near-field work items (leaf, first row), <= 64 rows each
     const int32_t* item_row0;
     const int32_t* box_parent;
     const int32_t* box_octant;
@@ -54,10 +54,11 @@ struct FarLaunch {
     const int32_t* leaf_of;      // device, per sorted panel
     const int64_t* m2l_off;      // host, per box (pair counts per level)
 };
-// Far field, added to Y: P2M, M2M, M2L, L2L, L2P (bbfmm.rs:209-448), scaled by
-// coef; M and Lc are nbox x n3 x R scratch.
-void launch_far_apply(Ctx& c, const DevPlan& p, const FarLaunch& f, const double* X, double* Y, int R, double* M,
-                      double* Lc, double coef);
+// Y = P_near X with an FP32 copy of P, FP32 input and arithmetic (Y is FP64).
+// R must be a multiple of 4 (16-byte aligned rows).
+void launch_near_apply32(Ctx& c, const DevPlan& p, int64_t nnz, const float* P, const float* X, double* Y, int R);
+// b = (float) a
+void launch_to_f32(Ctx& c, const double* a, float* b, int64_t n);
 // Far-field source weights W[j][m]: the Chebyshev interpolation weights of
 // panel j's charge in its leaf; quad 0: at the centroid (the reference's
 // point lumping), quad 1: averaged over 2x2 Gauss points of the panel.

@@ -74,12 +74,24 @@ __global__ void k_sqrt(double* v, int n) {
     if (i < n) v[i] = sqrt(v[i]);
 }
 
-// Z[n][r] = inv_diag[n] * V[n][r]
+// Z[n][r] (+)= inv_diag[n] * V[n][r]
 __global__ void k_diag_scale(const double* __restrict__ V, const double* __restrict__ d, double* __restrict__ Z,
-                             int64_t N, int R) {
+                             int64_t N, int R, int add) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
-    Z[o] = V[o] * d[o / R];
+    const double z = V[o] * d[o / R];
+    Z[o] = add ? Z[o] + z : z;
+}
+
+// out[n][r] = sum_i y[i][r] V_i[n][r]
+__global__ void k_lincomb(const double* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ y,
+                          double* __restrict__ out, int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= N * R) return;
+    const int r = (int)(o % R);
+    double s = 0.0;
+    for (int i = 0; i < ni; ++i) s += y[i * R + r] * V[i * strideV + o];
+    out[o] = s;
 }
 
 // Res[n][r] = b[n][r] - AX[n][r], b the unit-conductor right-hand side
@@ -90,6 +102,21 @@ __global__ void k_residual(const int32_t* __restrict__ cond, const int32_t* __re
     if (o >= N * R) return;
     const double b = cond[o / R] == rhs_cond[o % R] ? 1.0 : 0.0;
     Res[o] = AX ? b - AX[o] : b;
+}
+
+// Res = B - AX; X += D; zero the columns of V whose mask is set.
+__global__ void k_sub(const double* __restrict__ B, const double* __restrict__ AX, double* __restrict__ Res,
+                      int64_t n) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o < n) Res[o] = B[o] - AX[o];
+}
+__global__ void k_add(double* __restrict__ X, const double* __restrict__ D, int64_t n) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o < n) X[o] += D[o];
+}
+__global__ void k_zero_cols(double* __restrict__ V, const int32_t* __restrict__ mask, int64_t N, int R) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o < N * R && mask[o % R]) V[o] = 0.0;
 }
 
 // Per-column Hessenberg column k update, Givens rotation (krylov.rs:118-142,
@@ -245,9 +272,17 @@ void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thres
     c.launches += 1;
 }
 
-void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R) {
+void launch_lincomb(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, double* out, int64_t N,
+                    int R) {
+    KTimer t(c, K_VEC, 8.0 * (ni + 1) * (double)N * R, 2.0 * ni * (double)N * R);
+    k_lincomb<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, y, out, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add) {
     KTimer t(c, K_VEC, 16.0 * (double)N * R + 8.0 * N, (double)N * R);
-    k_diag_scale<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, d, Z, N, R);
+    k_diag_scale<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, d, Z, N, R, add ? 1 : 0);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
@@ -256,6 +291,27 @@ void launch_residual(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const
                      int R) {
     KTimer t(c, K_VEC, (AX ? 16.0 : 8.0) * (double)N * R + 4.0 * N, (double)N * R);
     k_residual<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(cond, rhs_cond, AX, Res, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_sub(Ctx& c, const double* B, const double* AX, double* Res, int64_t n) {
+    KTimer t(c, K_VEC, 24.0 * n, (double)n);
+    k_sub<<<blocks_for(n, 256), 256, 0, c.stream>>>(B, AX, Res, n);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_add(Ctx& c, double* X, const double* D, int64_t n) {
+    KTimer t(c, K_VEC, 24.0 * n, (double)n);
+    k_add<<<blocks_for(n, 256), 256, 0, c.stream>>>(X, D, n);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_zero_cols(Ctx& c, double* V, const int32_t* mask, int64_t N, int R) {
+    KTimer t(c, K_VEC, 8.0 * N * R, 0.0);
+    k_zero_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, mask, N, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }

@@ -35,9 +35,14 @@ void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const dou
 void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, int nblk, double* out);
 void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R);
 void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R);
-void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R);
+void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add = false);
+void launch_lincomb(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, double* out, int64_t N,
+                    int R);
 void launch_residual(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const double* AX, double* Res, int64_t N,
                      int R);
+void launch_sub(Ctx& c, const double* B, const double* AX, double* Res, int64_t n);
+void launch_add(Ctx& c, double* X, const double* D, int64_t n);
+void launch_zero_cols(Ctx& c, double* V, const int32_t* mask, int64_t N, int R);
 void launch_givens(Ctx& c, const GmresDev& g, int k);
 void launch_trisolve(Ctx& c, const GmresDev& g);
 void launch_combine(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, const double* d, double* X,

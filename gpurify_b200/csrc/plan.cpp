@@ -359,7 +359,8 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
             S += p.leaf_begin[p.near_src[e] + 1] - p.leaf_begin[p.near_src[e]];
         p.near_S[k] = (int32_t)S;
         p.max_S = std::max<int32_t>(p.max_S, (int32_t)S);
-        p.nval_off[k + 1] = p.nval_off[k] + (p.leaf_begin[k + 1] - p.leaf_begin[k]) * S;
+        // rows are stored with a stride padded to 4 entries (16-byte aligned rows)
+        p.nval_off[k + 1] = p.nval_off[k] + (p.leaf_begin[k + 1] - p.leaf_begin[k]) * ((S + 3) & ~int64_t(3));
     }
     p.item_leaf.clear();
     p.item_row0.clear();

@@ -44,10 +44,10 @@ struct Plan {
     std::vector<int32_t> near_off;    // nleaf+1
     std::vector<int32_t> near_src;    // leaf indices
     std::vector<int32_t> near_S;      // total source panels per target leaf
-    std::vector<int64_t> nval_off;    // nleaf+1: value offset of each leaf's m_t x S_t block
+    std::vector<int64_t> nval_off;    // nleaf+1: value offset of each leaf's m_t x Sp_t block (Sp = S rounded up to 4)
     int32_t max_S = 0;
     // Near-field work items: (target leaf, first row), at most kRowsPerItem rows each.
-    static constexpr int kRowsPerItem = 128;
+    static constexpr int kRowsPerItem = 64;
     std::vector<int32_t> item_leaf, item_row0;
 
     // M2L: per target box (global box index), sources + operator slot.
@@ -61,7 +61,12 @@ struct Plan {
 
     int64_t nleaf() const { return (int64_t)leaf_begin.size() - 1; }
     int64_t nbox() const { return (int64_t)lvl_off.back(); }
-    int64_t nnz() const { return nval_off.empty() ? 0 : nval_off.back(); }
+    int64_t nnz() const { return nval_off.empty() ? 0 : nval_off.back(); }  // stored entries (incl. row padding)
+    int64_t near_pairs() const {
+        int64_t s = 0;
+        for (size_t k = 0; k + 1 < leaf_begin.size(); ++k) s += (leaf_begin[k + 1] - leaf_begin[k]) * near_S[k];
+        return s;
+    }
     int64_t m2l_pairs() const { return m2l_off.empty() ? 0 : m2l_off.back(); }
 };
 

@@ -1,0 +1,155 @@
+// Leaf block-Jacobi preconditioner.  Blocks are runs of up to 48
+// consecutive panels inside one leaf; each block's matrix is the exact
+// (Wilton) self-interaction sub-block of the near field, inverted once by
+// Gauss-Jordan elimination with partial pivoting in FP64 and applied as a
+// small dense product per block.  The reference uses the diagonal of the same
+// near-field block (cap/fmm_solver.rs:133-162); both right preconditioners
+// leave the solution of P sigma = b unchanged.
+#include <algorithm>
+#include <vector>
+
+#include "precond.cuh"
+
+namespace gpx {
+
+namespace {
+
+constexpr int kB = 48;
+
+// One CTA per block: invert A (b x b) read from the leaf's near block.
+__global__ void __launch_bounds__(256) k_block_invert(DevPlan p, const double* __restrict__ P,
+                                                      const int32_t* __restrict__ blk_leaf,
+                                                      const int32_t* __restrict__ blk_row0,
+                                                      const int32_t* __restrict__ blk_size,
+                                                      double* __restrict__ Minv, int* __restrict__ singular) {
+    const int bi = blockIdx.x;
+    const int t = blk_leaf[bi], r0 = blk_row0[bi], b = blk_size[bi];
+    const int Sp = (p.near_S[t] + 3) & ~3;
+    const double* Pt = P + p.nval_off[t];
+    __shared__ double A[kB][kB + 1], I[kB][kB + 1];
+    __shared__ int piv;
+    __shared__ double pval;
+    for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) {
+        const int i = e / kB, j = e % kB;
+        A[i][j] = (i < b && j < b) ? Pt[(int64_t)(r0 + i) * Sp + r0 + j] : (i == j ? 1.0 : 0.0);
+        I[i][j] = i == j ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < b; ++k) {
+        if (threadIdx.x == 0) {
+            int best = k;
+            double mx = fabs(A[k][k]);
+            for (int i = k + 1; i < b; ++i)
+                if (fabs(A[i][k]) > mx) {
+                    mx = fabs(A[i][k]);
+                    best = i;
+                }
+            piv = best;
+            pval = A[best][k];
+            if (mx == 0.0) atomicExch(singular, 1);
+        }
+        __syncthreads();
+        if (piv != k)
+            for (int j = threadIdx.x; j < kB; j += blockDim.x) {
+                double a = A[k][j];
+                A[k][j] = A[piv][j];
+                A[piv][j] = a;
+                double c = I[k][j];
+                I[k][j] = I[piv][j];
+                I[piv][j] = c;
+            }
+        __syncthreads();
+        const double inv = pval != 0.0 ? 1.0 / pval : 0.0;
+        for (int j = threadIdx.x; j < kB; j += blockDim.x) {
+            A[k][j] *= inv;
+            I[k][j] *= inv;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) {
+            const int i = e / kB, j = e % kB;
+            if (i != k) {
+                const double f = A[i][k];
+                if (j != k) A[i][j] -= f * A[k][j];
+                I[i][j] -= f * I[k][j];
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kB; i += blockDim.x)
+            if (i != k) A[i][k] = 0.0;
+        __syncthreads();
+    }
+    double* out = Minv + (int64_t)bi * kB * kB;
+    for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) out[e] = I[e / kB][e % kB];
+}
+
+// One CTA per (block, 64-column chunk): Z[rows] = Minv V[rows].
+__global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ Minv,
+                                                     const int64_t* __restrict__ blk_start,
+                                                     const int32_t* __restrict__ blk_size, const double* __restrict__ V,
+                                                     double* __restrict__ Z, int R, int add) {
+    const int bi = blockIdx.x;
+    const int rc = blockIdx.y * 64;
+    const int64_t s0 = blk_start[bi];
+    const int b = blk_size[bi];
+    __shared__ double Ms[kB][kB + 1];
+    __shared__ double Vs[kB][65];
+    const double* M = Minv + (int64_t)bi * kB * kB;
+    for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) Ms[e / kB][e % kB] = M[e];
+    for (int e = threadIdx.x; e < kB * 64; e += blockDim.x) {
+        const int i = e >> 6, c = e & 63;
+        Vs[i][c] = (i < b && rc + c < R) ? V[(s0 + i) * R + rc + c] : 0.0;
+    }
+    __syncthreads();
+    const int c = threadIdx.x & 63, rg = threadIdx.x >> 6;  // 4 row groups
+    for (int i = rg; i < b; i += 4) {
+        if (rc + c >= R) break;
+        double acc = 0.0;
+        for (int k = 0; k < b; ++k) acc += Ms[i][k] * Vs[k][c];
+        double* z = Z + (s0 + i) * R + rc + c;
+        *z = add ? *z + acc : acc;
+    }
+}
+
+}  // namespace
+
+void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double* P) {
+    std::vector<int32_t> leaf, row0, size;
+    std::vector<int64_t> start;
+    for (int64_t k = 0; k + 1 < (int64_t)pl.leaf_begin.size(); ++k) {
+        const int64_t m = pl.leaf_begin[k + 1] - pl.leaf_begin[k];
+        for (int64_t r = 0; r < m; r += kB) {
+            leaf.push_back((int32_t)k);
+            row0.push_back((int32_t)r);
+            size.push_back((int32_t)std::min<int64_t>(kB, m - r));
+            start.push_back(pl.leaf_begin[k] + r);
+        }
+    }
+    nblk = (int)leaf.size();
+    d_leaf.upload(leaf, c.stream);
+    d_row0.upload(row0, c.stream);
+    d_size.upload(size, c.stream);
+    d_start.upload(start, c.stream);
+    Minv.alloc((size_t)nblk * kB * kB, c.stream);
+    d_sing.alloc(1, c.stream);
+    d_sing.zero();
+    {
+        KTimer t(c, K_SMALL, 8.0 * nblk * kB * kB * 2, 2.0 * nblk * (double)kB * kB * kB);
+        k_block_invert<<<nblk, 256, 0, c.stream>>>(dp, P, d_leaf.p, d_row0.p, d_size.p, Minv.p, d_sing.p);
+        GPX_LAUNCH_CHECK();
+        c.launches += 1;
+    }
+    int sing = 0;
+    d_sing.download(&sing, 1);
+    GPX_CUDA(cudaStreamSynchronize(c.stream));
+    if (sing) throw Error(GPX_ERR_CAPACITANCE, "singular near-field block in the block-Jacobi preconditioner");
+}
+
+void BlockJacobi::apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add) const {
+    KTimer t(c, K_VEC, 8.0 * (2.0 * N * R + (double)nblk * kB * kB), 2.0 * (double)N * kB * R);
+    k_block_apply<<<dim3(nblk, (R + 63) / 64), 256, 0, c.stream>>>(Minv.p, d_start.p, d_size.p, V, Z, R, add ? 1 : 0);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+    (void)N;
+}
+
+}  // namespace gpx

@@ -1,0 +1,20 @@
+// Right preconditioners of the GMRES iteration.
+#pragma once
+#include "kernels.cuh"
+#include "plan.h"
+
+namespace gpx {
+
+// Leaf block-Jacobi: blocks of up to 48 consecutive panels of one leaf,
+// inverted from the exact near-field self block.
+struct BlockJacobi {
+    int nblk = 0;
+    DBuf<int32_t> d_leaf, d_row0, d_size, d_sing;
+    DBuf<int64_t> d_start;
+    DBuf<double> Minv;
+    void build(Ctx& c, const Plan& pl, const DevPlan& dp, const double* P);
+    // Z = M^-1 V (or Z += M^-1 V), V and Z N x R row-major.
+    void apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add) const;
+};
+
+}  // namespace gpx

@@ -12,16 +12,21 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
+#include <functional>
 
+#include "farfield.cuh"
 #include "kernels.cuh"
 #include "krylov.cuh"
+#include "precond.cuh"
 #include "solver.h"
 
 namespace gpx {
 
 struct DevM2L {
     int n = 0, mode = 0;
-    DBuf<double> K;
+    DBuf<double> K;   // FP64 operators
+    DBuf<float> K32;  // the same, rounded to TF32 (round to nearest, ties away), for the tensor-core M2L
     std::vector<int32_t> rank;
 };
 
@@ -41,6 +46,16 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
     d->mode = mode;
     d->rank = host.rank;
     d->K.upload(host.K, ctx.stream);
+    std::vector<float> k32(host.K.size());
+    for (size_t i = 0; i < k32.size(); ++i) {
+        float f = (float)host.K[i];
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+        std::memcpy(&f, &u, 4);
+        k32[i] = f;
+    }
+    d->K32.upload(k32, ctx.stream);
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     ctx.m2l_cache.push_back(d);
     return d;
@@ -131,24 +146,100 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
     d.far.m2l_off = p.m2l_off.data();
 }
 
-// The precorrected potential operator of one plan for R right-hand sides.
+// Tensor-core M2L work lists of every level (pairs of target boxes of the
+// same octant class in Morton order sharing one offset loop).
+struct TcLists {
+    std::vector<TcLevel> level;  // per level (empty below 2)
+    DBuf<int32_t> item_t, item_off, slot, srcA, srcB;
+};
+
+void build_tc_lists(Ctx& ctx, const Plan& pl, TcLists& out) {
+    std::vector<int32_t> it, ioff, sl, sa, sb;
+    struct LevelRange {
+        size_t it0, off0;
+        int n;
+    };
+    std::vector<LevelRange> ranges(pl.L + 1, {0, 0, 0});
+    for (int l = 2; l <= pl.L; ++l) {
+        ranges[l].it0 = it.size() / 2;
+        ranges[l].off0 = ioff.size();
+        std::vector<int32_t> cls[8];
+        for (int32_t b = pl.lvl_off[l]; b < pl.lvl_off[l + 1]; ++b) {
+            if (pl.m2l_off[b + 1] == pl.m2l_off[b]) continue;
+            const int32_t* c = &pl.box_cell[3 * b];
+            cls[(c[0] & 1) | ((c[1] & 1) << 1) | ((c[2] & 1) << 2)].push_back(b);
+        }
+        int n = 0;
+        for (auto& v : cls)
+            for (size_t k = 0; k < v.size(); k += 2) {
+                const int32_t tA = v[k], tB = k + 1 < v.size() ? v[k + 1] : -1;
+                int32_t srcA[343], srcB[343];
+                std::fill(srcA, srcA + 343, -1);
+                std::fill(srcB, srcB + 343, -1);
+                for (int64_t e = pl.m2l_off[tA]; e < pl.m2l_off[tA + 1]; ++e) srcA[pl.m2l_slot[e]] = pl.m2l_src[e];
+                if (tB >= 0)
+                    for (int64_t e = pl.m2l_off[tB]; e < pl.m2l_off[tB + 1]; ++e) srcB[pl.m2l_slot[e]] = pl.m2l_src[e];
+                it.push_back(tA);
+                it.push_back(tB);
+                ioff.push_back((int32_t)sl.size());
+                for (int q = 0; q < 343; ++q)
+                    if (srcA[q] >= 0 || srcB[q] >= 0) {
+                        sl.push_back(q);
+                        sa.push_back(srcA[q]);
+                        sb.push_back(srcB[q]);
+                    }
+                ++n;
+            }
+        ranges[l].n = n;
+    }
+    ioff.push_back((int32_t)sl.size());
+    cudaStream_t s = ctx.stream;
+    out.item_t.upload(it, s);
+    out.item_off.upload(ioff, s);
+    out.slot.upload(sl, s);
+    out.srcA.upload(sa, s);
+    out.srcB.upload(sb, s);
+    out.level.assign(pl.L + 1, TcLevel());
+    for (int l = 2; l <= pl.L; ++l) {
+        TcLevel& v = out.level[l];
+        v.nitems = ranges[l].n;
+        v.item_t = out.item_t.p + 2 * ranges[l].it0;
+        v.item_off = out.item_off.p + ranges[l].off0;
+        v.slot = out.slot.p;
+        v.srcA = out.srcA.p;
+        v.srcB = out.srcB.p;
+    }
+}
+
+// The precorrected potential operator of one plan for R right-hand sides, in
+// FP64 (apply) and, for the mixed path, FP32 with tensor-core M2L (apply32).
 struct Operator {
     Ctx& ctx;
     const Plan& pl;
     DevPlanBufs& d;
     int R;
     int far_quad;
-    DBuf<double> P, inv_diag, M, Lc;
+    bool mixed;
+    const DevM2L* m2l;
+    DBuf<double> P, inv_diag, E64, L64;
+    DBuf<float> P32, E32, L32, X32;
+    DBuf<int32_t> tc_err;
+    TcLists tc;
+    int precond = 0;
+    BlockJacobi bj;
+    int Rb32 = 0;
     double t_assembly_s = 0.0;
-    int64_t applies = 0;
+    int64_t applies = 0, applies32 = 0;
 
-    Operator(Ctx& c, const Plan& p, DevPlanBufs& dd, int r, int fq) : ctx(c), pl(p), d(dd), R(r), far_quad(fq) {}
+    Operator(Ctx& c, const Plan& p, DevPlanBufs& dd, int r, int fq, bool mx, const DevM2L* m)
+        : ctx(c), pl(p), d(dd), R(r), far_quad(fq), mixed(mx), m2l(m) {}
 
     bool has_far() const { return pl.far && pl.m2l_pairs() > 0; }
 
     void assemble() {
         cudaStream_t s = ctx.stream;
         P.alloc((size_t)pl.nnz(), s);
+        P.zero();  // row padding stays zero
         inv_diag.alloc((size_t)pl.N, s);
         cudaEvent_t e0, e1;
         GPX_CUDA(cudaEventCreate(&e0));
@@ -157,6 +248,7 @@ struct Operator {
         launch_near_assemble(ctx, d.v, pl.nnz(), P.p, kCoulomb);
         GPX_CUDA(cudaEventRecord(e1, s));
         launch_diag_inv(ctx, d.v, P.p, inv_diag.p);
+        if (precond == 1) bj.build(ctx, pl, d.v, P.p);
         GPX_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         GPX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -164,19 +256,66 @@ struct Operator {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (has_far()) {
-            M.alloc((size_t)pl.nbox() * pl.n3 * R, s);
-            Lc.alloc((size_t)pl.nbox() * pl.n3 * R, s);
             d.wsrc.alloc((size_t)pl.N * pl.n3, s);
             launch_src_weights(ctx, d.v, far_quad, d.wsrc.p);
             d.v.wsrc = d.wsrc.p;
+            E64.alloc((size_t)pl.nbox() * pl.n3 * R, s);
+            L64.alloc((size_t)pl.nbox() * pl.n3 * R, s);
+        }
+        if (mixed) {
+            P32.alloc((size_t)pl.nnz(), s);
+            launch_to_f32(ctx, P.p, P32.p, pl.nnz());
+            X32.alloc((size_t)pl.N * R, s);
+            if (has_far()) {
+                Rb32 = (R + 63) / 64 * 64;
+                E32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
+                L32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
+                build_tc_lists(ctx, pl, tc);
+                tc_err.alloc(1, s);
+                tc_err.zero();
+            }
         }
     }
 
-    // Y = A X (X, Y: N x R, leaf-sorted panel order).
+    // Y = A X in FP64 (X, Y: N x R, leaf-sorted panel order).
     void apply(const double* X, double* Y) {
         launch_near_apply(ctx, d.v, pl.nnz(), P.p, X, Y, R);
-        if (has_far()) launch_far_apply(ctx, d.v, d.far, X, Y, R, M.p, Lc.p, kCoulomb);
+        if (has_far()) {
+            M2LLevelFn<double> m2l_fn = [&](int, int b0, int nb, double scale) {
+                launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
+            };
+            launch_far_field<double>(ctx, d.v, d.far, X, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
+        }
         applies += 1;
+    }
+
+    // Y = A32 X: FP32 near field, FP32 far field with TF32 tensor-core M2L.
+    void apply32(const double* X, double* Y) {
+        launch_to_f32(ctx, X, X32.p, pl.N * R);
+        launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
+        if (has_far()) {
+            M2LLevelFn<float> m2l_fn = [&](int level, int, int, double scale) {
+                launch_m2l_tc(ctx, tc.level[level], E32.p, L32.p, m2l->K32.p, Rb32, (float)scale, tc_err.p);
+            };
+            launch_far_field<float>(ctx, d.v, d.far, X32.p, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
+        }
+        applies32 += 1;
+    }
+
+    // Z (+)= M^-1 V with the chosen right preconditioner.
+    void precondition(const double* V, double* Z, bool add) {
+        if (precond == 1)
+            bj.apply(ctx, V, Z, pl.N, R, add);
+        else
+            launch_diag_scale(ctx, V, inv_diag.p, Z, pl.N, R, add);
+    }
+
+    void check_tc() {
+        if (!mixed || !has_far()) return;
+        int e = 0;
+        tc_err.download(&e, 1);
+        GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+        if (e) throw Error(GPX_ERR_CUDA, "tensor-core M2L pipeline wait expired");
     }
 };
 
@@ -211,10 +350,16 @@ struct SolveStats {
     bool converged = false;
 };
 
+using ApplyFn = std::function<void(const double*, double*)>;
+using PrecondFn = std::function<void(const double*, double*, bool)>;
+
 // Restarted right-preconditioned GMRES(m) on all R columns at once
-// (krylov.rs:50-191 per column); X (N x R) receives the solution.
-void gmres_multi(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d_rhs_cond, int R, int64_t N,
-                 double tol, int m, int max_restarts, DBuf<double>& X, SolveStats& st) {
+// (krylov.rs:50-191 per column); X (N x R) receives the solution.  The
+// right-hand sides are B (N x R) when given, else the unit-conductor vectors
+// of rhs_cond (cap/solver.rs:55-63).
+void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_t* d_cond,
+                 const int32_t* d_rhs_cond, const double* B, int R, int64_t N, double tol, int m, int max_restarts,
+                 DBuf<double>& X, SolveStats& st, bool reorth = true) {
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
     DBuf<double> V, W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
@@ -256,7 +401,10 @@ void gmres_multi(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         return count_zero ? R - *hcount : *hcount;
     };
     // ||b|| (krylov.rs:58, clamped to the smallest positive normal)
-    launch_residual(ctx, d_cond, d_rhs_cond, nullptr, Res.p, N, R);
+    if (B)
+        GPX_CUDA(cudaMemcpyAsync(Res.p, B, (size_t)NR * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    else
+        launch_residual(ctx, d_cond, d_rhs_cond, nullptr, Res.p, N, R);
     launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, bnorm.p);
     {
         KTimer kt(ctx, K_SMALL);
@@ -274,12 +422,16 @@ void gmres_multi(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         int kmax = 0;
         for (int k = 0; k < m; ++k) {
             const double* Vk = V.p + (int64_t)k * NR;
-            launch_diag_scale(ctx, Vk, op.inv_diag.p, Z.p, N, R);
-            op.apply(Z.p, W.p);
+            Minv(Vk, Z.p, false);
+            A(Z.p, W.p);
             launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h1.p, 0);
             launch_multi_axpy(ctx, V.p, NR, k + 1, h1.p, W.p, N, R);
-            launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h2.p, 0);
-            launch_multi_axpy(ctx, V.p, NR, k + 1, h2.p, W.p, N, R);
+            if (reorth) {
+                launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h2.p, 0);
+                launch_multi_axpy(ctx, V.p, NR, k + 1, h2.p, W.p, N, R);
+            } else if (k == 0) {
+                GPX_CUDA(cudaMemsetAsync(h2.p, 0, (size_t)(m + 1) * R * sizeof(double), s));
+            }
             launch_colnorm(ctx, W.p, N, R, partial.p, nblk, hnorm.p);
             launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, V.p + (int64_t)(k + 1) * NR, N, R);
             launch_givens(ctx, gd, k);
@@ -288,9 +440,13 @@ void gmres_multi(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
             if (read_count(act.p, false) == 0) break;
         }
         launch_trisolve(ctx, gd);
-        launch_combine(ctx, V.p, NR, kmax, y.p, op.inv_diag.p, X.p, N, R);
-        op.apply(X.p, W.p);
-        launch_residual(ctx, d_cond, d_rhs_cond, W.p, Res.p, N, R);
+        launch_lincomb(ctx, V.p, NR, kmax, y.p, Z.p, N, R);
+        Minv(Z.p, X.p, true);  // x += M^-1 (V y)  (krylov.rs:154-168)
+        A(X.p, W.p);
+        if (B)
+            launch_sub(ctx, B, W.p, Res.p, NR);
+        else
+            launch_residual(ctx, d_cond, d_rhs_cond, W.p, Res.p, N, R);
         launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, beta.p);
         launch_cycle_end(ctx, gd, beta.p);
         if (read_count(done.p, true) == 0) break;
@@ -321,8 +477,8 @@ Opts normalize(const gpx_solve_opts* o) {
     r.max_restarts = o->max_restarts > 0 ? o->max_restarts : 50;
     r.dense_below = o->dense_below == 0 ? 500 : o->dense_below;
     r.precond = o->precond;
-    r.solve_ground_rhs = o->solve_ground_rhs;
-    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 5;
+    r.skip_ground_rhs = o->skip_ground_rhs;
+    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 3;
     r.mesh_max_edge = o->mesh_max_edge_m;
     r.max_panels = o->max_panels;
     r.far_quad = o->far_quad;
@@ -338,10 +494,14 @@ int choose_depth(const Opts& o, int64_t n) {
     return d;
 }
 
-static void check_problem(int64_t n, const double* verts, const int32_t* cond, int ncond, int order) {
+static void check_problem(int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o) {
     if (n <= 0 || !verts) throw Error(GPX_ERR_CAPACITANCE, "no panels in geometry");
     if (ncond <= 0 || ncond > 4096) throw Error(GPX_ERR_INVALID_ARG, "n_conductors must be in [1, 4096]");
-    if (order < 2 || order > 8) throw Error(GPX_ERR_INVALID_ARG, "Chebyshev order must be in [2, 8]");
+    if (o.order < 2 || o.order > 6) throw Error(GPX_ERR_INVALID_ARG, "Chebyshev order must be in [2, 6]");
+    if (o.precision == GPX_PREC_MIXED && o.order != 4)
+        throw Error(GPX_ERR_INVALID_ARG, "the mixed-precision path runs order-4 expansions");
+    if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
+    if (o.precond != 0 && o.precond != 1) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -351,42 +511,130 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     }
 }
 
+namespace {
+
+struct Prepared {
+    Plan plan;
+    std::shared_ptr<DevM2L> m2l;
+    DevPlanBufs dp;
+    std::unique_ptr<Operator> op;
+};
+
+void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, int R,
+             int depth, Prepared& pr) {
+    build_plan(pr.plan, n, verts, cond, ncond, o.order, depth);
+    if (pr.plan.far && pr.plan.m2l_pairs() > 0) pr.m2l = get_m2l(ctx, o.order, o.m2l_mode);
+    upload_plan(ctx, pr.plan, pr.m2l.get(), pr.dp);
+    pr.op.reset(new Operator(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get()));
+    pr.op->precond = o.precond;
+    pr.op->assemble();
+}
+
+// FP64 iterative refinement around inner GMRES solves with the FP32 /
+// tensor-core operator: x += A32^-1 (b - A x) until the FP64 residual meets
+// the tolerance (design precedent: refine.rs:45-95, f32 LU + f64 residual).
+void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d_rhs, int R, int64_t N,
+                 const Opts& o, DBuf<double>& X, SolveStats& st, int& outer) {
+    cudaStream_t s = ctx.stream;
+    const int64_t NR = N * R;
+    const double inner_tol = std::pow(10.0, -o.inner_tol_exp);
+    DBuf<double> Res, W, D, partial, bn, rn;
+    DBuf<int32_t> mask;
+    Res.alloc(NR, s);
+    W.alloc(NR, s);
+    X.alloc(NR, s);
+    X.zero();
+    const int nblk = reduce_blocks_for(N);
+    partial.alloc((size_t)nblk * R, s);
+    bn.alloc(R, s);
+    rn.alloc(R, s);
+    mask.alloc(R, s);
+    launch_residual(ctx, d_cond, d_rhs, nullptr, Res.p, N, R);
+    launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, bn.p);
+    std::vector<double> hb(R), hr(R);
+    std::vector<int32_t> hm(R);
+    bn.download(hb.data(), R);
+    GPX_CUDA(cudaStreamSynchronize(s));
+    for (double& v : hb) v = std::max(v, 2.2250738585072014e-308);
+    st = SolveStats();
+    outer = 0;
+    const ApplyFn a32 = [&](const double* x, double* y) { op.apply32(x, y); };
+    for (int it = 0; it <= 12; ++it) {
+        launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, rn.p);
+        rn.download(hr.data(), R);
+        GPX_CUDA(cudaStreamSynchronize(s));
+        bool all = true;
+        st.max_resid = 0.0;
+        for (int r = 0; r < R; ++r) {
+            const double rel = hr[r] / hb[r];
+            st.max_resid = std::max(st.max_resid, rel);
+            hm[r] = rel <= o.tol;
+            all = all && hm[r];
+        }
+        if (all) {
+            st.converged = true;
+            break;
+        }
+        if (it == 12) break;
+        mask.upload(hm, s);
+        launch_zero_cols(ctx, Res.p, mask.p, N, R);
+        SolveStats in;
+        // Inner solves stop at 1e-3..1e-4: one classical Gram-Schmidt pass (FP64) keeps the
+        // basis orthogonal far below that, so the re-orthogonalisation pass is skipped.
+        const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
+        gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, o.max_restarts, D, in, false);
+        st.iterations += in.iterations;
+        launch_add(ctx, X.p, D.p, NR);
+        op.apply(X.p, W.p);
+        launch_residual(ctx, d_cond, d_rhs, W.p, Res.p, N, R);
+        outer += 1;
+    }
+    op.check_tc();
+}
+
+}  // namespace
+
 void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, double* C,
                gpx_solve_report* rep) {
     const double t0 = now_s();
     const int64_t l0 = ctx.launches;
-    check_problem(n, verts, cond, ncond, o.order);
-    if (o.precision != GPX_PREC_FP64)
-        throw Error(GPX_ERR_INVALID_ARG, "mixed precision is not available in this build");
+    check_problem(n, verts, cond, ncond, o);
     const int depth = choose_depth(o, n);
     const bool dense = depth == 1;
-    const int R = (o.solve_ground_rhs || ncond == 1) ? ncond : ncond - 1;
-    if (R > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
-    Plan plan;
-    build_plan(plan, n, verts, cond, ncond, o.order, depth);
-    std::shared_ptr<DevM2L> m2l;
-    if (plan.far && plan.m2l_pairs() > 0) m2l = get_m2l(ctx, o.order, o.m2l_mode);
-    DevPlanBufs dp;
-    upload_plan(ctx, plan, m2l.get(), dp);
-    Operator op(ctx, plan, dp, R, o.far_quad);
-    op.assemble();
+    const int Rn = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;  // conductors solved
+    if (Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
+    // Columns are padded to a multiple of 4 (16-byte rows); padding columns
+    // have a zero right-hand side and converge at once.
+    const int R = (Rn + 3) & ~3;
+    Prepared pr;
+    prepare(ctx, n, verts, cond, ncond, o, R, depth, pr);
+    Operator& op = *pr.op;
     std::vector<int32_t> rhs_cond(R);
-    for (int r = 0; r < R; ++r) rhs_cond[r] = r;
+    for (int r = 0; r < R; ++r) rhs_cond[r] = r < Rn ? r : -1;
     DBuf<int32_t> d_rhs;
     d_rhs.upload(rhs_cond, ctx.stream);
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     const double t1 = now_s();
     DBuf<double> X;
     SolveStats st;
+    int outer = 0;
     // The all-pairs path stands in for the reference's dense LU (cap/solver.rs:114-117):
     // solve it to a tighter tolerance so it matches a direct solve.
     const double tol = dense ? std::min(o.tol, 1e-12) : o.tol;
-    gmres_multi(ctx, op, dp.cond.p, d_rhs.p, R, n, tol, o.restart, o.max_restarts, X, st);
+    if (o.precision == GPX_PREC_MIXED) {
+        Opts oi = o;
+        oi.tol = tol;
+        mixed_solve(ctx, op, pr.dp.cond.p, d_rhs.p, R, n, oi, X, st, outer);
+    } else {
+        const ApplyFn a64 = [&](const double* x, double* y) { op.apply(x, y); };
+        const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
+        gmres_multi(ctx, a64, pc, pr.dp.cond.p, d_rhs.p, nullptr, R, n, tol, o.restart, o.max_restarts, X, st);
+    }
     DBuf<double> dC;
     dC.alloc((size_t)ncond * R, ctx.stream);
     {
         KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
-        k_accum_c<<<ncond, 256, 0, ctx.stream>>>(dp.cond.p, dp.area.p, X.p, n, R, dC.p);
+        k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, pr.dp.area.p, X.p, n, R, dC.p);
         GPX_LAUNCH_CHECK();
         ctx.launches += 1;
     }
@@ -397,9 +645,9 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     for (int i = 0; i < ncond; ++i)
         for (int j = 0; j < ncond; ++j) {
             double v;
-            if (j < R)
+            if (j < Rn)
                 v = hc[(size_t)i * R + j];
-            else if (i < R)
+            else if (i < Rn)
                 v = hc[(size_t)j * R + i];  // substrate column by symmetry
             else
                 v = std::nan("");
@@ -409,16 +657,16 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
         gpx_solve_report& r = *rep;
         r.n_panels = n;
         r.n_conductors = ncond;
-        r.n_rhs = R;
+        r.n_rhs = Rn;
         r.order = o.order;
         r.max_level = depth;
-        r.n_boxes = plan.nbox();
-        r.n_leaves = plan.nleaf();
-        r.nnz_near = plan.nnz();
-        r.m2l_pairs = plan.m2l_pairs();
+        r.n_boxes = pr.plan.nbox();
+        r.n_leaves = pr.plan.nleaf();
+        r.nnz_near = pr.plan.near_pairs();
+        r.m2l_pairs = pr.plan.m2l_pairs();
         r.iterations = st.iterations;
-        r.outer_iterations = 0;
-        r.operator_applies = op.applies;
+        r.outer_iterations = outer;
+        r.operator_applies = op.applies + op.applies32;
         r.max_rel_residual = st.max_resid;
         r.converged = st.converged ? 1 : 0;
         r.dense = dense ? 1 : 0;
@@ -434,40 +682,41 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
                                              " iterations");
 }
 
-void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int R, const double* sigma, double* y,
+void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int Rn, const double* sigma, double* y,
                     gpx_solve_report* rep) {
-    check_problem(n, verts, nullptr, 1, o.order);
-    if (R <= 0 || R > 256) throw Error(GPX_ERR_INVALID_ARG, "nrhs must be in [1, 256]");
+    check_problem(n, verts, nullptr, 1, o);
+    if (Rn <= 0 || Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "nrhs must be in [1, 256]");
+    const int R = (Rn + 3) & ~3;
     const int depth = choose_depth(o, n);
-    Plan plan;
-    build_plan(plan, n, verts, nullptr, 1, o.order, depth);
-    std::shared_ptr<DevM2L> m2l;
-    if (plan.far && plan.m2l_pairs() > 0) m2l = get_m2l(ctx, o.order, o.m2l_mode);
-    DevPlanBufs dp;
-    upload_plan(ctx, plan, m2l.get(), dp);
-    Operator op(ctx, plan, dp, R, o.far_quad);
-    op.assemble();
-    std::vector<double> xs((size_t)n * R), ys((size_t)n * R);
+    Prepared pr;
+    prepare(ctx, n, verts, nullptr, 1, o, R, depth, pr);
+    const Plan& plan = pr.plan;
+    std::vector<double> xs((size_t)n * R, 0.0), ys((size_t)n * R);
     for (int64_t s = 0; s < n; ++s)
-        for (int r = 0; r < R; ++r) xs[(size_t)s * R + r] = sigma[(size_t)plan.perm[s] * R + r];
+        for (int r = 0; r < Rn; ++r) xs[(size_t)s * R + r] = sigma[(size_t)plan.perm[s] * Rn + r];
     DBuf<double> X, Y;
     X.upload(xs, ctx.stream);
     Y.alloc(xs.size(), ctx.stream);
-    op.apply(X.p, Y.p);
+    if (o.precision == GPX_PREC_MIXED) {
+        pr.op->apply32(X.p, Y.p);
+        pr.op->check_tc();
+    } else {
+        pr.op->apply(X.p, Y.p);
+    }
     Y.download(ys.data(), ys.size());
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     for (int64_t s = 0; s < n; ++s)
-        for (int r = 0; r < R; ++r) y[(size_t)plan.perm[s] * R + r] = ys[(size_t)s * R + r];
+        for (int r = 0; r < Rn; ++r) y[(size_t)plan.perm[s] * Rn + r] = ys[(size_t)s * R + r];
     if (rep) {
         rep->n_panels = n;
         rep->max_level = depth;
         rep->order = o.order;
         rep->n_boxes = plan.nbox();
         rep->n_leaves = plan.nleaf();
-        rep->nnz_near = plan.nnz();
+        rep->nnz_near = plan.near_pairs();
         rep->m2l_pairs = plan.m2l_pairs();
         rep->dense = depth == 1;
-        rep->t_near_assembly_s = op.t_assembly_s;
+        rep->t_near_assembly_s = pr.op->t_assembly_s;
     }
 }
 

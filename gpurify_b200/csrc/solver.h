@@ -13,8 +13,8 @@ struct Opts {
     int restart = 200, max_restarts = 50;
     int dense_below = 500;
     int precond = 0;
-    int solve_ground_rhs = 1;
-    int inner_tol_exp = 5;
+    int skip_ground_rhs = 0;
+    int inner_tol_exp = 3;
     double mesh_max_edge = 0.0;
     int64_t max_panels = 0;
     int far_quad = 0;

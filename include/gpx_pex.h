@@ -87,8 +87,9 @@ typedef struct {
     int32_t dense_below;     /* all-pairs (no far field) below this many panels;
                                 0 -> 500 (bridge.rs:30), -1 -> never */
     int32_t precond;         /* 0 diagonal Jacobi (fmm_solver.rs:133-162), 1 leaf block-Jacobi */
-    int32_t solve_ground_rhs;/* 1: also solve the substrate column (reference does) */
-    int32_t inner_tol_exp;   /* mixed: inner solve tolerance 10^-x; 0 -> 5 */
+    int32_t skip_ground_rhs; /* 1: do not solve the substrate column (the reference solves it);
+                                the per-net result needs only the nets' columns */
+    int32_t inner_tol_exp;   /* mixed: inner solve tolerance 10^-x; 0 -> 3 */
     double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
@@ -125,8 +126,8 @@ typedef struct {
 
 /* Maxwell capacitance matrix (farads, no dielectric scaling) of the panel
  * problem.  maxwell_out: n_conductors x n_conductors row-major, C[i][j] =
- * charge on i per volt on j.  Columns not solved (substrate when
- * opts.solve_ground_rhs == 0: the last conductor) are filled by symmetry. */
+ * charge on i per volt on j.  With opts.skip_ground_rhs the last (substrate)
+ * column is filled by symmetry from its row and C[last][last] is NaN. */
 gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
                          double* maxwell_out, gpx_solve_report* report);
 

@@ -1,0 +1,65 @@
+"""Mixed-precision path: FP32 near-field apply and FP32 far field with the
+tcgen05 TF32 M2L, inside an FP64 iterative-refinement loop.
+
+Bars: the FP32/TF32 operator apply is within 1e-3 (norm-wise, per column) of the FP64
+operator (TF32 keeps 10 mantissa bits in the M2L; the near field is FP32);
+the refined Maxwell matrix is within 1e-6 of the plain FP64 solve, because
+the refinement residual is the FP64 operator's."""
+import numpy as np
+import pytest
+
+from gpurify_b200 import _lib, layouts
+from tests.helpers import rel_max
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = _lib.Context(0)
+    yield c
+    c.close()
+
+
+def window(nets=12, side=15.0, edge=0.3e-6):
+    lay = layouts.routing_window(nets, side, seed=11)
+    return _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                mesh_max_edge_m=edge, max_panels=-1)
+
+
+@pytest.mark.parametrize("nrhs", [3, 64, 100])
+def test_mixed_operator_close_to_fp64(ctx, nrhs):
+    p = window()
+    rng = np.random.default_rng(5)
+    sig = rng.standard_normal((len(p["verts"]), nrhs))
+    kw = dict(order=4, max_level=5, dense_below=-1, m2l_mode=1)
+    y64, rep = ctx.operator_apply(p["verts"], sig, precision=0, **kw)
+    y32, _ = ctx.operator_apply(p["verts"], sig, precision=1, **kw)
+    assert rep["m2l_pairs"] > 0
+    for j in range(nrhs):
+        e = np.linalg.norm(y32[:, j] - y64[:, j]) / np.linalg.norm(y64[:, j])
+        assert e < 1e-3, (j, e)
+
+
+@pytest.mark.parametrize("far_quad", [0, 1])
+def test_mixed_solve_matches_fp64(ctx, far_quad):
+    p = window()
+    nc = len(p["nets"]) + 1
+    kw = dict(order=4, max_level=5, dense_below=-1, far_quad=far_quad, skip_ground_rhs=1)
+    C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=0, **kw)
+    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, **kw)
+    assert r32["converged"] == 1 and r32["outer_iterations"] >= 1
+    assert r32["max_rel_residual"] <= 1e-8
+    R = nc - 1
+    d = np.abs(np.diag(C64[:R, :R]))
+    err = np.abs(C32[:R, :R] - C64[:R, :R]) / d[:, None]
+    assert err.max() < 1e-6, err.max()
+
+
+def test_mixed_two_wire_small_rhs(ctx):
+    lay = layouts.two_wires()
+    p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly)
+    C64, _ = ctx.cap_solve(p["verts"], p["cond"], 3, order=4, max_level=4)
+    C32, rep = ctx.cap_solve(p["verts"], p["cond"], 3, order=4, max_level=4, precision=1)
+    assert rep["converged"] == 1
+    assert rel_max(C32, C64) < 1e-6

@@ -162,3 +162,20 @@ def test_reference_known_answers_on_gpu(ctx, orc):
     assert rep["dense"] == 0
     assert abs(cf[0, 0] - cd[0, 0]) / cd[0, 0] < 5e-3
     assert abs(cf[0, 0] - FOUR_PI_EPS0) / FOUR_PI_EPS0 < 0.03
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_block_jacobi_matches_diagonal(ctx, orc, precision):
+    """The leaf block-Jacobi preconditioner changes the iteration, not the
+    solution: same Maxwell matrix within the GMRES tolerance, fewer iterations."""
+    lay = layouts.routing_window(12, 15.0, seed=11)
+    p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                             mesh_max_edge_m=0.3e-6, max_panels=-1)
+    nc = len(p["nets"]) + 1
+    kw = dict(order=4, max_level=5, dense_below=-1, precision=precision)
+    C0, r0 = ctx.cap_solve(p["verts"], p["cond"], nc, precond=0, **kw)
+    C1, r1 = ctx.cap_solve(p["verts"], p["cond"], nc, precond=1, **kw)
+    assert r1["converged"] == 1
+    assert r1["iterations"] < r0["iterations"]
+    d = np.abs(np.diag(C0))
+    assert (np.abs(C1 - C0) / d[:, None]).max() < 1e-6
