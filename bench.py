@@ -49,14 +49,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpx", choices=["gpx", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: time the plain FP64 path, then the mixed path (the headline value)")
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--depth", type=int, default=5)
     ap.add_argument("--nets", type=int, default=64)
     ap.add_argument("--side", type=float, default=40.0, help="window side in um")
     ap.add_argument("--restart", type=int, default=200, help="GMRES restart length")
-    ap.add_argument("--far-quad", type=int, default=0, help="0 centroid lumping (reference), 1 Gauss points")
-    ap.add_argument("--precond", type=int, default=0, help="0 diagonal Jacobi (reference), 1 leaf block-Jacobi")
+    ap.add_argument("--far-quad", type=int, default=1, help="0 centroid lumping (reference), 1 Gauss points")
+    ap.add_argument("--precond", type=int, default=1, help="0 diagonal Jacobi (reference), 1 leaf block-Jacobi")
+    ap.add_argument("--accuracy", type=int, default=1, help="1: report errors against the FP64 all-pairs solve")
+    ap.add_argument("--inner-tol-exp", type=int, default=0, help="mixed: inner GMRES tolerance 10^-x (0: default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     return ap.parse_args()
@@ -176,6 +179,57 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def time_solves(ctx, verts, cond, ncond, solve_kw, steps, warmup, stream, dist, local):
+    """Warm-up, then EXACTLY `steps` timed solves between a barrier and
+    device synchronisation, timed with CUDA events on the context stream;
+    per-kernel CUDA-event statistics over the timed region."""
+    import torch
+
+    reps = []
+    for _ in range(warmup):
+        ctx.cap_solve(verts, cond, ncond, **solve_kw)
+    ctx.set_profiling(True)
+    ctx.reset_stats()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    C = None
+    for _ in range(steps):
+        C, rep = ctx.cap_solve(verts, cond, ncond, **solve_kw)
+        reps.append(rep)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    ks = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, reps, ks, clocks, C
+
+
+def roofline_of(ks, ms_total):
+    hbm, bf16, peak_kind = load_peaks()
+    names = [k for k in ks if k != "total_launches"]
+    top = max(names, key=lambda k: ks[k]["ms"])
+    k = ks[top]
+    per_launch_ms = k["ms"] / max(1, k["launches"])
+    ach = k["bytes"] / max(1, k["launches"]) / (per_launch_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "kernel": top, "peak_source": "measured (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
+            "traffic": None, "launches": k["launches"], "ms_per_launch": per_launch_ms,
+            "share_of_step": k["ms"] / ms_total if ms_total > 0 else None,
+            "flops_per_s": k["flops"] / max(1, k["launches"]) / (per_launch_ms * 1e-3)}
+    return roof
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -198,10 +252,9 @@ def main():
     from gpurify_b200 import _lib, pex
 
     ctx = _lib.Context(local)
-    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
-    solve_kw = dict(order=args.order, max_level=args.depth, precision=prec, skip_ground_rhs=1, tol=1e-8,
-                    restart=args.restart, far_quad=args.far_quad, precond=args.precond)
-
+    base_kw = dict(order=args.order, max_level=args.depth, skip_ground_rhs=1, tol=1e-8, restart=args.restart,
+                   far_quad=args.far_quad, precond=args.precond, inner_tol_exp=args.inner_tol_exp)
+    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     lay = workload(rank, args.nets, args.side)
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
                              mesh_max_edge_m=EDGE_M, max_panels=-1)
@@ -211,95 +264,84 @@ def main():
     verts = torch.from_numpy(p["verts"]).pin_memory().numpy()
     cond = torch.from_numpy(p["cond"]).pin_memory().numpy()
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
-
-    def step():
-        C, rep = ctx.cap_solve(verts, cond, ncond, **solve_kw)
-        return rep
-
-    for _ in range(args.warmup):
-        step()
-    ctx.set_profiling(True)
-    ctx.reset_stats()
-    sampler = ClockSampler(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    reps = [step() for _ in range(args.steps)]
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    clocks = sampler.stop()
-    ks = ctx.kernel_stats()
-    ctx.set_profiling(False)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_step = ms / args.steps
+    runs = {}
+    for prec in precisions:
+        kw = dict(base_kw, precision=_lib.PREC_MIXED if prec == "mixed" else _lib.PREC_FP64)
+        ms, reps, ks, clocks, C = time_solves(ctx, verts, cond, ncond, kw, args.steps, args.warmup, stream, dist,
+                                              local)
+        runs[prec] = dict(ms=ms, reps=reps, ks=ks, clocks=clocks, C=C, kw=kw)
+    head = precisions[-1]
+    hr = runs[head]
+    ms_step = hr["ms"] / args.steps
     value = world * 1e3 / ms_step
 
-    # end to end through the public per-net API (layout -> per-net aF)
-    e2e_times = []
-    e2e_rep = {}
+    # end to end through the public per-net API (layout polygons -> per-net aF)
+    e2e_times, e2e_rep = [], {}
     for _ in range(2):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = pex.run_pex_by_net_checked(lay.store, lay.deck, lay.net_of_poly, ctx=ctx, report=e2e_rep,
-                                         mesh_max_edge_m=EDGE_M, max_panels=-1, order=args.order,
-                                         max_level=args.depth, precision=prec, restart=args.restart,
-                                         far_quad=args.far_quad, precond=args.precond)
+        pex.run_pex_by_net_checked(lay.store, lay.deck, lay.net_of_poly, ctx=ctx, report=e2e_rep,
+                                   mesh_max_edge_m=EDGE_M, max_panels=-1, **hr["kw"])
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
+    e2e_s = min(e2e_times)
     if dist:
-        t = torch.tensor([min(e2e_times)], device="cuda")
+        t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    else:
-        e2e_s = min(e2e_times)
+
+    accuracy = None
+    if args.accuracy and rank == 0:
+        # FP64 all-pairs reference (every entry by the exact Wilton integral),
+        # GMRES to 1e-10; errors normalised by the row's diagonal entry.
+        Cd, _ = ctx.cap_solve(verts, cond, ncond, dense_below=2**31 - 1, skip_ground_rhs=1, tol=1e-10,
+                              precond=args.precond)
+        Cn = Cd[:R, :R]
+        dg = np.abs(np.diag(Cn))
+        accuracy = {"reference": "FP64 all-pairs Wilton operator, GMRES tol 1e-10",
+                    "metric": "max_ij |C_ij - Cref_ij| / |Cref_ii|"}
+        for prec, rr in runs.items():
+            accuracy[prec] = float((np.abs(rr["C"][:R, :R] - Cn) / dg[:, None]).max())
+        if "mixed" in runs and "fp64" in runs:
+            accuracy["mixed_vs_fp64"] = float((np.abs(runs["mixed"]["C"][:R, :R] - runs["fp64"]["C"][:R, :R])
+                                               / np.abs(np.diag(runs["fp64"]["C"][:R, :R]))[:, None]).max())
 
     if rank == 0:
-        hbm, bf16, peak_kind = load_peaks()
-        names = [k for k in ks if k != "total_launches"]
-        top = max(names, key=lambda k: ks[k]["ms"])
-        k = ks[top]
-        per_launch_ms = k["ms"] / max(1, k["launches"])
-        tensor_kernels = ()
-        if top in tensor_kernels:
-            ach = k["flops"] / max(1, k["launches"]) / (per_launch_ms * 1e-3) / 1e12
-            roof = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16}
-        else:
-            ach = k["bytes"] / max(1, k["launches"]) / (per_launch_ms * 1e-3) / 1e9
-            roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm}
-        roof.update({"kernel": top, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json)" if peak_kind == "measured"
-                     else "fallback", "traffic": None, "launches": k["launches"], "ms_per_launch": per_launch_ms,
-                     "share_of_step": k["ms"] / ms if ms > 0 else None,
-                     "fp64_tflops": k["flops"] / max(1, k["launches"]) / (per_launch_ms * 1e-3) / 1e12})
-        breakdown = {n: {"ms_per_step": ks[n]["ms"] / args.steps, "launches_per_step": ks[n]["launches"] / args.steps}
-                     for n in names if ks[n]["launches"]}
+        roof = roofline_of(hr["ks"], hr["ms"])
+        names = [k for k in hr["ks"] if k != "total_launches"]
+        breakdown = {n: {"ms_per_step": hr["ks"][n]["ms"] / args.steps,
+                         "launches_per_step": hr["ks"][n]["launches"] / args.steps}
+                     for n in names if hr["ks"][n]["launches"]}
         cb = None
         if not args.no_cpu_baseline:
             cb = cpu_baseline(p, ncond, R, args.order, args.depth, args.cpu_threads)
             cb = {k2: cb[k2] for k2 in ("value", "unit", "cores", "kind", "sample")}
-        last = reps[-1]
+        per_prec = {}
+        for prec, rr in runs.items():
+            msp = rr["ms"] / args.steps
+            per_prec[prec] = {"solves_per_s": world * 1e3 / msp, "ms_per_step": msp,
+                              "panel_rhs_per_s": world * N * R / (msp * 1e-3),
+                              "iterations": rr["reps"][-1]["iterations"],
+                              "outer_iterations": rr["reps"][-1]["outer_iterations"],
+                              "max_rel_residual": rr["reps"][-1]["max_rel_residual"]}
         out = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == _lib.PREC_FP64 else "f32/tf32+f64",
+            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64 (FP64 refinement)",
             "data": "synthetic (seeded 64-net routing window; no public layout used)",
             "config": {"workload": f"routing window {args.nets} nets {args.side:g}x{args.side:g}um 3 layers, 0.25um "
                                    f"panels, {N} panels, {R} RHS, GMRES tol 1e-8",
-                       "panels": N, "rhs": R, "precision": args.precision, "order": args.order, "depth": args.depth,
+                       "panels": N, "rhs": R, "precision": head, "order": args.order, "depth": args.depth,
                        "far_quad": args.far_quad, "restart": args.restart, "precond": args.precond,
-                       "parallelism": f"replicas x{world}", "l2": "working set (Krylov basis ~7 GB) >> L2"},
+                       "parallelism": f"replicas x{world}", "l2": "working set (Krylov basis > 1 GB) >> L2"},
             "panel_rhs_per_s": world * N * R / (ms_step * 1e-3),
-            "iterations": last["iterations"], "max_rel_residual": last["max_rel_residual"],
-            "gpu_launches": ks["total_launches"],
+            "precisions": per_prec,
+            "speedup_mixed_vs_fp64": (per_prec["mixed"]["solves_per_s"] / per_prec["fp64"]["solves_per_s"]
+                                      if "mixed" in per_prec and "fp64" in per_prec else None),
+            "accuracy": accuracy,
+            "gpu_launches": hr["ks"]["total_launches"],
             "roofline": roof, "kernel_breakdown": breakdown,
-            "cpu_baseline": cb, "clocks": clocks,
+            "cpu_baseline": cb, "clocks": hr["clocks"],
             "e2e": {"value": world / e2e_s, "unit": "solves/s", "api": "run_pex_by_net_checked",
                     "h2d_bytes_per_step": int(e2e_rep.get("h2d_bytes", 0)),
                     "d2h_bytes_per_step": int(e2e_rep.get("d2h_bytes", 0)),

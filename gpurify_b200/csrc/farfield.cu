@@ -235,6 +235,175 @@ __global__ void __launch_bounds__(256) k_m2l64(DevPlan p, int b0, double* __rest
     }
 }
 
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
+// Factored M2L for low-rank (compressed) order-4 operators K_o = U_o Vt_o, in
+// two GEMM phases per level:
+//   phase 1, CTA per source box s: for every column c = (pair e, k) of the
+//     source's outgoing pairs, T[t_e][r][col(e,k)] = sum_l E_s[r][l] Vt_o[k][l];
+//   phase 2, CTA per target box t: L_t[r][m] += scale * sum_c T_t[r][c] Ut[c][m],
+//     the contraction running over the concatenated ranks of t's pairs.
+// T is stored target-major (R rows x Kp_t columns per target, Kp_t = the
+// summed ranks rounded up to 4) so phase 2 reads contiguous rows.
+// Phase 1 as a transposed GEMM per work item (source box, up to 64 of its
+// columns): C[c][r] = sum_l Vt_c[l] E_s[r][l].  The 64 gathered Vt rows (A)
+// stream through a cp.async double buffer; E_s^T (B) is staged once.
+template <class T>
+__global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __restrict__ item_src,
+                                                  const int64_t* __restrict__ item_c0,
+                                                  const int32_t* __restrict__ item_cnt, const T* __restrict__ E,
+                                                  int R) {
+    constexpr int V = 16 / sizeof(T);
+    constexpr int KC = 128 / sizeof(T);
+    constexpr int PP = KC + V;
+    constexpr int BP = 64 + V;
+    const int it = blockIdx.x;
+    const int rc = blockIdx.y * 64;
+    const int s = item_src[it];
+    const int64_t c0 = item_c0[it];
+    const int nc = item_cnt[it];
+    const int rows = min(64, R - rc);
+    extern __shared__ __align__(16) unsigned char fac_smem[];
+    T(*As)[64][PP] = reinterpret_cast<T(*)[64][PP]>(fac_smem);                        // [2][64][PP]: [c][l]
+    T(*Bs)[BP] = reinterpret_cast<T(*)[BP]>(fac_smem + sizeof(T) * 2 * 64 * PP);      // [64][BP]:  [l][r]
+    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+    auto issue = [&](int ch) {
+        const int k0 = ch * KC, buf = ch & 1;
+#pragma unroll
+        for (int q = 0; q < KC / V; ++q) {
+            const int id = tid + 64 * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
+            const bool ok = row < nc;
+            cp16(&As[buf][row][kc], ok ? (const void*)(f.Vt + f.col_vt[c0 + row] + k0 + kc) : (const void*)f.Vt, ok);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    issue(0);
+    const T* Es = E + ((int64_t)s * R + rc) * 64;
+    for (int e = tid; e < 64 * 64; e += 64) {
+        const int r = e >> 6, l = e & 63;
+        Bs[l][r] = r < rows ? Es[(int64_t)r * 64 + l] : (T)0;
+    }
+    T acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = (T)0;
+    constexpr int nch = 64 / KC;
+    for (int ch = 0; ch < nch; ++ch) {
+        __syncthreads();
+        if (ch + 1 < nch) {
+            issue(ch + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const int buf = ch & 1;
+#pragma unroll 4
+        for (int kk = 0; kk < KC; ++kk) {
+            T a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = As[buf][ty + 8 * i][kk];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Bs[ch * KC + kk][tx + 8 * j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int c = ty + 8 * i;
+        if (c >= nc) continue;
+        const int tg = f.col_tgt[c0 + c];
+        const int ld = (int)((f.tgt_col_off[tg + 1] - f.tgt_col_off[tg] + 3) & ~int64_t(3));
+        T* dst = f.Tm + f.tgt_base[tg] * R + (int64_t)rc * ld + f.col_pos[c0 + c];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = tx + 8 * j;
+            if (r < rows) dst[(int64_t)r * ld] = acc[i][j];
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __restrict__ L, int R, double scale) {
+    constexpr int V = 16 / sizeof(T);
+    constexpr int KC = 128 / sizeof(T);
+    constexpr int PP = KC + V;
+    constexpr int XP = 64 + V;
+    const int t = b0 + blockIdx.x;
+    const int rc = blockIdx.y * 64;
+    const int64_t k0g = f.tgt_col_off[t], K = f.tgt_col_off[t + 1] - k0g;
+    if (K == 0) return;
+    const int Kp = (int)((K + 3) & ~int64_t(3));
+    const T* A = f.Tm + f.tgt_base[t] * R + (int64_t)rc * Kp;
+    const int m = min(64, R - rc);
+    __shared__ __align__(16) T As[2][64][PP];
+    __shared__ __align__(16) T Bs[2][KC][XP];
+    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+    const int nchunk = (Kp + KC - 1) / KC;
+    auto issue = [&](int cch) {
+        const int k0 = cch * KC, buf = cch & 1;
+#pragma unroll
+        for (int q = 0; q < KC / V; ++q) {
+            const int id = tid + 64 * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
+            const bool ok = row < m && k0 + kc < Kp;
+            cp16(&As[buf][row][kc], ok ? (const void*)(A + (int64_t)row * Kp + k0 + kc) : (const void*)f.Tm, ok);
+        }
+#pragma unroll
+        for (int q = 0; q < KC / V; ++q) {
+            const int id = tid + 64 * q, kk = id / (64 / V), cc = (id % (64 / V)) * V;
+            const bool ok = k0 + kk < K;
+            cp16(&Bs[buf][kk][cc], ok ? (const void*)(f.Ut + f.tgt_ut[k0g + k0 + kk] + cc) : (const void*)f.Ut, ok);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    T acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = (T)0;
+    issue(0);
+    for (int cch = 0; cch < nchunk; ++cch) {
+        __syncthreads();
+        if (cch + 1 < nchunk) {
+            issue(cch + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const int buf = cch & 1;
+#pragma unroll 4
+        for (int kk = 0; kk < KC; ++kk) {
+            T a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = As[buf][ty + 8 * i][kk];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Bs[buf][kk][tx + 8 * j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int r = ty + 8 * i;
+        if (r >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            T* dst = L + ((int64_t)t * R + rc + r) * 64 + tx + 8 * j;
+            *dst += (T)scale * acc[i][j];
+        }
+    }
+}
+
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace
@@ -285,6 +454,26 @@ void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, 
         c.launches += 1;
     }
 }
+
+template <class T>
+void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int nb, T* L, const T* E, int R,
+                    double scale) {
+    constexpr int V = 16 / sizeof(T), KC = 128 / sizeof(T);
+    const int smem = (int)(sizeof(T) * (2 * 64 * (KC + V) + 64 * (64 + V)));
+    if (lv.nitems > 0) {
+        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_v<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_m2l_fac_v<T><<<dim3(lv.nitems, cdiv(R, 64)), 64, smem, c.stream>>>(f, lv.item_src, lv.item_c0, lv.item_cnt,
+                                                                              E, R);
+    }
+    GPX_LAUNCH_CHECK();
+    k_m2l_fac_u<T><<<dim3(nb, cdiv(R, 64)), 64, 0, c.stream>>>(f, b0, L, R, scale);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;  // the caller counts the other one
+}
+template void launch_m2l_fac<double>(Ctx&, const FacM2L<double>&, const FacLevel&, int, int, double*, const double*,
+                                     int, double);
+template void launch_m2l_fac<float>(Ctx&, const FacM2L<float>&, const FacLevel&, int, int, float*, const float*, int,
+                                    double);
 
 void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale) {
     k_m2l64<<<nb, 256, 0, c.stream>>>(p, b0, L, E, R, scale);

@@ -17,8 +17,35 @@ template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, double* Y, int R, int Rb, T* E,
                       T* L, double coef, const M2LLevelFn<T>& m2l);
 
-// FP64 M2L of one level with CUDA-core FMAs.
+// FP64 M2L of one level with CUDA-core FMAs (dense operators).
 void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale);
+
+// Factored M2L data (order 4, 64 nodes): low-rank factors of every offset,
+// per-source column lists for phase 1 and per-target B-row lists for phase 2.
+template <class T>
+struct FacM2L {
+    const T* Vt = nullptr;              // 343 x 64 x 64, row k of slot o = Vt_o[k][:]
+    const T* Ut = nullptr;              // 343 x 64 x 64, row k of slot o = U_o[:][k]
+    const int64_t* src_col_off = nullptr;  // nbox + 1: phase-1 columns of each source box
+    const int64_t* col_vt = nullptr;    // per column: offset of its Vt row
+    const int32_t* col_tgt = nullptr;   // per column: target box
+    const int32_t* col_pos = nullptr;   // per column: column in the target's T block
+    const int64_t* tgt_col_off = nullptr;  // nbox + 1: phase-2 contraction range of each target
+    const int64_t* tgt_ut = nullptr;    // per contraction index: offset of its Ut row
+    const int64_t* tgt_base = nullptr;  // nbox: sum of padded block widths of earlier boxes
+    T* Tm = nullptr;                    // target-major intermediate (R rows x Kp per target)
+};
+// Phase-1 work items of one level: (source box, first column, column count <= 64).
+struct FacLevel {
+    int nitems = 0;
+    const int32_t* item_src = nullptr;
+    const int64_t* item_c0 = nullptr;
+    const int32_t* item_cnt = nullptr;
+};
+// M2L of one level with the factored operators (two kernels).
+template <class T>
+void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int nb, T* L, const T* E, int R,
+                    double scale);
 
 // Tensor-core (tcgen05, TF32 inputs, FP32 accumulation) M2L work list of one
 // level: pairs of target boxes sharing one offset loop.

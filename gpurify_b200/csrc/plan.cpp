@@ -74,7 +74,8 @@ double powi_sq(double a, int b) {
 // Column-pivoted modified Gram-Schmidt truncation of the m x m kernel matrix
 // g (linalg.rs:277-381), returning the product Q_k * R_k (P^T applied):
 // the operator the reference applies as U * (V^T x).
-void qr_truncate_product(const std::vector<double>& g, int m, double eps, double* out, int32_t* rank) {
+void qr_truncate_product(const std::vector<double>& g, int m, double eps, double* out, int32_t* rank, double* Uo,
+                         double* Vto) {
     std::vector<double> q(g), r((size_t)m * m, 0.0), nrm(m);
     std::vector<int> perm(m);
     std::iota(perm.begin(), perm.end(), 0);
@@ -125,6 +126,10 @@ void qr_truncate_product(const std::vector<double>& g, int m, double eps, double
             for (int i = 0; i < k; ++i) s += q[(size_t)a * m + i] * vt[(size_t)i * m + b];
             out[(size_t)a * m + b] = s;
         }
+    for (int a = 0; a < m; ++a)
+        for (int i = 0; i < m; ++i) Uo[(size_t)a * m + i] = i < k ? q[(size_t)a * m + i] : 0.0;
+    for (int i = 0; i < m; ++i)
+        for (int b = 0; b < m; ++b) Vto[(size_t)i * m + b] = i < k ? vt[(size_t)i * m + b] : 0.0;
     *rank = k;
 }
 
@@ -168,6 +173,8 @@ void build_m2l_table(M2LTable& t, int n, int mode) {
     t.n = n;
     t.mode = mode;
     t.K.assign((size_t)343 * n3 * n3, 0.0);
+    t.U.assign((size_t)343 * n3 * n3, 0.0);
+    t.Vt.assign((size_t)343 * n3 * n3, 0.0);
     t.rank.assign(343, -1);
     std::vector<double> roots = cheb_roots(n);
     std::vector<double> ref((size_t)n3 * 3);
@@ -203,7 +210,7 @@ void build_m2l_table(M2LTable& t, int n, int mode) {
                 std::copy(g.begin(), g.end(), dst);
                 t.rank[s] = n3;
             } else {
-                qr_truncate_product(g, n3, eps, dst, &t.rank[s]);
+                qr_truncate_product(g, n3, eps, dst, &t.rank[s], &t.U[(size_t)s * n3 * n3], &t.Vt[(size_t)s * n3 * n3]);
             }
         }
     };

@@ -86,6 +86,10 @@ struct M2LTable {
     int n = 0, mode = 0;
     std::vector<double> K;      // 343 * n3 * n3
     std::vector<int32_t> rank;  // per slot (n3 for exact; -1 unused)
+    // Compressed mode: the factors, K = U * Vt, stored with a fixed stride of
+    // n3 columns (U: n3 x n3, first rank columns used) and n3 rows (Vt: first
+    // rank rows used).
+    std::vector<double> U, Vt;  // 343 * n3 * n3 each
 };
 void build_m2l_table(M2LTable& t, int n, int mode);
 

@@ -26,6 +26,11 @@ namespace gpx {
 struct DevM2L {
     int n = 0, mode = 0;
     DBuf<double> K;   // FP64 operators
+    DBuf<double> U, Vt;  // low-rank factors (compressed mode), stride n3
+    DBuf<double> Ut64, Vt64;  // factored-M2L tables: Vt rows and transposed U rows (order 4)
+    DBuf<float> Ut32, Vt32;
+    DBuf<int32_t> d_rank;
+    int max_rank = 0;
     DBuf<float> K32;  // the same, rounded to TF32 (round to nearest, ties away), for the tensor-core M2L
     std::vector<int32_t> rank;
 };
@@ -46,6 +51,28 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
     d->mode = mode;
     d->rank = host.rank;
     d->K.upload(host.K, ctx.stream);
+    if (mode == GPX_M2L_COMPRESSED) {
+        d->U.upload(host.U, ctx.stream);
+        d->Vt.upload(host.Vt, ctx.stream);
+    }
+    d->d_rank.upload(host.rank, ctx.stream);
+    for (int32_t r : host.rank) d->max_rank = std::max(d->max_rank, (int)r);
+    if (mode == GPX_M2L_COMPRESSED && n == 4) {
+        const size_t sz = (size_t)343 * 64 * 64;
+        std::vector<double> ut(sz);
+        std::vector<float> ut32(sz), vt32(sz);
+        for (int s = 0; s < 343; ++s)
+            for (int k = 0; k < 64; ++k)
+                for (int m = 0; m < 64; ++m) {
+                    ut[((size_t)s * 64 + k) * 64 + m] = host.U[((size_t)s * 64 + m) * 64 + k];
+                    ut32[((size_t)s * 64 + k) * 64 + m] = (float)ut[((size_t)s * 64 + k) * 64 + m];
+                    vt32[((size_t)s * 64 + k) * 64 + m] = (float)host.Vt[((size_t)s * 64 + k) * 64 + m];
+                }
+        d->Ut64.upload(ut, ctx.stream);
+        d->Vt64.upload(host.Vt, ctx.stream);
+        d->Ut32.upload(ut32, ctx.stream);
+        d->Vt32.upload(vt32, ctx.stream);
+    }
     std::vector<float> k32(host.K.size());
     for (size_t i = 0; i < k32.size(); ++i) {
         float f = (float)host.K[i];
@@ -227,6 +254,16 @@ struct Operator {
     TcLists tc;
     int precond = 0;
     BlockJacobi bj;
+    bool factored = false;  // M2L through the low-rank factors (order 4, compressed)
+    FacM2L<double> fac64;
+    FacM2L<float> fac32;
+    DBuf<int64_t> src_col_off, col_vt, tgt_col_off, tgt_ut, tgt_base;
+    DBuf<int32_t> col_tgt, col_pos;
+    DBuf<double> T64;
+    DBuf<float> T32;
+    std::vector<FacLevel> fac_level;
+    DBuf<int32_t> fi_src, fi_cnt;
+    DBuf<int64_t> fi_c0;
     int Rb32 = 0;
     double t_assembly_s = 0.0;
     int64_t applies = 0, applies32 = 0;
@@ -261,6 +298,7 @@ struct Operator {
             d.v.wsrc = d.wsrc.p;
             E64.alloc((size_t)pl.nbox() * pl.n3 * R, s);
             L64.alloc((size_t)pl.nbox() * pl.n3 * R, s);
+            if (m2l && m2l->mode == GPX_M2L_COMPRESSED && pl.n3 == 64 && m2l->max_rank <= 32) setup_factored();
         }
         if (mixed) {
             P32.alloc((size_t)pl.nnz(), s);
@@ -270,19 +308,124 @@ struct Operator {
                 Rb32 = (R + 63) / 64 * 64;
                 E32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
                 L32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
-                build_tc_lists(ctx, pl, tc);
+                if (!factored) build_tc_lists(ctx, pl, tc);
                 tc_err.alloc(1, s);
                 tc_err.zero();
             }
         }
     }
 
+    // Column lists of the factored M2L: phase 1 per source box, phase 2 per
+    // target box (see farfield.cu).
+    void setup_factored() {
+        const int64_t np = pl.m2l_pairs(), nb = pl.nbox();
+        std::vector<int32_t> rank(343);
+        m2l->d_rank.download(rank.data(), 343);
+        GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+        std::vector<int64_t> tcol(nb + 1, 0), base(nb, 0), pos_of_pair(np);
+        std::vector<int32_t> tgt_of_pair(np);
+        int64_t acc = 0;
+        for (int64_t b = 0; b < nb; ++b) {
+            int64_t k = 0;
+            for (int64_t e = pl.m2l_off[b]; e < pl.m2l_off[b + 1]; ++e) {
+                pos_of_pair[e] = k;
+                tgt_of_pair[e] = (int32_t)b;
+                k += rank[pl.m2l_slot[e]];
+            }
+            tcol[b + 1] = tcol[b] + k;
+            base[b] = acc;
+            acc += (k + 3) & ~int64_t(3);
+        }
+        std::vector<int64_t> ut(tcol[nb]);
+        for (int64_t b = 0; b < nb; ++b) {
+            int64_t j = tcol[b];
+            for (int64_t e = pl.m2l_off[b]; e < pl.m2l_off[b + 1]; ++e)
+                for (int k = 0; k < rank[pl.m2l_slot[e]]; ++k) ut[j++] = ((int64_t)pl.m2l_slot[e] * 64 + k) * 64;
+        }
+        // phase-1 columns grouped by source box
+        std::vector<int64_t> scol(nb + 1, 0);
+        for (int64_t e = 0; e < np; ++e) scol[pl.m2l_src[e] + 1] += rank[pl.m2l_slot[e]];
+        for (int64_t b = 0; b < nb; ++b) scol[b + 1] += scol[b];
+        std::vector<int64_t> cvt(scol[nb]), fill(scol.begin(), scol.end() - 1);
+        std::vector<int32_t> ctg(scol[nb]), cps(scol[nb]);
+        for (int64_t e = 0; e < np; ++e) {
+            const int s = pl.m2l_src[e], slot = pl.m2l_slot[e];
+            for (int k = 0; k < rank[slot]; ++k) {
+                const int64_t c = fill[s]++;
+                cvt[c] = ((int64_t)slot * 64 + k) * 64;
+                ctg[c] = tgt_of_pair[e];
+                cps[c] = (int32_t)(pos_of_pair[e] + k);
+            }
+        }
+        // phase-1 work items per level: each source box's columns in tiles of 64
+        std::vector<int32_t> isrc, icnt;
+        std::vector<int64_t> ic0;
+        std::vector<int> lvl_first(pl.L + 2, 0);
+        for (int l = 0; l <= pl.L; ++l) {
+            lvl_first[l] = (int)isrc.size();
+            for (int32_t b = pl.lvl_off[l]; b < pl.lvl_off[l + 1]; ++b)
+                for (int64_t c = scol[b]; c < scol[b + 1]; c += 64) {
+                    isrc.push_back(b);
+                    ic0.push_back(c);
+                    icnt.push_back((int32_t)std::min<int64_t>(64, scol[b + 1] - c));
+                }
+        }
+        lvl_first[pl.L + 1] = (int)isrc.size();
+        cudaStream_t s = ctx.stream;
+        fi_src.upload(isrc, s);
+        fi_cnt.upload(icnt, s);
+        fi_c0.upload(ic0, s);
+        fac_level.assign(pl.L + 1, FacLevel());
+        for (int l = 0; l <= pl.L; ++l) {
+            FacLevel& fl = fac_level[l];
+            fl.nitems = lvl_first[l + 1] - lvl_first[l];
+            fl.item_src = fi_src.p + lvl_first[l];
+            fl.item_c0 = fi_c0.p + lvl_first[l];
+            fl.item_cnt = fi_cnt.p + lvl_first[l];
+        }
+        src_col_off.upload(scol, s);
+        col_vt.upload(cvt, s);
+        col_tgt.upload(ctg, s);
+        col_pos.upload(cps, s);
+        tgt_col_off.upload(tcol, s);
+        tgt_ut.upload(ut, s);
+        tgt_base.upload(base, s);
+        auto wire = [&](auto& f) {
+            f.src_col_off = src_col_off.p;
+            f.col_vt = col_vt.p;
+            f.col_tgt = col_tgt.p;
+            f.col_pos = col_pos.p;
+            f.tgt_col_off = tgt_col_off.p;
+            f.tgt_ut = tgt_ut.p;
+            f.tgt_base = tgt_base.p;
+        };
+        wire(fac64);
+        wire(fac32);
+        T64.alloc((size_t)acc * R, s);
+        T64.zero();  // padding columns stay zero
+        fac64.Tm = T64.p;
+        fac64.Ut = m2l->Ut64.p;
+        fac64.Vt = m2l->Vt64.p;
+        if (mixed) {
+            Rb32 = (R + 63) / 64 * 64;
+            T32.alloc((size_t)acc * Rb32, s);
+            T32.zero();
+            fac32.Tm = T32.p;
+            fac32.Ut = m2l->Ut32.p;
+            fac32.Vt = m2l->Vt32.p;
+        }
+        factored = true;
+    }
+
     // Y = A X in FP64 (X, Y: N x R, leaf-sorted panel order).
     void apply(const double* X, double* Y) {
         launch_near_apply(ctx, d.v, pl.nnz(), P.p, X, Y, R);
         if (has_far()) {
-            M2LLevelFn<double> m2l_fn = [&](int, int b0, int nb, double scale) {
-                launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
+            M2LLevelFn<double> m2l_fn = [&](int level, int b0, int nb, double scale) {
+                if (factored)
+                    launch_m2l_fac<double>(ctx, fac64, fac_level[level], b0, nb, L64.p, E64.p, R, scale);
+                else
+                    launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
             };
             launch_far_field<double>(ctx, d.v, d.far, X, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
         }
@@ -294,8 +437,11 @@ struct Operator {
         launch_to_f32(ctx, X, X32.p, pl.N * R);
         launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
         if (has_far()) {
-            M2LLevelFn<float> m2l_fn = [&](int level, int, int, double scale) {
-                launch_m2l_tc(ctx, tc.level[level], E32.p, L32.p, m2l->K32.p, Rb32, (float)scale, tc_err.p);
+            M2LLevelFn<float> m2l_fn = [&](int level, int b0, int nb, double scale) {
+                if (factored)
+                    launch_m2l_fac<float>(ctx, fac32, fac_level[level], b0, nb, L32.p, E32.p, Rb32, scale);
+                else
+                    launch_m2l_tc(ctx, tc.level[level], E32.p, L32.p, m2l->K32.p, Rb32, (float)scale, tc_err.p);
             };
             launch_far_field<float>(ctx, d.v, d.far, X32.p, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
         }
@@ -478,7 +624,7 @@ Opts normalize(const gpx_solve_opts* o) {
     r.dense_below = o->dense_below == 0 ? 500 : o->dense_below;
     r.precond = o->precond;
     r.skip_ground_rhs = o->skip_ground_rhs;
-    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 3;
+    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 5;
     r.mesh_max_edge = o->mesh_max_edge_m;
     r.max_panels = o->max_panels;
     r.far_quad = o->far_quad;
@@ -537,7 +683,7 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
                  const Opts& o, DBuf<double>& X, SolveStats& st, int& outer) {
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
-    const double inner_tol = std::pow(10.0, -o.inner_tol_exp);
+    const double floor_tol = std::pow(10.0, -o.inner_tol_exp);
     DBuf<double> Res, W, D, partial, bn, rn;
     DBuf<int32_t> mask;
     Res.alloc(NR, s);
@@ -578,8 +724,13 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         if (it == 12) break;
         mask.upload(hm, s);
         launch_zero_cols(ctx, Res.p, mask.p, N, R);
+        // Adaptive inner tolerance: ask each inner solve for no more than the
+        // outer residual still needs (x 0.3 margin), but never below the floor
+        // 10^-inner_tol_exp that the FP32 operator supports.
+        const double need = 0.3 * o.tol / std::max(st.max_resid, 1e-300);
+        const double inner_tol = std::min(0.1, std::max(need, floor_tol));
         SolveStats in;
-        // Inner solves stop at 1e-3..1e-4: one classical Gram-Schmidt pass (FP64) keeps the
+        // Inner solves stop at 1e-3..1e-5: one classical Gram-Schmidt pass (FP64) keeps the
         // basis orthogonal far below that, so the re-orthogonalisation pass is skipped.
         const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
         gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, o.max_restarts, D, in, false);

@@ -89,7 +89,7 @@ typedef struct {
     int32_t precond;         /* 0 diagonal Jacobi (fmm_solver.rs:133-162), 1 leaf block-Jacobi */
     int32_t skip_ground_rhs; /* 1: do not solve the substrate column (the reference solves it);
                                 the per-net result needs only the nets' columns */
-    int32_t inner_tol_exp;   /* mixed: inner solve tolerance 10^-x; 0 -> 3 */
+    int32_t inner_tol_exp;   /* mixed: floor of the adaptive inner tolerance, 10^-x; 0 -> 5 */
     double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
