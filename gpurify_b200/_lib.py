@@ -28,7 +28,7 @@ EXPORTS = (
     "gpx_ctx_create", "gpx_ctx_destroy", "gpx_last_error", "gpx_version", "gpx_cap_solve",
     "gpx_cap_solve_batched", "gpx_operator_apply", "gpx_potential_matrix", "gpx_cap_solve_groups",
     "gpx_extract_quasistatic", "gpx_bridge_panelize", "gpx_plan_check", "gpx_ctx_stream",
-    "gpx_ctx_set_profiling", "gpx_ctx_kernel_stats", "gpx_ctx_reset_stats",
+    "gpx_ctx_set_profiling", "gpx_ctx_kernel_stats", "gpx_ctx_reset_stats", "gpx_cap_solve_small_static",
 )
 KERNEL_CLASSES = ("near_assemble", "near_apply", "p2m", "m2m", "m2l", "l2l", "l2p", "gs_dot", "gs_axpy", "vec",
                   "small")
@@ -142,6 +142,7 @@ def load(build_if_missing: bool = True):
         L.gpx_ctx_kernel_stats.argtypes = [vp, i32, C.POINTER(i64), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                            C.POINTER(C.c_double), C.POINTER(i64)]
         L.gpx_ctx_reset_stats.argtypes = [vp]
+        L.gpx_cap_solve_small_static.argtypes = [vp, i64, vp, vp, i32, vp]
         for name in EXPORTS:
             if name not in ("gpx_ctx_destroy", "gpx_last_error", "gpx_version", "gpx_ctx_stream"):
                 getattr(L, name).restype = C.c_int
@@ -222,6 +223,14 @@ class Context:
         self._check(self.L.gpx_operator_apply(self.h, C.byref(pb), C.byref(opts(**kw)), s.shape[1], s.ctypes.data,
                                               y.ctypes.data, C.byref(rep)))
         return y, rep.as_dict()
+
+    def cap_solve_small_static(self, n_panels: int, d_verts: int, d_conductor: int, n_conductors: int,
+                               d_maxwell_out: int):
+        """gpx_cap_solve_small_static on device pointers (integers): the
+        Maxwell matrix of <= 512 panels and <= 64 conductors, computed in the
+        library's fixed static device scratch without allocating."""
+        self._check(self.L.gpx_cap_solve_small_static(self.h, n_panels, d_verts, d_conductor, n_conductors,
+                                                      d_maxwell_out))
 
     def potential_matrix(self, src_verts, points):
         v = np.ascontiguousarray(src_verts, dtype=np.float64).reshape(-1, 12)

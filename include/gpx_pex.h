@@ -146,6 +146,45 @@ gpx_status gpx_operator_apply(gpx_ctx* ctx, const gpx_panel_problem* problem, co
 gpx_status gpx_potential_matrix(gpx_ctx* ctx, int64_t n_src, const double* src_verts, int64_t n_tgt,
                                 const double* tgt_points, double* out);
 
+/* ---- small problems without allocation ----
+ * No counterpart in the reference.
+ *
+ * Maxwell matrix (farads, no dielectric scaling, n_conductors x n_conductors
+ * row-major, same meaning as gpx_cap_solve's maxwell_out) of a small panel
+ * problem whose panels are already in device memory: d_verts (n_panels x 12
+ * doubles, layout of gpx_panel_problem), d_conductor (n_panels ints) and
+ * d_maxwell_out must be device (or managed) memory of the context's device.
+ * The algorithm is the reference's dense path: assemble P, LU with partial
+ * pivoting, one unit-potential solve per conductor, charge sums per conductor.
+ *
+ * Why it exists: the call allocates no memory, device or host, on its success
+ * path.  It is for callers that cannot let a library allocate: a process whose
+ * device memory is already carved up by its own pool allocator (an EDA tool
+ * or a framework that reserves nearly all of HBM up front, where a library
+ * allocation fails or fragments the pool), and tight per-window loops where
+ * allocating and freeing on every call would synchronise the device.  All
+ * intermediate data lives in one fixed array of 2,377,984 bytes (about
+ * 2.3 MiB) of static device memory per device, present once the library is
+ * loaded on that device.
+ *
+ * Limits: 1 <= n_panels <= 512 and 1 <= n_conductors <= 64; larger problems
+ * are rejected with GPX_ERR_INVALID_ARG and a message naming the limit (use
+ * gpx_cap_solve for them).  A conductor index outside [0, n_conductors) gives
+ * GPX_ERR_INVALID_ARG; a zero pivot gives GPX_ERR_CAPACITANCE.
+ *
+ * The caller zeroes nothing: the call clears its own status word before its
+ * first launch, and writes every other scratch element before reading it.
+ * The call runs on the context's stream and waits for that stream before it
+ * returns.  The first call on each device also does a one-time set-up (looks
+ * up the scratch array's device address and raises one kernel's shared-memory
+ * limit); make that first call before any stream capture on that device.
+ * Every call on one device uses the same scratch array, so two calls that
+ * overlapped would race on it; the library therefore serialises the calls of
+ * one process per device with a lock held until the call's stream work has
+ * finished.  Each process has its own copy of the array. */
+gpx_status gpx_cap_solve_small_static(gpx_ctx* ctx, int64_t n_panels, const double* d_verts,
+                                      const int32_t* d_conductor, int32_t n_conductors, double* d_maxwell_out);
+
 /* ---- bridge level ---- */
 typedef struct {
     uint32_t net;
