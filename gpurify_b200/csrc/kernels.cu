@@ -33,17 +33,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_near_assemble(DevPlan p, double
     __shared__ int64_t s_beg[28];
     __shared__ int32_t s_pre[29];
     __shared__ int64_t s_gid[kAsmTile];
-    const int e0 = p.near_off[t], ne = p.near_off[t + 1] - e0;
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int e = 0; e < ne; ++e) {
-            int src = p.near_src[e0 + e];
-            s_beg[e] = p.leaf_begin[src];
-            s_pre[e] = acc;
-            acc += (int)(p.leaf_begin[src + 1] - p.leaf_begin[src]);
-        }
-        s_pre[ne] = acc;
-    }
+    if (threadIdx.x < 32) near_ranges_warp(p, t, threadIdx.x, s_beg, s_pre);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kAsmThreads / 32;
     for (int base = 0; base < S; base += kAsmTile) {
@@ -117,17 +107,7 @@ __global__ void __launch_bounds__(64) k_near_apply(DevPlan p, const T* __restric
     __shared__ __align__(16) T Ps[2][64][PP];  // [row][k]
     __shared__ __align__(16) T Xs[2][KC][XP];  // [k][col]
     const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
-    const int e0 = p.near_off[t], ne = p.near_off[t + 1] - e0;
-    if (tid == 0) {
-        int acc = 0;
-        for (int e = 0; e < ne; ++e) {
-            const int src = p.near_src[e0 + e];
-            s_beg[e] = p.leaf_begin[src];
-            s_pre[e] = acc;
-            acc += (int)(p.leaf_begin[src + 1] - p.leaf_begin[src]);
-        }
-        s_pre[ne] = acc;
-    }
+    if (tid < 32) near_ranges_warp(p, t, tid, s_beg, s_pre);
     __syncthreads();
     const int nchunk = (Sp + KC - 1) / KC;
     auto gather_ids = [&](int c) {

@@ -39,6 +39,32 @@ struct DevPlan {
     const double* wsrc;       // N x n3 far-field source weights (P2M), set by launch_src_weights
 };
 
+// Source ranges of target leaf t's near list, read by the 32 lanes of one
+// warp in parallel: s_beg[e] = first panel of near leaf e, s_pre[e] = its
+// offset in the concatenated source order (s_pre[ne] = S).  A near list has
+// at most 27 leaves (the leaf and its 26 neighbours).
+__device__ __forceinline__ void near_ranges_warp(const DevPlan& p, int t, int lane, int64_t* s_beg, int32_t* s_pre) {
+    const int e0 = p.near_off[t], ne = p.near_off[t + 1] - e0;
+    int64_t b = 0;
+    int cnt = 0;
+    if (lane < ne) {
+        const int src = p.near_src[e0 + lane];
+        b = p.leaf_begin[src];
+        cnt = (int)(p.leaf_begin[src + 1] - b);
+    }
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane < ne) {
+        s_beg[lane] = b;
+        s_pre[lane] = inc - cnt;
+    }
+    if (lane == ne - 1) s_pre[ne] = inc;
+}
+
 // Wilton near-field block assembly: P (nnz doubles), one CTA per target leaf.
 void launch_near_assemble(Ctx& c, const DevPlan& p, int64_t nnz, double* P, double coef);
 // inv_diag[i] = 1 / P_ii (|P_ii| > 1e-30 else 1), the reference's DiagJacobi.
@@ -59,6 +85,13 @@ struct FarLaunch {
 void launch_near_apply32(Ctx& c, const DevPlan& p, int64_t nnz, const float* P, const float* X, double* Y, int R);
 // b = (float) a
 void launch_to_f32(Ctx& c, const double* a, float* b, int64_t n);
+// b = a rounded to TF32 (round to nearest), stored as FP32.
+void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n);
+// Y = P_near X on the tensor cores (TF32 inputs, FP32 accumulation, FP64 Y),
+// work items of <= 128 rows (it_leaf, it_row0); P holds TF32-rounded values;
+// R a multiple of 4.  *err becomes nonzero if a bounded pipeline wait expired.
+void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, const int32_t* it_leaf,
+                          const int32_t* it_row0, const float* P, const float* X, double* Y, int R, int* err);
 // Far-field source weights W[j][m]: the Chebyshev interpolation weights of
 // panel j's charge in its leaf; quad 0: at the centroid (the reference's
 // point lumping), quad 1: averaged over 2x2 Gauss points of the panel.

@@ -10,6 +10,7 @@
 // classical Gram-Schmidt with one re-orthogonalisation pass (CGS2) instead of
 // modified Gram-Schmidt, which turns k+1 dependent reductions into two.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -91,9 +92,10 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
 struct DevPlanBufs {
     DBuf<double> verts, cent, area, w1d, m2m1d;
     DBuf<int32_t> cond, near_off, near_src, near_S, box_parent, box_octant, m2l_src, m2l_slot, child_first,
-        child_count, leaf_of, item_leaf, item_row0;
+        child_count, leaf_of, item_leaf, item_row0, item128_leaf, item128_row0;
     DBuf<int64_t> leaf_begin, nval_off, m2l_off;
     DBuf<double> leaf_ctr, wsrc;
+    int nitems128 = 0;
     DevPlan v{};
     FarLaunch far{};
 };
@@ -141,6 +143,24 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
         for (int k = 0; k < p.n && k < 8; ++k) v.roots[k] = roots[k];
     }
     v.item_row0 = d.item_row0.p;
+    {
+        // 128-row work items of the tensor-core near apply, largest first so
+        // the last wave of CTAs holds the short items
+        std::vector<std::array<int64_t, 3>> items;
+        for (int64_t k = 0; k < p.nleaf(); ++k) {
+            const int64_t mk = p.leaf_begin[k + 1] - p.leaf_begin[k];
+            for (int64_t r = 0; r < mk; r += 128) items.push_back({std::min<int64_t>(128, mk - r) * p.near_S[k], k, r});
+        }
+        std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a[0] > b[0]; });
+        std::vector<int32_t> il, ir;
+        for (const auto& it : items) {
+            il.push_back((int32_t)it[1]);
+            ir.push_back((int32_t)it[2]);
+        }
+        d.item128_leaf.upload(il, s);
+        d.item128_row0.upload(ir, s);
+        d.nitems128 = (int)il.size();
+    }
     v.n = p.n;
     v.n3 = p.n3;
     v.L = p.L;
@@ -253,6 +273,7 @@ struct Operator {
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
+    int mixed_near = 0;  // 0: TF32 tensor-core near apply, 1: FP32 CUDA cores
     BlockJacobi bj;
     bool factored = false;  // M2L through the low-rank factors (order 4, compressed)
     FacM2L<double> fac64;
@@ -302,15 +323,18 @@ struct Operator {
         }
         if (mixed) {
             P32.alloc((size_t)pl.nnz(), s);
-            launch_to_f32(ctx, P.p, P32.p, pl.nnz());
+            if (mixed_near == 0)
+                launch_to_tf32(ctx, P.p, P32.p, pl.nnz());
+            else
+                launch_to_f32(ctx, P.p, P32.p, pl.nnz());
             X32.alloc((size_t)pl.N * R, s);
+            tc_err.alloc(1, s);
+            tc_err.zero();
             if (has_far()) {
                 Rb32 = (R + 63) / 64 * 64;
                 E32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
                 L32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
                 if (!factored) build_tc_lists(ctx, pl, tc);
-                tc_err.alloc(1, s);
-                tc_err.zero();
             }
         }
     }
@@ -435,7 +459,11 @@ struct Operator {
     // Y = A32 X: FP32 near field, FP32 far field with TF32 tensor-core M2L.
     void apply32(const double* X, double* Y) {
         launch_to_f32(ctx, X, X32.p, pl.N * R);
-        launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
+        if (mixed_near == 0)
+            launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, X32.p, Y,
+                                 R, tc_err.p);
+        else
+            launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
         if (has_far()) {
             M2LLevelFn<float> m2l_fn = [&](int level, int b0, int nb, double scale) {
                 if (factored)
@@ -457,11 +485,11 @@ struct Operator {
     }
 
     void check_tc() {
-        if (!mixed || !has_far()) return;
+        if (!mixed) return;
         int e = 0;
         tc_err.download(&e, 1);
         GPX_CUDA(cudaStreamSynchronize(ctx.stream));
-        if (e) throw Error(GPX_ERR_CUDA, "tensor-core M2L pipeline wait expired");
+        if (e) throw Error(GPX_ERR_CUDA, "tensor-core pipeline wait expired (near apply or M2L)");
     }
 };
 
@@ -624,10 +652,13 @@ Opts normalize(const gpx_solve_opts* o) {
     r.dense_below = o->dense_below == 0 ? 500 : o->dense_below;
     r.precond = o->precond;
     r.skip_ground_rhs = o->skip_ground_rhs;
-    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : 5;
+    // The TF32 near apply perturbs the inner operator by ~2^-11 per entry, so
+    // inner solves past 1e-3 buy little; the FP32 near apply supports 1e-5.
+    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : (o->mixed_near == 0 ? 3 : 5);
     r.mesh_max_edge = o->mesh_max_edge_m;
     r.max_panels = o->max_panels;
     r.far_quad = o->far_quad;
+    r.mixed_near = o->mixed_near;
     return r;
 }
 
@@ -648,6 +679,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
         throw Error(GPX_ERR_INVALID_ARG, "the mixed-precision path runs order-4 expansions");
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
     if (o.precond != 0 && o.precond != 1) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0 or 1");
+    if (o.mixed_near != 0 && o.mixed_near != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -673,6 +705,7 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     upload_plan(ctx, pr.plan, pr.m2l.get(), pr.dp);
     pr.op.reset(new Operator(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get()));
     pr.op->precond = o.precond;
+    pr.op->mixed_near = o.mixed_near;
     pr.op->assemble();
 }
 

@@ -18,6 +18,7 @@ struct Opts {
     double mesh_max_edge = 0.0;
     int64_t max_panels = 0;
     int far_quad = 0;
+    int mixed_near = 0;
 };
 Opts normalize(const gpx_solve_opts* o);
 

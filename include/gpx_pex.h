@@ -67,8 +67,9 @@ const char* gpx_version(void);
 
 typedef enum {
     GPX_PREC_FP64 = 0,  /* plain: every operator apply and all GMRES work in FP64 */
-    GPX_PREC_MIXED = 1  /* FP32 far field (M2L on tensor cores) + FP32 near apply
-                           inside an FP64 iterative-refinement loop */
+    GPX_PREC_MIXED = 1  /* FP32 far field and near apply (TF32 tensor cores for the
+                           near apply and, with exact M2L, for M2L) inside an FP64
+                           iterative-refinement loop */
 } gpx_precision;
 
 typedef enum {
@@ -89,12 +90,14 @@ typedef struct {
     int32_t precond;         /* 0 diagonal Jacobi (fmm_solver.rs:133-162), 1 leaf block-Jacobi */
     int32_t skip_ground_rhs; /* 1: do not solve the substrate column (the reference solves it);
                                 the per-net result needs only the nets' columns */
-    int32_t inner_tol_exp;   /* mixed: floor of the adaptive inner tolerance, 10^-x; 0 -> 5 */
+    int32_t inner_tol_exp;   /* mixed: floor of the adaptive inner tolerance, 10^-x; 0 -> 3 with the
+                                tensor-core near apply, 5 with the FP32 one */
     double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
                                 (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
-    int32_t reserved[7];
+    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05), 1 -> FP32 CUDA cores */
+    int32_t reserved[6];
 } gpx_solve_opts;
 
 typedef struct {

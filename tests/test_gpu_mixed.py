@@ -1,8 +1,9 @@
-"""Mixed-precision path: FP32 near-field apply and FP32 far field with the
-tcgen05 TF32 M2L, inside an FP64 iterative-refinement loop.
+"""Mixed-precision path: near-field apply on the tcgen05 TF32 tensor cores (or
+FP32 CUDA cores, mixed_near=1) and FP32 far field with the tcgen05 TF32 M2L,
+inside an FP64 iterative-refinement loop.
 
 Bars: the FP32/TF32 operator apply is within 1e-3 (norm-wise, per column) of the FP64
-operator (TF32 keeps 10 mantissa bits in the M2L; the near field is FP32);
+operator (TF32 keeps 10 mantissa bits, rounded to nearest);
 the refined Maxwell matrix is within 1e-6 of the plain FP64 solve, because
 the refinement residual is the FP64 operator's."""
 import numpy as np
@@ -27,27 +28,28 @@ def window(nets=12, side=15.0, edge=0.3e-6):
                                 mesh_max_edge_m=edge, max_panels=-1)
 
 
+@pytest.mark.parametrize("mixed_near", [0, 1])
 @pytest.mark.parametrize("nrhs", [3, 64, 100])
-def test_mixed_operator_close_to_fp64(ctx, nrhs):
+def test_mixed_operator_close_to_fp64(ctx, nrhs, mixed_near):
     p = window()
     rng = np.random.default_rng(5)
     sig = rng.standard_normal((len(p["verts"]), nrhs))
     kw = dict(order=4, max_level=5, dense_below=-1, m2l_mode=1)
     y64, rep = ctx.operator_apply(p["verts"], sig, precision=0, **kw)
-    y32, _ = ctx.operator_apply(p["verts"], sig, precision=1, **kw)
+    y32, _ = ctx.operator_apply(p["verts"], sig, precision=1, mixed_near=mixed_near, **kw)
     assert rep["m2l_pairs"] > 0
     for j in range(nrhs):
         e = np.linalg.norm(y32[:, j] - y64[:, j]) / np.linalg.norm(y64[:, j])
         assert e < 1e-3, (j, e)
 
 
-@pytest.mark.parametrize("far_quad", [0, 1])
-def test_mixed_solve_matches_fp64(ctx, far_quad):
+@pytest.mark.parametrize("far_quad,mixed_near", [(0, 0), (1, 0), (1, 1)])
+def test_mixed_solve_matches_fp64(ctx, far_quad, mixed_near):
     p = window()
     nc = len(p["nets"]) + 1
     kw = dict(order=4, max_level=5, dense_below=-1, far_quad=far_quad, skip_ground_rhs=1)
     C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=0, **kw)
-    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, **kw)
+    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, mixed_near=mixed_near, **kw)
     assert r32["converged"] == 1 and r32["outer_iterations"] >= 1
     assert r32["max_rel_residual"] <= 1e-8
     R = nc - 1
