@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--accuracy", type=int, default=1, help="1: report errors against the FP64 all-pairs solve")
     ap.add_argument("--inner-tol-exp", type=int, default=0, help="mixed: inner GMRES tolerance 10^-x (0: default)")
     ap.add_argument("--mixed-near", type=int, default=0, help="mixed near apply: 0 TF32 tensor cores, 1 FP32 CUDA cores")
+    ap.add_argument("--m2l-mode", type=int, default=0, help="0 QR-compressed M2L operators (reference), 1 exact")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     return ap.parse_args()
@@ -255,7 +256,7 @@ def main():
     ctx = _lib.Context(local)
     base_kw = dict(order=args.order, max_level=args.depth, skip_ground_rhs=1, tol=1e-8, restart=args.restart,
                    far_quad=args.far_quad, precond=args.precond, inner_tol_exp=args.inner_tol_exp,
-                   mixed_near=args.mixed_near)
+                   mixed_near=args.mixed_near, m2l_mode=args.m2l_mode)
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     lay = workload(rank, args.nets, args.side)
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
