@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--impl", default="gpx", choices=["gpx", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: time the plain FP64 path, then the mixed path (the headline value)")
-    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--order", type=int, default=5)
     ap.add_argument("--depth", type=int, default=5)
     ap.add_argument("--nets", type=int, default=64)
     ap.add_argument("--side", type=float, default=40.0, help="window side in um")

@@ -48,7 +48,7 @@ class SolveOpts(C.Structure):
         ("tol", C.c_double), ("restart", C.c_int32), ("max_restarts", C.c_int32), ("dense_below", C.c_int32),
         ("precond", C.c_int32), ("skip_ground_rhs", C.c_int32), ("inner_tol_exp", C.c_int32),
         ("mesh_max_edge_m", C.c_double), ("max_panels", C.c_int64), ("far_quad", C.c_int32),
-        ("mixed_near", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("mixed_near", C.c_int32), ("mixed_m2l", C.c_int32), ("reserved", C.c_int32 * 5),
     ]
 
 

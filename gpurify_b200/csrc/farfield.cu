@@ -1,192 +1,318 @@
 // Chebyshev far field (fmm/bbfmm.rs:209-448) for R right-hand sides, in FP64
-// (plain path) or FP32 (mixed path).  Expansions are stored per box as
-// E[box][r][node] (node index fastest): one 64-node row per right-hand side
-// is one contiguous 256 B (FP32) row, which is the K-major operand layout the
-// tensor-core M2L (m2l_tc.cu) reads.
+// (plain path) or FP32 (mixed path), for expansion orders 2 to 6.
+// Expansions are stored per box as E[box][r][node] with a node stride ns =
+// n^3 rounded up to a multiple of 32 (node index fastest, padding nodes zero):
+// one right-hand side's expansion is one contiguous, 128-byte-aligned row,
+// which is also the K-major operand row of the tensor-core M2L (m2l_tc.cu).
 //
 //  P2M  E[leaf][r][m]  = sum_j W_j[m] a_j X[j][r]          (W: source weights)
-//  M2M  E[par][r][.]  += (Mx (x) My (x) Mz) E[child][r][.]  (tensor product, O(n^4))
+//  M2M  E[par][r][.]   = sum_children (Mx (x) My (x) Mz) E[child][r][.]
 //  M2L  L[t][r][m]    += (1/half) sum_s sum_l K_off[m][l] E[s][r][l]
 //  L2L  L[child][r][.] += (Mx (x) My (x) Mz)^T L[par][r][.]
 //  L2P  Y[j][r]       += coef sum_m S(c_j)[m] L[leaf][r][m]  (collocation point)
+//
+// P2M and L2P are register-tiled GEMMs per leaf.  M2M and L2L run one CTA per
+// parent box over all eight octants at once: the 1-D operator of an axis
+// depends only on the child's bit along that axis, so the eight children's
+// contractions share partial sums along a binary tree (z, then y, then x for
+// M2M; the reverse for L2L): 14 n^4 multiply-adds per parent and right-hand
+// side instead of 24 n^4.
 #include "farfield.cuh"
 
 namespace gpx {
 
 namespace {
 
-constexpr int kRC = 8;  // right-hand sides per shared-memory chunk in M2M/L2L
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
 
-// P2M: one CTA per leaf; outputs (r, m) in passes of 256 x 16 held in
-// registers; the leaf's source weights and charges staged 16 panels at a time.
-template <class T>
-__global__ void __launch_bounds__(256) k_p2m_t(DevPlan p, const T* __restrict__ X, T* __restrict__ E, int R,
-                                               int Rb) {
+template <int N>
+struct Ord {
+    static constexpr int n3 = N * N * N;
+    static constexpr int ns = (n3 + 31) & ~31;
+};
+
+// P2M as a GEMM per (leaf, 64-wide chunk of rows r):
+//   E[leaf][r][m] = sum_j W[j][m] * (a_j X[j][r])
+// 256 threads; thread (tm, tr) holds nodes tm + 32 i and rows tr + 8 j.
+// Panels are staged 32 (FP32) or 16 (FP64) at a time.  Every row r < Rb and node m < ns of the
+// chunk is written (zeros outside r < R, m < n3).
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X, const T* __restrict__ W,
+                                             T* __restrict__ E, int R, int Rb) {
+    constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, MI = NS / 32;
+    constexpr int KP = sizeof(T) == 8 ? 16 : 32;  // panels per staged chunk (static shared memory <= 48 KB)
     const int t = blockIdx.x;
-    const int n3 = p.n3;
+    const int rc = blockIdx.y * 64;
     const int64_t j0 = p.leaf_begin[t], j1 = p.leaf_begin[t + 1];
-    T* out = E + (int64_t)(p.leaf_box0 + t) * Rb * n3;
-    __shared__ T Ws[16][217];
-    __shared__ T Qs[16][65];
-    const int nout = R * n3;
-    for (int base = 0; base < nout; base += 256 * 16) {
-        T acc[16];
+    __shared__ T Ws[KP][NS + 1];
+    __shared__ T Qs[KP][65];
+    const int tid = threadIdx.x, tm = tid >> 3, tr = tid & 7;
+    T acc[MI][8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = (T)0;
-        const int rlo = base / n3, rhi = min(R, (base + 256 * 16 + n3 - 1) / n3);
-        for (int r0 = (rlo / 64) * 64; r0 < rhi; r0 += 64) {
-            for (int64_t jb = j0; jb < j1; jb += 16) {
-                const int cnt = (int)min((int64_t)16, j1 - jb);
-                __syncthreads();
-                for (int e = threadIdx.x; e < 16 * n3; e += 256) {
-                    const int jj = e / n3, mm = e % n3;
-                    Ws[jj][mm] = jj < cnt ? (T)p.wsrc[(jb + jj) * n3 + mm] : (T)0;
-                }
-                for (int e = threadIdx.x; e < 16 * 64; e += 256) {
-                    const int jj = e >> 6, rr = e & 63;
-                    Qs[jj][rr] = (jj < cnt && r0 + rr < R) ? (T)p.area[jb + jj] * X[(jb + jj) * R + r0 + rr] : (T)0;
-                }
-                __syncthreads();
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int o = base + threadIdx.x + 256 * q;
-                    const int r = o / n3, mm = o % n3;
-                    if (o < nout && r >= r0 && r < r0 + 64) {
-                        T a = acc[q];
-                        for (int jj = 0; jj < cnt; ++jj) a += Ws[jj][mm] * Qs[jj][r - r0];
-                        acc[q] = a;
-                    }
-                }
+        for (int j = 0; j < 8; ++j) acc[i][j] = (T)0;
+    for (int64_t jb = j0; jb < j1; jb += KP) {
+        const int cnt = (int)min((int64_t)KP, j1 - jb);
+        __syncthreads();
+        for (int e = tid; e < KP * NS; e += 256) {
+            const int k = e / NS, m = e % NS;
+            Ws[k][m] = (k < cnt && m < N3) ? W[(jb + k) * N3 + m] : (T)0;
+        }
+        for (int e = tid; e < KP * 64; e += 256) {
+            const int k = e >> 6, r = e & 63;
+            Qs[k][r] = (k < cnt && rc + r < R) ? (T)p.area[jb + k] * X[(jb + k) * R + rc + r] : (T)0;
+        }
+        __syncthreads();
+        for (int k = 0; k < cnt; ++k) {
+            T a[MI], b[8];
+#pragma unroll
+            for (int i = 0; i < MI; ++i) a[i] = Ws[k][tm + 32 * i];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Qs[k][tr + 8 * j];
+#pragma unroll
+            for (int i = 0; i < MI; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
+        }
+    }
+    T* out = E + ((int64_t)(p.leaf_box0 + t) * Rb + rc) * NS;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int r = tr + 8 * j;
+        if (rc + r >= Rb) continue;
+#pragma unroll
+        for (int i = 0; i < MI; ++i) {
+            const int m = tm + 32 * i;
+            out[(int64_t)r * NS + m] = (m < N3 && rc + r < R) ? acc[i][j] : (T)0;
+        }
+    }
+}
+
+// L2P as a GEMM per (leaf, 64-wide chunk of r):
+//   Y[j][r] += coef * sum_m S_j[m] L[leaf][r][m],  S_j[m] = wx[a] wy[b] wz[c]
+// 256 threads; thread (tj, tr) holds panels tj + 16 i and rows tr + 16 q.
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L, double* __restrict__ Y, int R,
+                                             int Rb, double coef) {
+    constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns;
+    const int t = blockIdx.x;
+    const int rc = blockIdx.y * 64;
+    const int64_t j0 = p.leaf_begin[t], j1 = p.leaf_begin[t + 1];
+    const T* src = L + ((int64_t)(p.leaf_box0 + t) * Rb + rc) * NS;
+    __shared__ T wv[64][3 * N];
+    __shared__ T Ss[64][33];
+    __shared__ T Ls[32][65];
+    const int tid = threadIdx.x, tj = tid >> 4, tr = tid & 15;
+    for (int64_t jb = j0; jb < j1; jb += 64) {
+        const int cnt = (int)min((int64_t)64, j1 - jb);
+        __syncthreads();
+        for (int e = tid; e < 64 * 3 * N; e += 256) {
+            const int jj = e / (3 * N);
+            wv[jj][e % (3 * N)] = jj < cnt ? (T)p.w1d[jb * 3 * N + e] : (T)0;
+        }
+        T acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][q] = (T)0;
+        for (int m0 = 0; m0 < N3; m0 += 32) {
+            __syncthreads();
+            for (int e = tid; e < 64 * 32; e += 256) {
+                const int jj = e >> 5, mm = e & 31, m = m0 + mm;
+                T v = (T)0;
+                if (m < N3) v = wv[jj][m / (N * N)] * wv[jj][N + (m / N) % N] * wv[jj][2 * N + m % N];
+                Ss[jj][mm] = v;
+            }
+            for (int e = tid; e < 32 * 64; e += 256) {
+                const int mm = e & 31, r = e >> 5;
+                Ls[mm][r] = (m0 + mm < N3 && rc + r < R) ? src[(int64_t)r * NS + m0 + mm] : (T)0;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int k = 0; k < 32; ++k) {
+                T a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = Ss[tj + 16 * i][k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) b[q] = Ls[k][tr + 16 * q];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[i][q] += a[i] * b[q];
             }
         }
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int o = base + threadIdx.x + 256 * q;
-            if (o < nout) out[o] = acc[q];
+        for (int i = 0; i < 4; ++i) {
+            const int jj = tj + 16 * i;
+            if (jj >= cnt) continue;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = rc + tr + 16 * q;
+                if (r < R) Y[(jb + jj) * R + r] += coef * (double)acc[i][q];
+            }
         }
     }
 }
 
-// Three 1-D contractions of an (a,b,c) node array along z, y, x.
-// transpose = false: parent from child (M2M), mat[m*n+k], k child node, m parent node.
-// transpose = true : child from parent (L2L).
-template <class T>
-__device__ __forceinline__ void tensor3(const double* mx, const double* my, const double* mz, int n, bool transpose,
-                                        T (*S0)[256], T (*S1)[256], int rc, int n3) {
-    // stage z: S1[r][(a,b,c')] = sum_c Z[c'][c] S0[r][(a,b,c)]
-    for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) {
-        const int r = o / n3, m = o % n3, a = m / (n * n), b = (m / n) % n, cp = m % n;
-        T s = 0;
-        for (int c = 0; c < n; ++c) s += (T)(transpose ? mz[c * n + cp] : mz[cp * n + c]) * S0[r][(a * n + b) * n + c];
-        S1[r][m] = s;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) {
-        const int r = o / n3, m = o % n3, a = m / (n * n), bp = (m / n) % n, cp = m % n;
-        T s = 0;
-        for (int b = 0; b < n; ++b) s += (T)(transpose ? my[b * n + bp] : my[bp * n + b]) * S1[r][(a * n + b) * n + cp];
-        S0[r][m] = s;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) {
-        const int r = o / n3, m = o % n3, ap = m / (n * n), bp = (m / n) % n, cp = m % n;
-        T s = 0;
-        for (int a = 0; a < n; ++a) s += (T)(transpose ? mx[a * n + ap] : mx[ap * n + a]) * S0[r][(a * n + bp) * n + cp];
-        S1[r][m] = s;
-    }
-    __syncthreads();
+// Rows of right-hand sides per M2M / L2L block.
+template <class T, int N>
+constexpr int tree_rc() {
+    return (sizeof(T) == 8 && N >= 6) ? 4 : 8;
+}
+template <class T, int N>
+constexpr size_t tree_smem() {
+    return sizeof(T) * (size_t)(8 + 4 + 2) * tree_rc<T, N>() * Ord<N>::n3;
 }
 
-// M2M: CTA per parent box; children are contiguous (Morton order).
-template <class T>
-__global__ void __launch_bounds__(256) k_m2m_t(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
-                                               const int32_t* __restrict__ child_count, T* __restrict__ E, int R,
-                                               int Rb) {
+// 1-D operators of the three axes as T: M1[axis][bit][m][k] (m parent node,
+// k child node), from the plan's per-octant table mat[(o*3+axis)*n*n + m*n + k].
+template <class T, int N>
+__device__ __forceinline__ void load_m1(const double* m2m1d, T (*M1)[2][N * N]) {
+    for (int e = threadIdx.x; e < 3 * 2 * N * N; e += blockDim.x) {
+        const int axis = e / (2 * N * N), bit = (e / (N * N)) & 1, mk = e % (N * N);
+        const int oct = bit << axis;  // any octant with this bit on this axis
+        M1[axis][bit][mk] = (T)m2m1d[(oct * 3 + axis) * N * N + mk];
+    }
+}
+
+// M2M, one CTA per (parent box, chunk of RC rows r); children are contiguous
+// (Morton order).  A[oct] holds the child of octant oct (zero if absent);
+// B[q] = sum_oz Z_oz A[q | oz<<2] (q = ox | oy<<1); C[ox] = sum_oy Y_oy B;
+// E_par = sum_ox X_ox C[ox].  The parent row is overwritten (the parent has
+// no other contribution), padding nodes written as zero.
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_m2m_tree(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
+                                                  const int32_t* __restrict__ child_count, T* __restrict__ E, int Rb) {
+    constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>(), NN = N * N;
     const int pb = pb0 + blockIdx.x;
-    const int n = p.n, n3 = p.n3;
-    __shared__ T S0[kRC][256], S1[kRC][256], A[kRC][256];
+    const int r0 = blockIdx.y * RC;
+    const int rc = min(RC, Rb - r0);
+    extern __shared__ __align__(16) unsigned char tree_smem_raw[];
+    T* A = reinterpret_cast<T*>(tree_smem_raw);  // [8][RC][N3]
+    T* B = A + 8 * RC * N3;                      // [4][RC][N3]
+    T* C = B + 4 * RC * N3;                      // [2][RC][N3]
+    __shared__ T M1[3][2][NN];
+    load_m1<T, N>(p.m2m1d, M1);
     const int cf = child_first[pb], cc = child_count[pb];
-    for (int r0 = 0; r0 < R; r0 += kRC) {
-        const int rc = min(kRC, R - r0);
-        for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) A[o / n3][o % n3] = 0;
-        for (int ch = cf; ch < cf + cc; ++ch) {
-            __syncthreads();
-            const T* src = E + ((int64_t)ch * Rb + r0) * n3;
-            for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) S0[o / n3][o % n3] = src[o];
-            __syncthreads();
-            const int oc = p.box_octant[ch];
-            tensor3<T>(p.m2m1d + (oc * 3 + 0) * n * n, p.m2m1d + (oc * 3 + 1) * n * n, p.m2m1d + (oc * 3 + 2) * n * n,
-                       n, false, S0, S1, rc, n3);
-            for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) A[o / n3][o % n3] += S1[o / n3][o % n3];
+    for (int e = threadIdx.x; e < 8 * RC * N3; e += blockDim.x) A[e] = (T)0;
+    __syncthreads();
+    for (int ch = cf; ch < cf + cc; ++ch) {
+        const int oc = p.box_octant[ch];
+        const T* src = E + ((int64_t)ch * Rb + r0) * NS;
+        for (int e = threadIdx.x; e < rc * N3; e += blockDim.x) {
+            const int r = e / N3, m = e % N3;
+            A[(oc * RC + r) * N3 + m] = src[(int64_t)r * NS + m];
         }
-        __syncthreads();
-        T* dst = E + ((int64_t)pb * Rb + r0) * n3;
-        for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) dst[o] += A[o / n3][o % n3];
-        __syncthreads();
-    }
-}
-
-// L2L: CTA per child box.
-template <class T>
-__global__ void __launch_bounds__(256) k_l2l_t(DevPlan p, int cb0, T* __restrict__ L, int R, int Rb) {
-    const int cb = cb0 + blockIdx.x;
-    const int n = p.n, n3 = p.n3;
-    __shared__ T S0[kRC][256], S1[kRC][256];
-    const int pb = p.box_parent[cb], oc = p.box_octant[cb];
-    for (int r0 = 0; r0 < R; r0 += kRC) {
-        const int rc = min(kRC, R - r0);
-        __syncthreads();
-        const T* src = L + ((int64_t)pb * Rb + r0) * n3;
-        for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) S0[o / n3][o % n3] = src[o];
-        __syncthreads();
-        tensor3<T>(p.m2m1d + (oc * 3 + 0) * n * n, p.m2m1d + (oc * 3 + 1) * n * n, p.m2m1d + (oc * 3 + 2) * n * n, n,
-                   true, S0, S1, rc, n3);
-        T* dst = L + ((int64_t)cb * Rb + r0) * n3;
-        for (int o = threadIdx.x; o < rc * n3; o += blockDim.x) dst[o] += S1[o / n3][o % n3];
-    }
-}
-
-// L2P: one CTA per (leaf, chunk of 16 right-hand sides): the leaf's local
-// expansion rows staged in shared memory, one thread per (panel, rhs).
-template <class T>
-__global__ void __launch_bounds__(256) k_l2p_t(DevPlan p, const T* __restrict__ L, double* __restrict__ Y, int R,
-                                               int Rb, double coef) {
-    const int t = blockIdx.x;
-    const int rc = blockIdx.y * 16;
-    const int n = p.n, n3 = p.n3;
-    const int64_t j0 = p.leaf_begin[t], j1 = p.leaf_begin[t + 1];
-    __shared__ T Ls[16][217];
-    const T* src = L + ((int64_t)(p.leaf_box0 + t) * Rb + rc) * n3;
-    for (int e = threadIdx.x; e < 16 * n3; e += 256) {
-        const int rr = e / n3, mm = e % n3;
-        Ls[rr][mm] = rc + rr < R ? src[(int64_t)rr * n3 + mm] : (T)0;
     }
     __syncthreads();
-    const int rr = threadIdx.x & 15;
-    for (int64_t j = j0 + (threadIdx.x >> 4); j < j1; j += 16) {
-        if (rc + rr >= R) continue;
-        const double* w = p.w1d + j * 3 * n;
-        T wz[8];
-        for (int c = 0; c < n; ++c) wz[c] = (T)w[2 * n + c];
-        T acc = 0;
-        for (int a = 0; a < n; ++a)
-            for (int b = 0; b < n; ++b) {
-                const T wab = (T)(w[a] * w[n + b]);
-                const T* row = &Ls[rr][(a * n + b) * n];
-                T s = 0;
-                for (int c = 0; c < n; ++c) s += wz[c] * row[c];
-                acc += wab * s;
-            }
-        Y[j * R + rc + rr] += coef * (double)acc;
+    // z: B[q][r][(a,b,c')] = sum_oz sum_c Z_oz[c'][c] A[q|oz<<2][r][(a,b,c)]
+    for (int e = threadIdx.x; e < 4 * RC * N3; e += blockDim.x) {
+        const int q = e / (RC * N3), r = (e / N3) % RC, m = e % N3, ab = m / N, cp = m % N;
+        const T* a0 = A + (q * RC + r) * N3 + ab * N;
+        const T* a1 = A + ((q | 4) * RC + r) * N3 + ab * N;
+        T s = (T)0;
+#pragma unroll
+        for (int c = 0; c < N; ++c) s += M1[2][0][cp * N + c] * a0[c] + M1[2][1][cp * N + c] * a1[c];
+        B[e] = s;
+    }
+    __syncthreads();
+    // y: C[ox][r][(a,b',c)] = sum_oy sum_b Y_oy[b'][b] B[ox|oy<<1][r][(a,b,c)]
+    for (int e = threadIdx.x; e < 2 * RC * N3; e += blockDim.x) {
+        const int ox = e / (RC * N3), r = (e / N3) % RC, m = e % N3, a = m / NN, bp = (m / N) % N, c = m % N;
+        const T* b0 = B + (ox * RC + r) * N3 + a * NN + c;
+        const T* b1 = B + ((ox | 2) * RC + r) * N3 + a * NN + c;
+        T s = (T)0;
+#pragma unroll
+        for (int b = 0; b < N; ++b) s += M1[1][0][bp * N + b] * b0[b * N] + M1[1][1][bp * N + b] * b1[b * N];
+        C[e] = s;
+    }
+    __syncthreads();
+    // x: E_par[r][(a',b,c)] = sum_ox sum_a X_ox[a'][a] C[ox][r][(a,b,c)]
+    T* dst = E + ((int64_t)pb * Rb + r0) * NS;
+    for (int e = threadIdx.x; e < rc * NS; e += blockDim.x) {
+        const int r = e / NS, m = e % NS;
+        T s = (T)0;
+        if (m < N3) {
+            const int ap = m / NN, bc = m % NN;
+            const T* c0 = C + r * N3 + bc;
+            const T* c1 = C + (RC + r) * N3 + bc;
+#pragma unroll
+            for (int a = 0; a < N; ++a) s += M1[0][0][ap * N + a] * c0[a * NN] + M1[0][1][ap * N + a] * c1[a * NN];
+        }
+        dst[(int64_t)r * NS + m] = s;
     }
 }
 
-// FP64 M2L: CTA per target box, 64 (m) x 64 (r) tile, 4x4 register tile per
-// thread, operator and source tiles of 32 along the contraction in shared memory.
+// L2L, one CTA per (parent box, chunk of RC rows r): the transposed tree.
+// C[ox] = X_ox^T L_par; B[ox|oy<<1] = Y_oy^T C[ox]; child of octant oct:
+// L_child += Z_oz^T B[oct & 3].
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_l2l_tree(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
+                                                  const int32_t* __restrict__ child_count, T* __restrict__ L, int Rb) {
+    constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>(), NN = N * N;
+    const int pb = pb0 + blockIdx.x;
+    const int r0 = blockIdx.y * RC;
+    const int rc = min(RC, Rb - r0);
+    extern __shared__ __align__(16) unsigned char tree_smem_raw[];
+    T* P = reinterpret_cast<T*>(tree_smem_raw);  // [RC][N3]
+    T* B = P + 8 * RC * N3;                      // [4][RC][N3]
+    T* C = B + 4 * RC * N3;                      // [2][RC][N3]
+    __shared__ T M1[3][2][NN];
+    load_m1<T, N>(p.m2m1d, M1);
+    const T* src = L + ((int64_t)pb * Rb + r0) * NS;
+    for (int e = threadIdx.x; e < RC * N3; e += blockDim.x) {
+        const int r = e / N3, m = e % N3;
+        P[e] = r < rc ? src[(int64_t)r * NS + m] : (T)0;
+    }
+    __syncthreads();
+    // x: C[ox][r][(a,b,c)] = sum_a' X_ox[a'][a] P[r][(a',b,c)]
+    for (int e = threadIdx.x; e < 2 * RC * N3; e += blockDim.x) {
+        const int ox = e / (RC * N3), r = (e / N3) % RC, m = e % N3, a = m / NN, bc = m % NN;
+        const T* pr = P + r * N3 + bc;
+        T s = (T)0;
+#pragma unroll
+        for (int ap = 0; ap < N; ++ap) s += M1[0][ox][ap * N + a] * pr[ap * NN];
+        C[e] = s;
+    }
+    __syncthreads();
+    // y: B[q][r][(a,b,c)] = sum_b' Y_oy[b'][b] C[ox][r][(a,b',c)],  q = ox | oy<<1
+    for (int e = threadIdx.x; e < 4 * RC * N3; e += blockDim.x) {
+        const int q = e / (RC * N3), r = (e / N3) % RC, m = e % N3, a = m / NN, b = (m / N) % N, c = m % N;
+        const T* cr = C + ((q & 1) * RC + r) * N3 + a * NN + c;
+        const int oy = q >> 1;
+        T s = (T)0;
+#pragma unroll
+        for (int bp = 0; bp < N; ++bp) s += M1[1][oy][bp * N + b] * cr[bp * N];
+        B[e] = s;
+    }
+    __syncthreads();
+    // z, straight into each existing child: L_child[r][(a,b,c)] += sum_c' Z_oz[c'][c] B[oct&3][r][(a,b,c')]
+    const int cf = child_first[pb], cc = child_count[pb];
+    for (int ch = cf; ch < cf + cc; ++ch) {
+        const int oc = p.box_octant[ch], q = oc & 3, oz = oc >> 2;
+        T* dst = L + ((int64_t)ch * Rb + r0) * NS;
+        for (int e = threadIdx.x; e < rc * N3; e += blockDim.x) {
+            const int r = e / N3, m = e % N3, ab = m / N, c = m % N;
+            const T* br = B + (q * RC + r) * N3 + ab * N;
+            T s = (T)0;
+#pragma unroll
+            for (int cp = 0; cp < N; ++cp) s += M1[2][oz][cp * N + c] * br[cp];
+            dst[(int64_t)r * NS + m] += s;
+        }
+    }
+}
+
+// FP64 M2L with dense operators: CTA per target box, 64 (m) x 64 (r) tile,
+// 4x4 register tile per thread, operator and source tiles of 32 along the
+// contraction in shared memory.  K table: 343 x n3 x n3; E, L: node stride ns.
 __global__ void __launch_bounds__(256) k_m2l64(DevPlan p, int b0, double* __restrict__ L, const double* __restrict__ E,
                                                int R, double scale) {
     const int tb = b0 + blockIdx.x;
-    const int n3 = p.n3;
+    const int n3 = p.n3, ns = p.ns;
     __shared__ double Ks[32][65];  // [l][m]
     __shared__ double Ms[32][65];  // [l][r]
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -201,13 +327,13 @@ __global__ void __launch_bounds__(256) k_m2l64(DevPlan p, int b0, double* __rest
                 for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
             for (int64_t e = s0; e < s1; ++e) {
                 const double* K = p.m2l_K + (int64_t)p.m2l_slot[e] * n3 * n3;
-                const double* Es = E + (int64_t)p.m2l_src[e] * R * n3;
+                const double* Es = E + (int64_t)p.m2l_src[e] * R * ns;
                 for (int lc = 0; lc < n3; lc += 32) {
                     __syncthreads();
                     for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
                         const int a = idx >> 5, b = idx & 31;  // a: m or r (64), b: l (32)
                         Ks[b][a] = (mc + a < n3 && lc + b < n3) ? K[(int64_t)(mc + a) * n3 + lc + b] : 0.0;
-                        Ms[b][a] = (rcn + a < R && lc + b < n3) ? Es[(int64_t)(rcn + a) * n3 + lc + b] : 0.0;
+                        Ms[b][a] = (rcn + a < R && lc + b < n3) ? Es[(int64_t)(rcn + a) * ns + lc + b] : 0.0;
                     }
                     __syncthreads();
 #pragma unroll 4
@@ -229,28 +355,24 @@ __global__ void __launch_bounds__(256) k_m2l64(DevPlan p, int b0, double* __rest
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int mm = mc + ty + 16 * i, rr = rcn + tx + 16 * j;
-                    if (mm < n3 && rr < R) L[((int64_t)tb * R + rr) * n3 + mm] += scale * acc[i][j];
+                    if (mm < n3 && rr < R) L[((int64_t)tb * R + rr) * ns + mm] += scale * acc[i][j];
                 }
         }
     }
 }
 
-__device__ __forceinline__ void cp16(void* dst, const void* src, bool valid) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
-}
-
-// Factored M2L for low-rank (compressed) order-4 operators K_o = U_o Vt_o, in
-// two GEMM phases per level:
-//   phase 1, CTA per source box s: for every column c = (pair e, k) of the
+// Factored M2L for low-rank (compressed) operators K_o = U_o Vt_o, in two
+// GEMM phases per level:
+//   phase 1, per source box s: for every column c = (pair e, k) of the
 //     source's outgoing pairs, T[t_e][r][col(e,k)] = sum_l E_s[r][l] Vt_o[k][l];
-//   phase 2, CTA per target box t: L_t[r][m] += scale * sum_c T_t[r][c] Ut[c][m],
+//   phase 2, per target box t: L_t[r][m] += scale * sum_c T_t[r][c] Ut[c][m],
 //     the contraction running over the concatenated ranks of t's pairs.
 // T is stored target-major (R rows x Kp_t columns per target, Kp_t = the
 // summed ranks rounded up to 4) so phase 2 reads contiguous rows.
-// Phase 1 as a transposed GEMM per work item (source box, up to 64 of its
-// columns): C[c][r] = sum_l Vt_c[l] E_s[r][l].  The 64 gathered Vt rows (A)
-// stream through a cp.async double buffer; E_s^T (B) is staged once.
+// Phase 1 as a transposed GEMM per work item (source box, up to
+// kFacItemCols of its columns): C[c][r] = sum_l Vt_c[l] E_s[r][l].  E_s^T (B)
+// is staged once per item; the gathered Vt rows (A) of each 64-column
+// sub-block stream through a cp.async double buffer over the ns nodes.
 template <class T>
 __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __restrict__ item_src,
                                                   const int64_t* __restrict__ item_c0,
@@ -260,18 +382,25 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
     constexpr int KC = 128 / sizeof(T);
     constexpr int PP = KC + V;
     constexpr int BP = 64 + V;
+    const int ns = f.ns;
     const int it = blockIdx.x;
     const int rc = blockIdx.y * 64;
     const int s = item_src[it];
-    const int64_t c0 = item_c0[it];
-    const int nc = item_cnt[it];
+    const int64_t cbase = item_c0[it];
+    const int ncols = item_cnt[it];
     const int rows = min(64, R - rc);
     extern __shared__ __align__(16) unsigned char fac_smem[];
     T(*As)[64][PP] = reinterpret_cast<T(*)[64][PP]>(fac_smem);                        // [2][64][PP]: [c][l]
-    T(*Bs)[BP] = reinterpret_cast<T(*)[BP]>(fac_smem + sizeof(T) * 2 * 64 * PP);      // [64][BP]:  [l][r]
+    T(*Bs)[BP] = reinterpret_cast<T(*)[BP]>(fac_smem + sizeof(T) * 2 * 64 * PP);      // [ns][BP]:  [l][r]
     const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
-    auto issue = [&](int ch) {
-        const int k0 = ch * KC, buf = ch & 1;
+    const int nch = ns / KC;                      // node chunks per sub-block
+    const int nsub = (ncols + 63) / 64;           // 64-column sub-blocks
+    const int nsteps = nsub * nch;
+    auto issue = [&](int step) {
+        const int sub = step / nch, ch = step % nch;
+        const int64_t c0 = cbase + 64 * sub;
+        const int nc = min(64, ncols - 64 * sub);
+        const int k0 = ch * KC, buf = step & 1;
 #pragma unroll
         for (int q = 0; q < KC / V; ++q) {
             const int id = tid + 64 * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
@@ -281,27 +410,29 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     issue(0);
-    const T* Es = E + ((int64_t)s * R + rc) * 64;
-    for (int e = tid; e < 64 * 64; e += 64) {
-        const int r = e >> 6, l = e & 63;
-        Bs[l][r] = r < rows ? Es[(int64_t)r * 64 + l] : (T)0;
+    const T* Es = E + ((int64_t)s * R + rc) * ns;
+    for (int e = tid; e < 64 * ns; e += 64) {
+        const int r = e / ns, l = e % ns;
+        Bs[l][r] = r < rows ? Es[(int64_t)r * ns + l] : (T)0;
     }
     T acc[8][8];
+    for (int step = 0; step < nsteps; ++step) {
+        const int sub = step / nch, ch = step % nch;
+        if (ch == 0) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = (T)0;
-    constexpr int nch = 64 / KC;
-    for (int ch = 0; ch < nch; ++ch) {
+                for (int j = 0; j < 8; ++j) acc[i][j] = (T)0;
+        }
         __syncthreads();
-        if (ch + 1 < nch) {
-            issue(ch + 1);
+        if (step + 1 < nsteps) {
+            issue(step + 1);
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         } else {
             asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
-        const int buf = ch & 1;
+        const int buf = step & 1;
 #pragma unroll 4
         for (int kk = 0; kk < KC; ++kk) {
             T a[8], b[8];
@@ -314,30 +445,37 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
 #pragma unroll
                 for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
         }
-    }
+        if (ch == nch - 1) {
+            const int64_t c0 = cbase + 64 * sub;
+            const int nc = min(64, ncols - 64 * sub);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int c = ty + 8 * i;
-        if (c >= nc) continue;
-        const int tg = f.col_tgt[c0 + c];
-        const int ld = (int)((f.tgt_col_off[tg + 1] - f.tgt_col_off[tg] + 3) & ~int64_t(3));
-        T* dst = f.Tm + f.tgt_base[tg] * R + (int64_t)rc * ld + f.col_pos[c0 + c];
+            for (int i = 0; i < 8; ++i) {
+                const int c = ty + 8 * i;
+                if (c >= nc) continue;
+                const int tg = f.col_tgt[c0 + c];
+                const int ld = (int)((f.tgt_col_off[tg + 1] - f.tgt_col_off[tg] + 3) & ~int64_t(3));
+                T* dst = f.Tm + f.tgt_base[tg] * R + (int64_t)rc * ld + f.col_pos[c0 + c];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int r = tx + 8 * j;
-            if (r < rows) dst[(int64_t)r * ld] = acc[i][j];
+                for (int j = 0; j < 8; ++j) {
+                    const int r = tx + 8 * j;
+                    if (r < rows) dst[(int64_t)r * ld] = acc[i][j];
+                }
+            }
         }
     }
 }
 
+// Phase 2: CTA per (target box, 64 rows r, 64 nodes m).
 template <class T>
 __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __restrict__ L, int R, double scale) {
     constexpr int V = 16 / sizeof(T);
     constexpr int KC = 128 / sizeof(T);
     constexpr int PP = KC + V;
     constexpr int XP = 64 + V;
+    const int ns = f.ns;
     const int t = b0 + blockIdx.x;
     const int rc = blockIdx.y * 64;
+    const int m0 = blockIdx.z * 64;
     const int64_t k0g = f.tgt_col_off[t], K = f.tgt_col_off[t + 1] - k0g;
     if (K == 0) return;
     const int Kp = (int)((K + 3) & ~int64_t(3));
@@ -358,8 +496,9 @@ __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
 #pragma unroll
         for (int q = 0; q < KC / V; ++q) {
             const int id = tid + 64 * q, kk = id / (64 / V), cc = (id % (64 / V)) * V;
-            const bool ok = k0 + kk < K;
-            cp16(&Bs[buf][kk][cc], ok ? (const void*)(f.Ut + f.tgt_ut[k0g + k0 + kk] + cc) : (const void*)f.Ut, ok);
+            const bool ok = k0 + kk < K && m0 + cc < ns;
+            cp16(&Bs[buf][kk][cc], ok ? (const void*)(f.Ut + f.tgt_ut[k0g + k0 + kk] + m0 + cc) : (const void*)f.Ut,
+                 ok);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -398,7 +537,9 @@ __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
         if (r >= m) continue;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            T* dst = L + ((int64_t)t * R + rc + r) * 64 + tx + 8 * j;
+            const int mm = m0 + tx + 8 * j;
+            if (mm >= ns) continue;
+            T* dst = L + ((int64_t)t * R + rc + r) * ns + mm;
             *dst += (T)scale * acc[i][j];
         }
     }
@@ -406,27 +547,32 @@ __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
-}  // namespace
-
-template <class T>
-void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, double* Y, int R, int Rb, T* E,
-                      T* L, double coef, const M2LLevelFn<T>& m2l) {
+template <class T, int N>
+void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const T* W, double* Y, int R, int Rb,
+                 T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
     cudaStream_t s = c.stream;
-    const int n = p.n, n3 = p.n3, Lv = p.L;
-    const double box_bytes = (double)sizeof(T) * n3 * R;
-    GPX_CUDA(cudaMemsetAsync(E, 0, (size_t)p.nbox * n3 * Rb * sizeof(T), s));
-    GPX_CUDA(cudaMemsetAsync(L, 0, (size_t)p.nbox * n3 * Rb * sizeof(T), s));
+    constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>();
+    constexpr size_t smem = tree_smem<T, N>();
+    const int Lv = p.L;
+    const double w = (double)sizeof(T);
+    const double box_bytes = w * N3 * R;
+    const unsigned rchunks64 = cdiv(Rb, 64), rchunks_tree = cdiv(Rb, RC);
+    GPX_CUDA(cudaMemsetAsync(L, 0, (size_t)p.nbox * NS * Rb * sizeof(T), s));
     {
-        KTimer t(c, K_P2M, (double)p.N * (8.0 * R + 8.0 * n3 + 8.0) + p.nleaf * box_bytes, 2.0 * (double)p.N * n3 * R);
-        k_p2m_t<T><<<p.nleaf, 256, 0, s>>>(p, X, E, R, Rb);
+        KTimer t(c, K_P2M, (double)p.N * (w * R + w * N3 + 8.0) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
+        k_p2m<T, N><<<dim3(p.nleaf, rchunks64), 256, 0, s>>>(p, X, W, E, R, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
+    }
+    if (smem > 48 * 1024) {
+        GPX_CUDA(cudaFuncSetAttribute(k_m2m_tree<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        GPX_CUDA(cudaFuncSetAttribute(k_l2l_tree<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
     for (int l = Lv; l >= 3; --l) {
         const int pb0 = f.lvl_off[l - 1], npb = f.lvl_off[l] - pb0, nch = f.lvl_off[l + 1] - f.lvl_off[l];
         if (npb == 0) continue;
-        KTimer t(c, K_M2M, (double)(npb + nch) * box_bytes, 2.0 * 3.0 * n * n3 * R * (double)nch);
-        k_m2m_t<T><<<npb, 256, 0, s>>>(p, pb0, f.child_first, f.child_count, E, R, Rb);
+        KTimer t(c, K_M2M, (double)(npb + nch) * box_bytes, 2.0 * 14.0 * N * N3 * R * (double)npb);
+        k_m2m_tree<T, N><<<dim3(npb, rchunks_tree), 256, smem, s>>>(p, pb0, f.child_first, f.child_count, E, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
@@ -435,23 +581,38 @@ void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, 
         if (nb == 0) continue;
         const double pairs = (double)(f.m2l_off[b0 + nb] - f.m2l_off[b0]);
         if (pairs == 0) continue;
-        KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)n3 * n3 * R * pairs);
+        KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
         m2l(l, b0, nb, 1.0 / f.lvl_half[l]);
         c.launches += 1;
     }
     for (int l = 2; l < Lv; ++l) {
-        const int cb0 = f.lvl_off[l + 1], ncb = f.lvl_off[l + 2] - cb0, npb = f.lvl_off[l + 1] - f.lvl_off[l];
+        const int pb0 = f.lvl_off[l], npb = f.lvl_off[l + 1] - pb0, ncb = f.lvl_off[l + 2] - f.lvl_off[l + 1];
         if (ncb == 0) continue;
-        KTimer t(c, K_L2L, (double)(npb + 2 * ncb) * box_bytes, 2.0 * 3.0 * n * n3 * R * (double)ncb);
-        k_l2l_t<T><<<ncb, 256, 0, s>>>(p, cb0, L, R, Rb);
+        KTimer t(c, K_L2L, (double)(npb + 2 * ncb) * box_bytes, 2.0 * 14.0 * N * N3 * R * (double)npb);
+        k_l2l_tree<T, N><<<dim3(npb, rchunks_tree), 256, smem, s>>>(p, pb0, f.child_first, f.child_count, L, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
     {
-        KTimer t(c, K_L2P, (double)p.N * (16.0 * R + 24.0 * n) + p.nleaf * box_bytes, 2.0 * (double)p.N * n3 * R);
-        k_l2p_t<T><<<dim3(p.nleaf, cdiv(R, 16)), 256, 0, s>>>(p, L, Y, R, Rb, coef);
+        KTimer t(c, K_L2P, (double)p.N * (16.0 * R + 24.0 * N) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
+        k_l2p<T, N><<<dim3(p.nleaf, cdiv(R, 64)), 256, 0, s>>>(p, L, Y, R, Rb, coef);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
+    }
+}
+
+}  // namespace
+
+template <class T>
+void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const T* W, double* Y, int R, int Rb,
+                      T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
+    switch (p.n) {
+        case 2: far_field_n<T, 2>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
+        case 3: far_field_n<T, 3>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
+        case 4: far_field_n<T, 4>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
+        case 5: far_field_n<T, 5>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
+        case 6: far_field_n<T, 6>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
+        default: throw Error(GPX_ERR_INVALID_ARG, "far field runs Chebyshev orders 2 to 6");
     }
 }
 
@@ -459,14 +620,14 @@ template <class T>
 void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int nb, T* L, const T* E, int R,
                     double scale) {
     constexpr int V = 16 / sizeof(T), KC = 128 / sizeof(T);
-    const int smem = (int)(sizeof(T) * (2 * 64 * (KC + V) + 64 * (64 + V)));
+    const int smem = (int)(sizeof(T) * (2 * 64 * (KC + V) + f.ns * (64 + V)));
     if (lv.nitems > 0) {
         GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_v<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         k_m2l_fac_v<T><<<dim3(lv.nitems, cdiv(R, 64)), 64, smem, c.stream>>>(f, lv.item_src, lv.item_c0, lv.item_cnt,
                                                                               E, R);
     }
     GPX_LAUNCH_CHECK();
-    k_m2l_fac_u<T><<<dim3(nb, cdiv(R, 64)), 64, 0, c.stream>>>(f, b0, L, R, scale);
+    k_m2l_fac_u<T><<<dim3(nb, cdiv(R, 64), cdiv(f.ns, 64)), 64, 0, c.stream>>>(f, b0, L, R, scale);
     GPX_LAUNCH_CHECK();
     c.launches += 1;  // the caller counts the other one
 }
@@ -480,9 +641,9 @@ void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const dou
     GPX_LAUNCH_CHECK();
 }
 
-template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*, double*, int, int,
-                                       double*, double*, double, const M2LLevelFn<double>&);
-template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, double*, int, int,
-                                      float*, float*, double, const M2LLevelFn<float>&);
+template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*, const double*, double*,
+                                       int, int, double*, double*, double, const M2LLevelFn<double>&);
+template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, const float*, double*, int,
+                                      int, float*, float*, double, const M2LLevelFn<float>&);
 
 }  // namespace gpx

@@ -10,22 +10,26 @@ namespace gpx {
 template <class T>
 using M2LLevelFn = std::function<void(int, int, int, double)>;
 
-// Y += coef * far-field potential of X (N x R, type T), expansions E and L of
-// type T (nbox x Rb x n3 each with Rb >= R rows per box, zeroed here), M2L
-// supplied per level.
+// Y += coef * far-field potential of X (N x R, type T).  W: N x n3 source
+// weights (type T).  Expansions E and L: nbox x Rb x ns each (Rb >= R rows per
+// box, node stride ns); E is written in full by P2M and M2M (zero padding
+// rows and nodes), L is zeroed here.  M2L is supplied per level.
 template <class T>
-void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, double* Y, int R, int Rb, T* E,
-                      T* L, double coef, const M2LLevelFn<T>& m2l);
+void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const T* W, double* Y, int R, int Rb,
+                      T* E, T* L, double coef, const M2LLevelFn<T>& m2l);
 
 // FP64 M2L of one level with CUDA-core FMAs (dense operators).
 void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale);
 
-// Factored M2L data (order 4, 64 nodes): low-rank factors of every offset,
-// per-source column lists for phase 1 and per-target B-row lists for phase 2.
+// Factored M2L data (orders 4-6, ranks <= kFacMaxRank): low-rank factors of
+// every offset, per-source column lists for phase 1 and per-target B-row lists
+// for phase 2.
+constexpr int kFacMaxRank = 32;
 template <class T>
 struct FacM2L {
-    const T* Vt = nullptr;              // 343 x 64 x 64, row k of slot o = Vt_o[k][:]
-    const T* Ut = nullptr;              // 343 x 64 x 64, row k of slot o = U_o[:][k]
+    int ns = 64;                        // node stride
+    const T* Vt = nullptr;              // 343 x 32 x ns, row k of slot o = Vt_o[k][:]
+    const T* Ut = nullptr;              // 343 x 32 x ns, row k of slot o = U_o[:][k]
     const int64_t* src_col_off = nullptr;  // nbox + 1: phase-1 columns of each source box
     const int64_t* col_vt = nullptr;    // per column: offset of its Vt row
     const int32_t* col_tgt = nullptr;   // per column: target box
@@ -35,7 +39,8 @@ struct FacM2L {
     const int64_t* tgt_base = nullptr;  // nbox: sum of padded block widths of earlier boxes
     T* Tm = nullptr;                    // target-major intermediate (R rows x Kp per target)
 };
-// Phase-1 work items of one level: (source box, first column, column count <= 64).
+// Phase-1 work items of one level: (source box, first column, column count <= kFacItemCols).
+constexpr int kFacItemCols = 512;
 struct FacLevel {
     int nitems = 0;
     const int32_t* item_src = nullptr;
@@ -57,10 +62,11 @@ struct TcLevel {
     const int32_t* srcA = nullptr;      // per entry: source box of the first target or -1
     const int32_t* srcB = nullptr;      // per entry: source box of the second target or -1
 };
-// L[t][r][m] = scale * sum K[m][l] E[s][r][l] for order-4 expansions (64
-// nodes), R a multiple of 64.  err receives a nonzero code if a bounded wait
-// on the tensor-core pipeline expired.
-void launch_m2l_tc(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale,
+// L[t][r][m] = scale * sum K[m][l] E[s][r][l] for order-4 (node stride 64)
+// or order-5 (node stride 128) expansions; K32: 343 x ns x ns TF32-rounded
+// operators; R a multiple of 64.  err receives a nonzero code if a bounded
+// wait on the tensor-core pipeline expired.
+void launch_m2l_tc(Ctx& c, const TcLevel& lv, int ns, const float* E, float* L, const float* K32, int R, float scale,
                    int* err);
 
 }  // namespace gpx

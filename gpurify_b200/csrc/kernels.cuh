@@ -11,6 +11,7 @@ namespace gpx {
 // Device pointers of one uploaded plan (all arrays in leaf-sorted order).
 struct DevPlan {
     int n, n3, L;
+    int ns;                   // node stride of one expansion row: n3 rounded up to a multiple of 32
     int64_t N;
     int32_t nleaf, nbox, leaf_box0, nitems;
     const double* verts;      // 12 per panel
@@ -71,6 +72,11 @@ void launch_near_assemble(Ctx& c, const DevPlan& p, int64_t nnz, double* P, doub
 void launch_diag_inv(Ctx& c, const DevPlan& p, const double* P, double* inv_diag);
 // Y = P_near X (overwrite), X/Y are N x R row-major.
 void launch_near_apply(Ctx& c, const DevPlan& p, int64_t nnz, const double* P, const double* X, double* Y, int R);
+// Node stride of an expansion row for Chebyshev order n: n^3 rounded up to a
+// multiple of 32 (64, 128, 224 for orders 4, 5, 6), so every row is 128-byte
+// aligned and a whole number of 32-node contraction chunks.
+inline int node_stride(int n) { return (n * n * n + 31) & ~31; }
+
 // Host-side level table plus device child ranges used to sequence the far field.
 struct FarLaunch {
     const int32_t* lvl_off;      // host, L+2 entries

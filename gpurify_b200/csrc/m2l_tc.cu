@@ -1,17 +1,24 @@
 // M2L on the 5th-generation tensor cores (tcgen05, kind::tf32, FP32
-// accumulation in tensor memory) for order-4 Chebyshev expansions.
+// accumulation in tensor memory) for expansions of order 4 (64 nodes) and
+// order 5 (125 nodes, stored with a node stride of 128).
 //
 // For one offset o every target box t with a source s = t + o needs
-//     L_t^T (R x 64) += E_s^T (R x 64) * K_o^T (64 x 64).
+//     L_t^T (R x NS) += E_s^T (R x NS) * K_o^T (NS x NS).
 // A CTA owns two target boxes (tA, tB) and a 64-wide chunk of right-hand
-// sides: D (128 x 64, FP32, in TMEM) = [E_sA^T; E_sB^T] (128 x 64, A operand)
-// times K_o^T (64 x 64, B operand), accumulated over the union of the two
-// boxes' offsets.  Expansions are stored E[box][r][node], so each A row (one
-// right-hand side) and each B row (one target node of K_o) is a contiguous
-// 256 B K-major row; rows are staged into shared memory in the 128-byte
-// swizzled layout, two K-halves of 32 tf32 each, double buffered: the 128
-// threads stage entry i+1 while the single issuing thread's MMAs of entry i
-// run; completion is tracked by tcgen05.commit on an mbarrier per stage.
+// sides: D (128 x NS, FP32, in TMEM) = [E_sA^T; E_sB^T] (128 x NS, A operand)
+// times K_o^T (NS x NS, B operand), accumulated over the union of the two
+// boxes' offsets.  Expansions are stored E[box][r][node] and the operator
+// table K[o][m][l] (target node m, source node l), both with node stride NS,
+// so every A row (one right-hand side) and every B row (one target node) is a
+// contiguous K-major row: the contraction over source nodes runs in chunks of
+// 32 TF32 (one 128-byte swizzle atom per row), and each chunk is one pipeline
+// stage: A (128 rows x 128 B) and B (NS rows x 128 B) copied with cp.async
+// straight into the 128-byte-swizzled layout the MMA descriptors name, kStages
+// stages in a ring, loads running kStages - 2 chunks ahead of the MMAs.  One
+// thread issues the four K=8 MMAs of a chunk and commits them to the stage's
+// mbarrier; a stage is refilled only after the MMAs that read it completed.
+// The tensor cores read FP32 operands as TF32 (the operator table is stored
+// rounded to TF32, the expansions are truncated by the hardware).
 // Every mbarrier wait is bounded; on expiry the kernel records an error code,
 // drains (bounded) its own MMAs, frees its TMEM and returns.
 #include "farfield.cuh"
@@ -21,16 +28,7 @@ namespace gpx {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr uint32_t kAHalf = 128 * 128;  // 128 rows x 128 B
-constexpr uint32_t kBHalf = 64 * 128;   // 64 rows x 128 B
-constexpr uint32_t kAStage = 2 * kAHalf;
-constexpr uint32_t kBStage = 2 * kBHalf;
-constexpr uint32_t kSmemBytes = 2 * kAStage + 2 * kBStage + 64 + 1024;  // + barriers + alignment slack
-constexpr uint32_t kTmemCols = 64;
-constexpr int kWaitLimit = 1 << 20;
-
-// Instruction descriptor: D F32, A/B TF32, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr int kWaitLimit = 1 << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -47,14 +45,13 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
     return d;
 }
 
+// Byte offset of 16-byte chunk `chunk` (0..7) of row `row` in a 128B-swizzled tile.
 __device__ __forceinline__ uint32_t swz(uint32_t row, uint32_t chunk) {
     return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk ^ (row & 7u)) << 4);
 }
 
-__device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
@@ -78,32 +75,46 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
+template <int NS>
+struct TcCfg {
+    static constexpr int kStages = 6;
+    static constexpr uint32_t kATile = 128 * 128;              // 128 rows x 128 B
+    static constexpr uint32_t kBTile = NS * 128;               // NS rows x 128 B
+    static constexpr uint32_t kStage = kATile + kBTile;        // multiple of 1024
+    static constexpr uint32_t kSmem = kStages * kStage + 1024 + 128;  // + alignment slack + barriers
+    static constexpr uint32_t kTmemCols = NS;                  // 64 or 128 FP32 columns
+    static constexpr int kChunks = NS / 32;                    // contraction chunks per entry
+    // Instruction descriptor: D F32, A/B TF32, both K-major, N = NS, M = 128.
+    static constexpr uint32_t kIdesc =
+        (1u << 4) | (2u << 7) | (2u << 10) | (((uint32_t)NS >> 3) << 17) | ((128u >> 4) << 24);
+};
+
+template <int NS>
 __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __restrict__ E, float* __restrict__ L,
                                                      const float* __restrict__ K32, int R, float scale,
                                                      int* __restrict__ err) {
+    using C = TcCfg<NS>;
+    constexpr int S = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* sbase = smem_raw + (base - raw);
-    uint8_t* sA = sbase;                    // 2 stages x 2 halves x 128 rows
-    uint8_t* sB = sbase + 2 * kAStage;      // 2 stages x 2 halves x 64 rows
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + 2 * kAStage + 2 * kBStage);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S * C::kStage);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int item = blockIdx.x;
     const int r0 = blockIdx.y * 64;
     const int tA = lv.item_t[2 * item], tB = lv.item_t[2 * item + 1];
     const int e0 = lv.item_off[item], e1 = lv.item_off[item + 1];
-    const int nent = e1 - e0;
+    const int total = (e1 - e0) * C::kChunks;
 
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[1])));
+        for (int k = 0; k < S; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[k])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(kTmemCols));
+                     "r"(C::kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -111,91 +122,94 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tslot;
 
+    // Copy chunk q (entry q / kChunks, source nodes 32 (q % kChunks) ..) into
+    // its stage: A rows 0..63 from tA's source, 64..127 from tB's source
+    // (zero-filled where the target has no source at this offset), B rows =
+    // the operator's target nodes.  Every thread copies 8 A and NS/16 B
+    // 16-byte pieces; 8 consecutive threads read one 128-byte row segment.
+    auto issue = [&](int q) {
+        if (q < total) {
+            const int e = e0 + q / C::kChunks, kc = q % C::kChunks;
+            const int sa = lv.srcA[e], sb = lv.srcB[e];
+            const uint32_t a = base + (uint32_t)(q % S) * C::kStage;
+            const uint32_t b = a + C::kATile;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int id = tid + kThreads * i, row = id >> 3, pc = id & 7;
+                const int src = row < 64 ? sa : sb;
+                const float* g = src >= 0 ? E + ((int64_t)src * R + r0 + (row & 63)) * NS + kc * 32 + pc * 4 : E;
+                cp16(a + swz(row, pc), g, src >= 0);
+            }
+            const float* Ko = K32 + (int64_t)lv.slot[e] * NS * NS + kc * 32;
+#pragma unroll
+            for (int i = 0; i < NS / 16; ++i) {
+                const int id = tid + kThreads * i, row = id >> 3, pc = id & 7;
+                cp16(b + swz(row, pc), Ko + (int64_t)row * NS + pc * 4, true);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
     bool bad = false;
-    for (int i = 0; i < nent; ++i) {
-        const int st = i & 1;
-        if (i >= 2) {
-            const bool ok = mbar_wait(smem_u32(&bars[st]), (uint32_t)(((i - 2) >> 1) & 1));
+    int issued = 0;
+    for (int q = 0; q < S - 2; ++q) issue(q);
+    for (int q = 0; q < total; ++q) {
+        if (q >= 2) {  // the stage of chunk q + S - 2 was last read by the MMAs of chunk q - 2
+            const bool ok = mbar_wait(smem_u32(&bars[(q - 2) % S]), (uint32_t)(((q - 2) / S) & 1));
             if (__syncthreads_or(!ok)) {
                 bad = true;
                 break;
             }
         }
-        const int e = e0 + i;
-        const int sa = lv.srcA[e], sb = lv.srcB[e];
-        const float* Ko = K32 + (int64_t)lv.slot[e] * 64 * 64;
-        uint8_t* a = sA + st * kAStage;
-        uint8_t* b = sB + st * kBStage;
-        // A: 128 rows (tA rhs 0..63, tB rhs 0..63) x 16 float4 of K
-#pragma unroll 4
-        for (int q = 0; q < 16; ++q) {
-            const int idx = tid + kThreads * q;
-            const int row = idx >> 4, c16 = idx & 15;
-            const int src = row < 64 ? sa : sb;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (src >= 0) {
-                v = *reinterpret_cast<const float4*>(E + ((int64_t)src * R + r0 + (row & 63)) * 64 + 4 * c16);
-                v.x = to_tf32(v.x);
-                v.y = to_tf32(v.y);
-                v.z = to_tf32(v.z);
-                v.w = to_tf32(v.w);
-            }
-            *reinterpret_cast<float4*>(a + (c16 >> 3) * kAHalf + swz(row, c16 & 7)) = v;
-        }
-        // B: 64 rows (target node m) x 16 float4 of K (source node l)
-#pragma unroll 4
-        for (int q = 0; q < 8; ++q) {
-            const int idx = tid + kThreads * q;
-            const int row = idx >> 4, c16 = idx & 15;
-            const float4 v = *reinterpret_cast<const float4*>(Ko + row * 64 + 4 * c16);
-            *reinterpret_cast<float4*>(b + (c16 >> 3) * kBHalf + swz(row, c16 & 7)) = v;
-        }
+        issue(q + S - 2);
+        asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t abase = smem_u32(a), bbase = smem_u32(b);
+            const uint32_t abase = base + (uint32_t)(q % S) * C::kStage, bbase = abase + C::kATile;
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                const uint32_t koff = (uint32_t)(s & 3) * 32u;  // 8 tf32 per MMA along K
-                const uint64_t ad = desc_sw128(abase + (uint32_t)(s >> 2) * kAHalf + koff);
-                const uint64_t bd = desc_sw128(bbase + (uint32_t)(s >> 2) * kBHalf + koff);
-                const uint32_t acc = (i > 0 || s > 0) ? 1u : 0u;
+            for (int s = 0; s < 4; ++s) {
+                const uint64_t ad = desc_sw128(abase + (uint32_t)s * 32u);
+                const uint64_t bd = desc_sw128(bbase + (uint32_t)s * 32u);
+                const uint32_t acc = (q > 0 || s > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+                    "l"(ad), "l"(bd), "r"(C::kIdesc), "r"(acc));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&bars[st]))
+                             smem_u32(&bars[q % S]))
                          : "memory");
         }
+        issued = q + 1;
     }
-    // Drain: the last commit covers every MMA issued before it.
-    if (nent > 0) {
-        const int last = nent - 1;
-        const bool ok = mbar_wait(smem_u32(&bars[last & 1]), (uint32_t)((last >> 1) & 1));
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // Drain: the last commit covers every MMA issued before it (after an
+    // expired wait too, so the TMEM is idle before it is freed).
+    if (issued > 0) {
+        const int last = issued - 1;
+        const bool ok = mbar_wait(smem_u32(&bars[last % S]), (uint32_t)((last / S) & 1));
         if (__syncthreads_or(!ok)) bad = true;
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (bad) {
         if (tid == 0) atomicExch(err, 1);
-    } else {
+    } else if (issued > 0) {
         // Epilogue: warp w reads TMEM lanes 32w..32w+31 = rows of D.
         const int row = warp * 32 + lane;
         const int t = row < 64 ? tA : tB;
-        const int r = r0 + (row & 63);
-        float* dst = (t >= 0) ? L + ((int64_t)t * R + r) * 64 : nullptr;
+        float* dst = (t >= 0) ? L + ((int64_t)t * R + r0 + (row & 63)) * NS : nullptr;
 #pragma unroll
-        for (int cb = 0; cb < 4; ++cb) {
+        for (int cb = 0; cb < NS / 16; ++cb) {
             uint32_t v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 16), v);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (dst && nent > 0) {
+            if (dst) {
 #pragma unroll
                 for (int k = 0; k < 16; k += 4) {
-                    float4 o = make_float4(scale * __uint_as_float(v[k]), scale * __uint_as_float(v[k + 1]),
-                                           scale * __uint_as_float(v[k + 2]), scale * __uint_as_float(v[k + 3]));
+                    const float4 o = make_float4(scale * __uint_as_float(v[k]), scale * __uint_as_float(v[k + 1]),
+                                                 scale * __uint_as_float(v[k + 2]), scale * __uint_as_float(v[k + 3]));
                     *reinterpret_cast<float4*>(dst + cb * 16 + k) = o;
                 }
             }
@@ -204,18 +218,29 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::kTmemCols));
+}
+
+template <int NS>
+void launch_ns(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale, int* err) {
+    using Cf = TcCfg<NS>;
+    GPX_CUDA(cudaFuncSetAttribute(k_m2l_tc<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::kSmem));
+    k_m2l_tc<NS><<<dim3(lv.nitems, R / 64), kThreads, Cf::kSmem, c.stream>>>(lv, E, L, K32, R, scale, err);
+    GPX_LAUNCH_CHECK();
 }
 
 }  // namespace
 
-void launch_m2l_tc(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale,
+void launch_m2l_tc(Ctx& c, const TcLevel& lv, int ns, const float* E, float* L, const float* K32, int R, float scale,
                    int* err) {
     if (lv.nitems == 0) return;
     if (R % 64 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core M2L needs R a multiple of 64");
-    GPX_CUDA(cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
-    k_m2l_tc<<<dim3(lv.nitems, R / 64), kThreads, kSmemBytes, c.stream>>>(lv, E, L, K32, R, scale, err);
-    GPX_LAUNCH_CHECK();
+    if (ns == 64)
+        launch_ns<64>(c, lv, E, L, K32, R, scale, err);
+    else if (ns == 128)
+        launch_ns<128>(c, lv, E, L, K32, R, scale, err);
+    else
+        throw Error(GPX_ERR_INTERNAL, "tensor-core M2L runs node strides 64 and 128 (orders 4 and 5)");
 }
 
 }  // namespace gpx

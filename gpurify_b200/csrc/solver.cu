@@ -28,11 +28,12 @@ struct DevM2L {
     int n = 0, mode = 0;
     DBuf<double> K;   // FP64 operators
     DBuf<double> U, Vt;  // low-rank factors (compressed mode), stride n3
-    DBuf<double> Ut64, Vt64;  // factored-M2L tables: Vt rows and transposed U rows (order 4)
+    DBuf<double> Ut64, Vt64;  // factored-M2L tables: Vt rows and transposed U rows, 343 x 32 x ns
     DBuf<float> Ut32, Vt32;
+    bool factored_ok = false;
     DBuf<int32_t> d_rank;
     int max_rank = 0;
-    DBuf<float> K32;  // the same, rounded to TF32 (round to nearest, ties away), for the tensor-core M2L
+    DBuf<float> K32;  // the same, rounded to TF32 (round to nearest, ties away), 343 x ns x ns, orders 4-5
     std::vector<int32_t> rank;
 };
 
@@ -58,32 +59,45 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
     }
     d->d_rank.upload(host.rank, ctx.stream);
     for (int32_t r : host.rank) d->max_rank = std::max(d->max_rank, (int)r);
-    if (mode == GPX_M2L_COMPRESSED && n == 4) {
-        const size_t sz = (size_t)343 * 64 * 64;
-        std::vector<double> ut(sz);
-        std::vector<float> ut32(sz), vt32(sz);
-        for (int s = 0; s < 343; ++s)
-            for (int k = 0; k < 64; ++k)
-                for (int m = 0; m < 64; ++m) {
-                    ut[((size_t)s * 64 + k) * 64 + m] = host.U[((size_t)s * 64 + m) * 64 + k];
-                    ut32[((size_t)s * 64 + k) * 64 + m] = (float)ut[((size_t)s * 64 + k) * 64 + m];
-                    vt32[((size_t)s * 64 + k) * 64 + m] = (float)host.Vt[((size_t)s * 64 + k) * 64 + m];
+    if (mode == GPX_M2L_COMPRESSED && n >= 4 && n <= 6 && d->max_rank <= kFacMaxRank) {
+        // factored tables: Vt rows and transposed U rows, kFacMaxRank rows of
+        // node stride ns per slot (rows beyond the rank and padding nodes zero)
+        const int n3 = n * n * n, ns = node_stride(n), KR = kFacMaxRank;
+        const size_t sz = (size_t)343 * KR * ns;
+        std::vector<double> ut(sz, 0.0), vt(sz, 0.0);
+        std::vector<float> ut32(sz, 0.f), vt32(sz, 0.f);
+        for (int sl = 0; sl < 343; ++sl)
+            for (int k = 0; k < std::max(0, (int)host.rank[sl]); ++k)
+                for (int m = 0; m < n3; ++m) {
+                    const size_t o = ((size_t)sl * KR + k) * ns + m;
+                    ut[o] = host.U[((size_t)sl * n3 + m) * n3 + k];
+                    vt[o] = host.Vt[((size_t)sl * n3 + k) * n3 + m];
+                    ut32[o] = (float)ut[o];
+                    vt32[o] = (float)vt[o];
                 }
         d->Ut64.upload(ut, ctx.stream);
-        d->Vt64.upload(host.Vt, ctx.stream);
+        d->Vt64.upload(vt, ctx.stream);
         d->Ut32.upload(ut32, ctx.stream);
         d->Vt32.upload(vt32, ctx.stream);
+        d->factored_ok = true;
     }
-    std::vector<float> k32(host.K.size());
-    for (size_t i = 0; i < k32.size(); ++i) {
-        float f = (float)host.K[i];
-        uint32_t u;
-        std::memcpy(&u, &f, 4);
-        if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
-        std::memcpy(&f, &u, 4);
-        k32[i] = f;
+    if (n == 4 || n == 5) {
+        // TF32-rounded (nearest, ties away) operators for the tensor-core M2L,
+        // node stride ns in both indices, padding zero
+        const int n3 = n * n * n, ns = node_stride(n);
+        std::vector<float> k32((size_t)343 * ns * ns, 0.f);
+        for (int sl = 0; sl < 343; ++sl)
+            for (int m = 0; m < n3; ++m)
+                for (int l = 0; l < n3; ++l) {
+                    float f = (float)host.K[((size_t)sl * n3 + m) * n3 + l];
+                    uint32_t u;
+                    std::memcpy(&u, &f, 4);
+                    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+                    std::memcpy(&f, &u, 4);
+                    k32[((size_t)sl * ns + m) * ns + l] = f;
+                }
+        d->K32.upload(k32, ctx.stream);
     }
-    d->K32.upload(k32, ctx.stream);
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     ctx.m2l_cache.push_back(d);
     return d;
@@ -163,6 +177,7 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
     }
     v.n = p.n;
     v.n3 = p.n3;
+    v.ns = node_stride(p.n);
     v.L = p.L;
     v.N = p.N;
     v.nleaf = (int32_t)p.nleaf();
@@ -269,13 +284,14 @@ struct Operator {
     bool mixed;
     const DevM2L* m2l;
     DBuf<double> P, inv_diag, E64, L64;
-    DBuf<float> P32, E32, L32, X32;
+    DBuf<float> P32, E32, L32, X32, W32;
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
     int mixed_near = 0;  // 0: TF32 tensor-core near apply, 1: FP32 CUDA cores
     BlockJacobi bj;
-    bool factored = false;  // M2L through the low-rank factors (order 4, compressed)
+    bool factored = false;  // M2L through the low-rank factors (compressed operators)
+    bool tc32 = false;      // mixed: FP32 M2L on the tensor cores (orders 4 and 5)
     FacM2L<double> fac64;
     FacM2L<float> fac32;
     DBuf<int64_t> src_col_off, col_vt, tgt_col_off, tgt_ut, tgt_base;
@@ -314,12 +330,13 @@ struct Operator {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (has_far()) {
+            const int ns = node_stride(pl.n);
             d.wsrc.alloc((size_t)pl.N * pl.n3, s);
             launch_src_weights(ctx, d.v, far_quad, d.wsrc.p);
             d.v.wsrc = d.wsrc.p;
-            E64.alloc((size_t)pl.nbox() * pl.n3 * R, s);
-            L64.alloc((size_t)pl.nbox() * pl.n3 * R, s);
-            if (m2l && m2l->mode == GPX_M2L_COMPRESSED && pl.n3 == 64 && m2l->max_rank <= 32) setup_factored();
+            E64.alloc((size_t)pl.nbox() * ns * R, s);
+            L64.alloc((size_t)pl.nbox() * ns * R, s);
+            if (m2l && m2l->factored_ok) setup_factored();
         }
         if (mixed) {
             P32.alloc((size_t)pl.nnz(), s);
@@ -331,10 +348,13 @@ struct Operator {
             tc_err.alloc(1, s);
             tc_err.zero();
             if (has_far()) {
+                const int ns = node_stride(pl.n);
                 Rb32 = (R + 63) / 64 * 64;
-                E32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
-                L32.alloc((size_t)pl.nbox() * pl.n3 * Rb32, s);
-                if (!factored) build_tc_lists(ctx, pl, tc);
+                E32.alloc((size_t)pl.nbox() * ns * Rb32, s);
+                L32.alloc((size_t)pl.nbox() * ns * Rb32, s);
+                W32.alloc((size_t)pl.N * pl.n3, s);
+                launch_to_f32(ctx, d.wsrc.p, W32.p, pl.N * pl.n3);
+                if (tc32) build_tc_lists(ctx, pl, tc);
             }
         }
     }
@@ -343,6 +363,7 @@ struct Operator {
     // target box (see farfield.cu).
     void setup_factored() {
         const int64_t np = pl.m2l_pairs(), nb = pl.nbox();
+        const int ns = node_stride(pl.n);
         std::vector<int32_t> rank(343);
         m2l->d_rank.download(rank.data(), 343);
         GPX_CUDA(cudaStreamSynchronize(ctx.stream));
@@ -364,7 +385,8 @@ struct Operator {
         for (int64_t b = 0; b < nb; ++b) {
             int64_t j = tcol[b];
             for (int64_t e = pl.m2l_off[b]; e < pl.m2l_off[b + 1]; ++e)
-                for (int k = 0; k < rank[pl.m2l_slot[e]]; ++k) ut[j++] = ((int64_t)pl.m2l_slot[e] * 64 + k) * 64;
+                for (int k = 0; k < rank[pl.m2l_slot[e]]; ++k)
+                    ut[j++] = ((int64_t)pl.m2l_slot[e] * kFacMaxRank + k) * ns;
         }
         // phase-1 columns grouped by source box
         std::vector<int64_t> scol(nb + 1, 0);
@@ -376,22 +398,23 @@ struct Operator {
             const int s = pl.m2l_src[e], slot = pl.m2l_slot[e];
             for (int k = 0; k < rank[slot]; ++k) {
                 const int64_t c = fill[s]++;
-                cvt[c] = ((int64_t)slot * 64 + k) * 64;
+                cvt[c] = ((int64_t)slot * kFacMaxRank + k) * ns;
                 ctg[c] = tgt_of_pair[e];
                 cps[c] = (int32_t)(pos_of_pair[e] + k);
             }
         }
-        // phase-1 work items per level: each source box's columns in tiles of 64
+        // phase-1 work items per level: each source box's columns in pieces of
+        // at most kFacItemCols (one CTA stages the source expansion once per piece)
         std::vector<int32_t> isrc, icnt;
         std::vector<int64_t> ic0;
         std::vector<int> lvl_first(pl.L + 2, 0);
         for (int l = 0; l <= pl.L; ++l) {
             lvl_first[l] = (int)isrc.size();
             for (int32_t b = pl.lvl_off[l]; b < pl.lvl_off[l + 1]; ++b)
-                for (int64_t c = scol[b]; c < scol[b + 1]; c += 64) {
+                for (int64_t c = scol[b]; c < scol[b + 1]; c += kFacItemCols) {
                     isrc.push_back(b);
                     ic0.push_back(c);
-                    icnt.push_back((int32_t)std::min<int64_t>(64, scol[b + 1] - c));
+                    icnt.push_back((int32_t)std::min<int64_t>(kFacItemCols, scol[b + 1] - c));
                 }
         }
         lvl_first[pl.L + 1] = (int)isrc.size();
@@ -415,6 +438,7 @@ struct Operator {
         tgt_ut.upload(ut, s);
         tgt_base.upload(base, s);
         auto wire = [&](auto& f) {
+            f.ns = ns;
             f.src_col_off = src_col_off.p;
             f.col_vt = col_vt.p;
             f.col_tgt = col_tgt.p;
@@ -430,7 +454,7 @@ struct Operator {
         fac64.Tm = T64.p;
         fac64.Ut = m2l->Ut64.p;
         fac64.Vt = m2l->Vt64.p;
-        if (mixed) {
+        if (mixed && !tc32) {
             Rb32 = (R + 63) / 64 * 64;
             T32.alloc((size_t)acc * Rb32, s);
             T32.zero();
@@ -451,7 +475,7 @@ struct Operator {
                 else
                     launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
             };
-            launch_far_field<double>(ctx, d.v, d.far, X, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
+            launch_far_field<double>(ctx, d.v, d.far, X, d.wsrc.p, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
         }
         applies += 1;
     }
@@ -466,12 +490,13 @@ struct Operator {
             launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
         if (has_far()) {
             M2LLevelFn<float> m2l_fn = [&](int level, int b0, int nb, double scale) {
-                if (factored)
-                    launch_m2l_fac<float>(ctx, fac32, fac_level[level], b0, nb, L32.p, E32.p, Rb32, scale);
+                if (tc32)
+                    launch_m2l_tc(ctx, tc.level[level], node_stride(pl.n), E32.p, L32.p, m2l->K32.p, Rb32,
+                                  (float)scale, tc_err.p);
                 else
-                    launch_m2l_tc(ctx, tc.level[level], E32.p, L32.p, m2l->K32.p, Rb32, (float)scale, tc_err.p);
+                    launch_m2l_fac<float>(ctx, fac32, fac_level[level], b0, nb, L32.p, E32.p, Rb32, scale);
             };
-            launch_far_field<float>(ctx, d.v, d.far, X32.p, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
+            launch_far_field<float>(ctx, d.v, d.far, X32.p, W32.p, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
         }
         applies32 += 1;
     }
@@ -659,6 +684,7 @@ Opts normalize(const gpx_solve_opts* o) {
     r.max_panels = o->max_panels;
     r.far_quad = o->far_quad;
     r.mixed_near = o->mixed_near;
+    r.mixed_m2l = o->mixed_m2l;
     return r;
 }
 
@@ -675,11 +701,17 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (n <= 0 || !verts) throw Error(GPX_ERR_CAPACITANCE, "no panels in geometry");
     if (ncond <= 0 || ncond > 4096) throw Error(GPX_ERR_INVALID_ARG, "n_conductors must be in [1, 4096]");
     if (o.order < 2 || o.order > 6) throw Error(GPX_ERR_INVALID_ARG, "Chebyshev order must be in [2, 6]");
-    if (o.precision == GPX_PREC_MIXED && o.order != 4)
-        throw Error(GPX_ERR_INVALID_ARG, "the mixed-precision path runs order-4 expansions");
+    if (o.precision == GPX_PREC_MIXED && o.order < 4)
+        throw Error(GPX_ERR_INVALID_ARG, "the mixed-precision path runs expansion orders 4 to 6");
+    if (o.precision == GPX_PREC_MIXED && o.m2l_mode == GPX_M2L_EXACT &&
+        (o.mixed_m2l != 0 || o.order > 5 || o.far_quad != 0))
+        throw Error(GPX_ERR_INVALID_ARG,
+                    "the mixed-precision path runs exact M2L operators on the tensor cores, at orders 4 and 5 "
+                    "with centroid far-field sources (far_quad 0)");
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
     if (o.precond != 0 && o.precond != 1) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0 or 1");
     if (o.mixed_near != 0 && o.mixed_near != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0 or 1");
+    if (o.mixed_m2l != 0 && o.mixed_m2l != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -706,6 +738,11 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     pr.op.reset(new Operator(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get()));
     pr.op->precond = o.precond;
     pr.op->mixed_near = o.mixed_near;
+    // TF32 M2L only with centroid sources: with 2x2 Gauss sources the leaf
+    // expansions carry large alternating node values (sources slightly outside
+    // their leaf box) and the TF32 inputs lose 1e-2 of the far field.
+    pr.op->tc32 = o.precision == GPX_PREC_MIXED && o.mixed_m2l == 0 && (o.order == 4 || o.order == 5) &&
+                  (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT);
     pr.op->assemble();
 }
 

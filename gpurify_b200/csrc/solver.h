@@ -19,6 +19,7 @@ struct Opts {
     int64_t max_panels = 0;
     int far_quad = 0;
     int mixed_near = 0;
+    int mixed_m2l = 0;
 };
 Opts normalize(const gpx_solve_opts* o);
 

@@ -97,7 +97,10 @@ typedef struct {
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
                                 (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
     int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05), 1 -> FP32 CUDA cores */
-    int32_t reserved[6];
+    int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5, else the
+                                factored low-rank form on FP32 CUDA cores; 1 -> always the factored form
+                                (compressed operators) */
+    int32_t reserved[5];
 } gpx_solve_opts;
 
 typedef struct {

@@ -43,11 +43,36 @@ def test_mixed_operator_close_to_fp64(ctx, nrhs, mixed_near):
         assert e < 1e-3, (j, e)
 
 
-@pytest.mark.parametrize("far_quad,mixed_near", [(0, 0), (1, 0), (1, 1)])
-def test_mixed_solve_matches_fp64(ctx, far_quad, mixed_near):
+@pytest.mark.parametrize("order,m2l_mode,mixed_m2l,far_quad", [(4, 0, 0, 0), (4, 0, 0, 1), (4, 0, 1, 1), (5, 0, 0, 0),
+                                                               (5, 0, 0, 1), (5, 1, 0, 0), (6, 0, 0, 1)])
+def test_mixed_operator_close_to_fp64_high_order(ctx, order, m2l_mode, mixed_m2l, far_quad):
+    """FP32 far field with the M2L on the tensor cores (orders 4-5, centroid
+    sources) or in the factored low-rank form on the CUDA cores, against the
+    FP64 operator with the same M2L operators."""
+    p = window()
+    rng = np.random.default_rng(5)
+    sig = rng.standard_normal((len(p["verts"]), 64))
+    kw = dict(order=order, max_level=5, dense_below=-1, far_quad=far_quad, m2l_mode=m2l_mode)
+    y64, rep = ctx.operator_apply(p["verts"], sig, precision=0, **kw)
+    y32, _ = ctx.operator_apply(p["verts"], sig, precision=1, mixed_m2l=mixed_m2l, **kw)
+    assert rep["m2l_pairs"] > 0
+    e = np.linalg.norm(y32 - y64, axis=0) / np.linalg.norm(y64, axis=0)
+    assert e.max() < 1e-3, e.max()
+
+
+def test_mixed_exact_m2l_needs_centroid_sources(ctx):
+    p = window()
+    with pytest.raises(_lib.GpxError) as ei:
+        ctx.operator_apply(p["verts"], np.ones((len(p["verts"]), 4)), precision=1, order=4, max_level=5,
+                           dense_below=-1, m2l_mode=1, far_quad=1)
+    assert ei.value.status == 1 and "far_quad 0" in ei.value.message
+
+
+@pytest.mark.parametrize("order,far_quad,mixed_near", [(4, 0, 0), (4, 1, 0), (4, 1, 1), (5, 1, 0)])
+def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near):
     p = window()
     nc = len(p["nets"]) + 1
-    kw = dict(order=4, max_level=5, dense_below=-1, far_quad=far_quad, skip_ground_rhs=1)
+    kw = dict(order=order, max_level=5, dense_below=-1, far_quad=far_quad, skip_ground_rhs=1)
     C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=0, **kw)
     C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, mixed_near=mixed_near, **kw)
     assert r32["converged"] == 1 and r32["outer_iterations"] >= 1

@@ -105,17 +105,37 @@ def test_wilton_matrix_matches_oracle(ctx, orc):
         assert e_gpu <= 1e-13 and e_gpu <= e_orc + 1e-15, (i, j, e_gpu, e_orc)
 
 
-@pytest.mark.parametrize("nrhs", [1, 5])
-def test_operator_apply_matches_oracle(ctx, orc, nrhs):
+@pytest.mark.parametrize("order,nrhs", [(4, 1), (4, 5), (2, 3), (3, 2), (5, 3), (6, 3)])
+def test_operator_apply_matches_oracle(ctx, orc, order, nrhs):
+    """Same tree, same QR-compressed M2L operators (factored on the GPU) at
+    every Chebyshev order the solver runs: FP64 reassociation only."""
     p = two_wire_panels()
     rng = np.random.default_rng(7)
     sig = rng.standard_normal((len(p["verts"]), nrhs))
-    y, rep = ctx.operator_apply(p["verts"], sig, order=4, max_level=4, dense_below=-1)
+    y, rep = ctx.operator_apply(p["verts"], sig, order=order, max_level=4, dense_below=-1)
     assert rep["m2l_pairs"] > 0 and rep["dense"] == 0
     for j in range(nrhs):
-        yo, nnz = orc.fmm_cap_apply(p["verts"], sig[:, j], 4, 4)
+        yo, nnz = orc.fmm_cap_apply(p["verts"], sig[:, j], order, 4)
         assert nnz == rep["nnz_near"]
         assert np.linalg.norm(y[:, j] - yo) / np.linalg.norm(yo) < 1e-11
+
+
+def test_exact_m2l_apply_tracks_all_pairs(ctx):
+    """Uncompressed (exact Chebyshev) M2L: the FMM apply approaches the
+    all-pairs Wilton apply as the order rises."""
+    lay = layouts.routing_window(12, 15.0, seed=11)
+    p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                             mesh_max_edge_m=0.3e-6, max_panels=-1)
+    rng = np.random.default_rng(3)
+    sig = 1.0 + 0.1 * rng.standard_normal((len(p["verts"]), 4))
+    yd, _ = ctx.operator_apply(p["verts"], sig, dense_below=2**31 - 1)
+    errs = []
+    for order in (4, 5, 6):
+        yf, rep = ctx.operator_apply(p["verts"], sig, order=order, max_level=5, dense_below=-1, m2l_mode=1,
+                                     far_quad=1)
+        assert rep["dense"] == 0 and rep["m2l_pairs"] > 0
+        errs.append(np.linalg.norm(yf - yd) / np.linalg.norm(yd))
+    assert errs[0] < 1e-3 and errs[1] < errs[0] and errs[2] < errs[0], errs
 
 
 def test_dense_path_matches_oracle_lu(ctx, orc):
