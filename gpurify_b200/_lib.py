@@ -29,6 +29,7 @@ EXPORTS = (
     "gpx_cap_solve_batched", "gpx_operator_apply", "gpx_potential_matrix", "gpx_cap_solve_groups",
     "gpx_extract_quasistatic", "gpx_bridge_panelize", "gpx_plan_check", "gpx_ctx_stream",
     "gpx_ctx_set_profiling", "gpx_ctx_kernel_stats", "gpx_ctx_reset_stats", "gpx_cap_solve_small_static",
+    "gpx_cap_sensitivity",
 )
 KERNEL_CLASSES = ("near_assemble", "near_apply", "p2m", "m2m", "m2l", "l2l", "l2p", "gs_dot", "gs_axpy", "vec",
                   "small")
@@ -143,6 +144,8 @@ def load(build_if_missing: bool = True):
                                            C.POINTER(C.c_double), C.POINTER(i64)]
         L.gpx_ctx_reset_stats.argtypes = [vp]
         L.gpx_cap_solve_small_static.argtypes = [vp, i64, vp, vp, i32, vp]
+        L.gpx_cap_sensitivity.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), i32, vp, vp, vp,
+                                          C.POINTER(SolveReport)]
         for name in EXPORTS:
             if name not in ("gpx_ctx_destroy", "gpx_last_error", "gpx_version", "gpx_ctx_stream"):
                 getattr(L, name).restype = C.c_int
@@ -211,6 +214,21 @@ class Context:
         rep = SolveReport()
         self._check(self.L.gpx_cap_solve(self.h, C.byref(pb), C.byref(opts(**kw)), Cm.ctypes.data, C.byref(rep)))
         return Cm, rep.as_dict()
+
+    def cap_sensitivity(self, verts, cond, ncond, velocities, **kw):
+        """Maxwell matrix and its derivatives along vertex velocity fields
+        (``velocities``: n_params x n_panels x 12).  Returns (C, dC, report)
+        with dC n_params x ncond x ncond (farads per unit parameter)."""
+        v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)
+        c = np.ascontiguousarray(cond, dtype=np.int32)
+        V = np.ascontiguousarray(velocities, dtype=np.float64).reshape(-1, len(v), 12)
+        pb = PanelProblem(len(v), v.ctypes.data, c.ctypes.data, ncond)
+        Cm = np.zeros((ncond, ncond))
+        dC = np.zeros((len(V), ncond, ncond))
+        rep = SolveReport()
+        self._check(self.L.gpx_cap_sensitivity(self.h, C.byref(pb), C.byref(opts(**kw)), len(V), V.ctypes.data,
+                                               Cm.ctypes.data, dC.ctypes.data, C.byref(rep)))
+        return Cm, dC, rep.as_dict()
 
     def operator_apply(self, verts, sigma, **kw):
         v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)

@@ -41,7 +41,7 @@ struct Ord {
 // chunk is written (zeros outside r < R, m < n3).
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X, const T* __restrict__ W,
-                                             T* __restrict__ E, int R, int Rb) {
+                                             bool mul_area, T* __restrict__ E, int R, int Rb) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, MI = NS / 32;
     constexpr int KP = sizeof(T) == 8 ? 16 : 32;  // panels per staged chunk (static shared memory <= 48 KB)
     const int t = blockIdx.x;
@@ -64,7 +64,8 @@ __global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X,
         }
         for (int e = tid; e < KP * 64; e += 256) {
             const int k = e >> 6, r = e & 63;
-            Qs[k][r] = (k < cnt && rc + r < R) ? (T)p.area[jb + k] * X[(jb + k) * R + rc + r] : (T)0;
+            Qs[k][r] = (k < cnt && rc + r < R) ? (mul_area ? (T)p.area[jb + k] : (T)1) * X[(jb + k) * R + rc + r]
+                                               : (T)0;
         }
         __syncthreads();
         for (int k = 0; k < cnt; ++k) {
@@ -94,10 +95,12 @@ __global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X,
 
 // L2P as a GEMM per (leaf, 64-wide chunk of r):
 //   Y[j][r] += coef * sum_m S_j[m] L[leaf][r][m],  S_j[m] = wx[a] wy[b] wz[c]
+// (the centroid's separable weights), or S_j = Wt[j] (times a_j if mul_area)
+// when explicit weights are given.
 // 256 threads; thread (tj, tr) holds panels tj + 16 i and rows tr + 16 q.
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L, double* __restrict__ Y, int R,
-                                             int Rb, double coef) {
+__global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L, const T* __restrict__ Wt,
+                                             bool mul_area, double* __restrict__ Y, int R, int Rb, double coef) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns;
     const int t = blockIdx.x;
     const int rc = blockIdx.y * 64;
@@ -124,7 +127,11 @@ __global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L,
             for (int e = tid; e < 64 * 32; e += 256) {
                 const int jj = e >> 5, mm = e & 31, m = m0 + mm;
                 T v = (T)0;
-                if (m < N3) v = wv[jj][m / (N * N)] * wv[jj][N + (m / N) % N] * wv[jj][2 * N + m % N];
+                if (m < N3 && jj < cnt) {
+                    v = Wt ? Wt[(jb + jj) * N3 + m]
+                           : wv[jj][m / (N * N)] * wv[jj][N + (m / N) % N] * wv[jj][2 * N + m % N];
+                    if (mul_area) v *= (T)p.area[jb + jj];
+                }
                 Ss[jj][mm] = v;
             }
             for (int e = tid; e < 32 * 64; e += 256) {
@@ -548,19 +555,19 @@ __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 template <class T, int N>
-void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const T* W, double* Y, int R, int Rb,
-                 T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
+void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y, int R,
+                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
     cudaStream_t s = c.stream;
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>();
     constexpr size_t smem = tree_smem<T, N>();
     const int Lv = p.L;
-    const double w = (double)sizeof(T);
-    const double box_bytes = w * N3 * R;
+    const double wb = (double)sizeof(T);
+    const double box_bytes = wb * N3 * R;
     const unsigned rchunks64 = cdiv(Rb, 64), rchunks_tree = cdiv(Rb, RC);
     GPX_CUDA(cudaMemsetAsync(L, 0, (size_t)p.nbox * NS * Rb * sizeof(T), s));
     {
-        KTimer t(c, K_P2M, (double)p.N * (w * R + w * N3 + 8.0) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
-        k_p2m<T, N><<<dim3(p.nleaf, rchunks64), 256, 0, s>>>(p, X, W, E, R, Rb);
+        KTimer t(c, K_P2M, (double)p.N * (wb * R + wb * N3 + 8.0) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
+        k_p2m<T, N><<<dim3(p.nleaf, rchunks64), 256, 0, s>>>(p, X, w.src, w.src_area, E, R, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
@@ -595,7 +602,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     }
     {
         KTimer t(c, K_L2P, (double)p.N * (16.0 * R + 24.0 * N) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
-        k_l2p<T, N><<<dim3(p.nleaf, cdiv(R, 64)), 256, 0, s>>>(p, L, Y, R, Rb, coef);
+        k_l2p<T, N><<<dim3(p.nleaf, cdiv(R, 64)), 256, 0, s>>>(p, L, w.tgt, w.tgt_area, Y, R, Rb, coef);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
@@ -604,14 +611,14 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
 }  // namespace
 
 template <class T>
-void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const T* W, double* Y, int R, int Rb,
-                      T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
+void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
+                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
     switch (p.n) {
-        case 2: far_field_n<T, 2>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
-        case 3: far_field_n<T, 3>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
-        case 4: far_field_n<T, 4>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
-        case 5: far_field_n<T, 5>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
-        case 6: far_field_n<T, 6>(c, p, f, X, W, Y, R, Rb, E, L, coef, m2l); break;
+        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
+        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
+        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
+        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
+        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
         default: throw Error(GPX_ERR_INVALID_ARG, "far field runs Chebyshev orders 2 to 6");
     }
 }
@@ -641,9 +648,10 @@ void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const dou
     GPX_LAUNCH_CHECK();
 }
 
-template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*, const double*, double*,
-                                       int, int, double*, double*, double, const M2LLevelFn<double>&);
-template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, const float*, double*, int,
-                                      int, float*, float*, double, const M2LLevelFn<float>&);
+template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*,
+                                       const FarWeights<double>&, double*, int, int, double*, double*, double,
+                                       const M2LLevelFn<double>&);
+template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, const FarWeights<float>&,
+                                      double*, int, int, float*, float*, double, const M2LLevelFn<float>&);
 
 }  // namespace gpx

@@ -10,13 +10,27 @@ namespace gpx {
 template <class T>
 using M2LLevelFn = std::function<void(int, int, int, double)>;
 
-// Y += coef * far-field potential of X (N x R, type T).  W: N x n3 source
-// weights (type T).  Expansions E and L: nbox x Rb x ns each (Rb >= R rows per
-// box, node stride ns); E is written in full by P2M and M2M (zero padding
-// rows and nodes), L is zeroed here.  M2L is supplied per level.
+// Weights of the far field's two ends.  P2M: E[leaf][r][m] = sum_j src[j][m]
+// (a_j if src_area) X[j][r]; L2P: Y[j][r] += coef sum_m tgt[j][m] (a_j if
+// tgt_area) L[leaf][r][m], where tgt = null means the separable collocation
+// weights S(c_j) of the panel centroid (from the plan's 1-D weights).  The
+// operator P uses (W, area) at P2M and (S(c), none) at L2P; its transpose uses
+// (S(c) as an array, none) at P2M and (W, area) at L2P.
 template <class T>
-void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const T* W, double* Y, int R, int Rb,
-                      T* E, T* L, double coef, const M2LLevelFn<T>& m2l);
+struct FarWeights {
+    const T* src = nullptr;  // N x n3
+    bool src_area = true;
+    const T* tgt = nullptr;  // N x n3 or null
+    bool tgt_area = false;
+};
+
+// Y += coef * far-field potential of X (N x R, type T).  Expansions E and L:
+// nbox x Rb x ns each (Rb >= R rows per box, node stride ns); E is written in
+// full by P2M and M2M (zero padding rows and nodes), L is zeroed here.  M2L is
+// supplied per level.
+template <class T>
+void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
+                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l);
 
 // FP64 M2L of one level with CUDA-core FMAs (dense operators).
 void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale);

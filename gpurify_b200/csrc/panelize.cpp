@@ -247,9 +247,13 @@ void panelize_groups(const std::vector<VolumeGroup>& groups, double xy, double m
             zbest = g.z0;
             geps = g.k;
         }
+    // Reference rule: cells of 4 gap, 4..32 per side.  Target-edge mode: cells
+    // of at most 4 max_edge and no cap, so plate panels stay small next to the
+    // far-field boxes the wires' mesh size calls for.
     const double cap = me > 0.0 ? 4096.0 : 32.0;
-    const size_t gnx = (size_t)std::min(std::max(std::ceil(lx / (4.0 * gap)), 4.0), cap);
-    const size_t gny = (size_t)std::min(std::max(std::ceil(ly / (4.0 * gap)), 4.0), cap);
+    const double cell = me > 0.0 ? std::min(4.0 * gap, 4.0 * me) : 4.0 * gap;
+    const size_t gnx = (size_t)std::min(std::max(std::ceil(lx / cell), 4.0), cap);
+    const size_t gny = (size_t)std::min(std::max(std::ceil(ly / cell), 4.0), cap);
     const double cx = 0.5 * (lo_x + hi_x), cy = 0.5 * (lo_y + hi_y);
     const double x0 = cx - lx / 2.0, y0 = cy - ly / 2.0, dx = lx / (double)gnx, dy = ly / (double)gny;
     const int32_t gid = (int32_t)res.nets.size();

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <functional>
 
+#include "adjoint.cuh"
 #include "farfield.cuh"
 #include "kernels.cuh"
 #include "krylov.cuh"
@@ -106,7 +107,7 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
 struct DevPlanBufs {
     DBuf<double> verts, cent, area, w1d, m2m1d;
     DBuf<int32_t> cond, near_off, near_src, near_S, box_parent, box_octant, m2l_src, m2l_slot, child_first,
-        child_count, leaf_of, item_leaf, item_row0, item128_leaf, item128_row0;
+        child_count, leaf_of, item_leaf, item_row0, item128_leaf, item128_row0, near_rev, near_pre;
     DBuf<int64_t> leaf_begin, nval_off, m2l_off;
     DBuf<double> leaf_ctr, wsrc;
     int nitems128 = 0;
@@ -146,6 +147,24 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
     }
     d.item_leaf.upload(p.item_leaf, s);
     d.item_row0.upload(p.item_row0, s);
+    {
+        // per near entry (t, e): its column offset in t's concatenated source
+        // list, and the index of t in the near list of leaf near_src[e]
+        std::vector<int32_t> pre(p.near_src.size()), rev(p.near_src.size(), -1);
+        for (int64_t t = 0; t < p.nleaf(); ++t) {
+            int32_t acc = 0;
+            for (int32_t e = p.near_off[t]; e < p.near_off[t + 1]; ++e) {
+                pre[e] = acc;
+                const int32_t u = p.near_src[e];
+                acc += (int32_t)(p.leaf_begin[u + 1] - p.leaf_begin[u]);
+                for (int32_t f = p.near_off[u]; f < p.near_off[u + 1]; ++f)
+                    if (p.near_src[f] == (int32_t)t) rev[e] = f - p.near_off[u];
+                if (rev[e] < 0) throw Error(GPX_ERR_INTERNAL, "near-leaf relation is not symmetric");
+            }
+        }
+        d.near_pre.upload(pre, s);
+        d.near_rev.upload(rev, s);
+    }
     DevPlan& v = d.v;
     v.nitems = (int32_t)p.item_leaf.size();
     v.item_leaf = d.item_leaf.p;
@@ -284,7 +303,11 @@ struct Operator {
     bool mixed;
     const DevM2L* m2l;
     DBuf<double> P, inv_diag, E64, L64;
-    DBuf<float> P32, E32, L32, X32, W32;
+    DBuf<float> P32, E32, L32, X32, W32, Sc32;
+    DBuf<double> Sc;  // transposed operator: collocation weights as P2M weights
+    FarWeights<double> w64;
+    FarWeights<float> w32;
+    bool transposed = false;
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
@@ -310,8 +333,12 @@ struct Operator {
 
     bool has_far() const { return pl.far && pl.m2l_pairs() > 0; }
 
-    void assemble() {
+    // Near blocks: the Wilton assembly, or (fwd given) the transpose of the
+    // forward operator's blocks; then the preconditioners and the far-field
+    // end weights (swapped for the transpose).
+    void assemble(const Operator* fwd = nullptr) {
         cudaStream_t s = ctx.stream;
+        transposed = fwd != nullptr;
         P.alloc((size_t)pl.nnz(), s);
         P.zero();  // row padding stays zero
         inv_diag.alloc((size_t)pl.N, s);
@@ -319,7 +346,10 @@ struct Operator {
         GPX_CUDA(cudaEventCreate(&e0));
         GPX_CUDA(cudaEventCreate(&e1));
         GPX_CUDA(cudaEventRecord(e0, s));
-        launch_near_assemble(ctx, d.v, pl.nnz(), P.p, kCoulomb);
+        if (transposed)
+            launch_near_transpose(ctx, d.v, d.near_rev.p, d.near_pre.p, fwd->P.p, P.p, pl.nnz());
+        else
+            launch_near_assemble(ctx, d.v, pl.nnz(), P.p, kCoulomb);
         GPX_CUDA(cudaEventRecord(e1, s));
         launch_diag_inv(ctx, d.v, P.p, inv_diag.p);
         if (precond == 1) bj.build(ctx, pl, d.v, P.p);
@@ -331,9 +361,16 @@ struct Operator {
         cudaEventDestroy(e1);
         if (has_far()) {
             const int ns = node_stride(pl.n);
-            d.wsrc.alloc((size_t)pl.N * pl.n3, s);
-            launch_src_weights(ctx, d.v, far_quad, d.wsrc.p);
-            d.v.wsrc = d.wsrc.p;
+            if (!transposed) {
+                d.wsrc.alloc((size_t)pl.N * pl.n3, s);
+                launch_src_weights(ctx, d.v, far_quad, d.wsrc.p);
+                d.v.wsrc = d.wsrc.p;
+                w64 = FarWeights<double>{d.wsrc.p, true, nullptr, false};
+            } else {
+                Sc.alloc((size_t)pl.N * pl.n3, s);
+                launch_centroid_weights(ctx, d.v, nullptr, Sc.p);
+                w64 = FarWeights<double>{Sc.p, false, d.wsrc.p, true};
+            }
             E64.alloc((size_t)pl.nbox() * ns * R, s);
             L64.alloc((size_t)pl.nbox() * ns * R, s);
             if (m2l && m2l->factored_ok) setup_factored();
@@ -354,6 +391,13 @@ struct Operator {
                 L32.alloc((size_t)pl.nbox() * ns * Rb32, s);
                 W32.alloc((size_t)pl.N * pl.n3, s);
                 launch_to_f32(ctx, d.wsrc.p, W32.p, pl.N * pl.n3);
+                if (!transposed) {
+                    w32 = FarWeights<float>{W32.p, true, nullptr, false};
+                } else {
+                    Sc32.alloc((size_t)pl.N * pl.n3, s);
+                    launch_to_f32(ctx, Sc.p, Sc32.p, pl.N * pl.n3);
+                    w32 = FarWeights<float>{Sc32.p, false, W32.p, true};
+                }
                 if (tc32) build_tc_lists(ctx, pl, tc);
             }
         }
@@ -475,9 +519,21 @@ struct Operator {
                 else
                     launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
             };
-            launch_far_field<double>(ctx, d.v, d.far, X, d.wsrc.p, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
+            launch_far_field<double>(ctx, d.v, d.far, X, w64, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
         }
         applies += 1;
+    }
+
+    // Y += far field of X with the given end weights (FP64).
+    void apply_far_with(const double* X, double* Y, const FarWeights<double>& w) {
+        if (!has_far()) return;
+        M2LLevelFn<double> m2l_fn = [&](int level, int b0, int nb, double scale) {
+            if (factored)
+                launch_m2l_fac<double>(ctx, fac64, fac_level[level], b0, nb, L64.p, E64.p, R, scale);
+            else
+                launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
+        };
+        launch_far_field<double>(ctx, d.v, d.far, X, w, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
     }
 
     // Y = A32 X: FP32 near field, FP32 far field with TF32 tensor-core M2L.
@@ -496,7 +552,7 @@ struct Operator {
                 else
                     launch_m2l_fac<float>(ctx, fac32, fac_level[level], b0, nb, L32.p, E32.p, Rb32, scale);
             };
-            launch_far_field<float>(ctx, d.v, d.far, X32.p, W32.p, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
+            launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
         }
         applies32 += 1;
     }
@@ -704,14 +760,14 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.precision == GPX_PREC_MIXED && o.order < 4)
         throw Error(GPX_ERR_INVALID_ARG, "the mixed-precision path runs expansion orders 4 to 6");
     if (o.precision == GPX_PREC_MIXED && o.m2l_mode == GPX_M2L_EXACT &&
-        (o.mixed_m2l != 0 || o.order > 5 || o.far_quad != 0))
+        (o.mixed_m2l == 1 || o.order > 5 || (o.far_quad != 0 && o.mixed_m2l != 2)))
         throw Error(GPX_ERR_INVALID_ARG,
                     "the mixed-precision path runs exact M2L operators on the tensor cores, at orders 4 and 5 "
                     "with centroid far-field sources (far_quad 0)");
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
     if (o.precond != 0 && o.precond != 1) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0 or 1");
     if (o.mixed_near != 0 && o.mixed_near != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0 or 1");
-    if (o.mixed_m2l != 0 && o.mixed_m2l != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0 or 1");
+    if (o.mixed_m2l < 0 || o.mixed_m2l > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1 or 2");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -741,16 +797,16 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     // TF32 M2L only with centroid sources: with 2x2 Gauss sources the leaf
     // expansions carry large alternating node values (sources slightly outside
     // their leaf box) and the TF32 inputs lose 1e-2 of the far field.
-    pr.op->tc32 = o.precision == GPX_PREC_MIXED && o.mixed_m2l == 0 && (o.order == 4 || o.order == 5) &&
-                  (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT);
+    pr.op->tc32 = o.precision == GPX_PREC_MIXED && o.mixed_m2l != 1 && (o.order == 4 || o.order == 5) &&
+                  (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT || o.mixed_m2l == 2);
     pr.op->assemble();
 }
 
 // FP64 iterative refinement around inner GMRES solves with the FP32 /
 // tensor-core operator: x += A32^-1 (b - A x) until the FP64 residual meets
 // the tolerance (design precedent: refine.rs:45-95, f32 LU + f64 residual).
-void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d_rhs, int R, int64_t N,
-                 const Opts& o, DBuf<double>& X, SolveStats& st, int& outer) {
+void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d_rhs, const double* B, int R,
+                 int64_t N, const Opts& o, DBuf<double>& X, SolveStats& st, int& outer) {
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
     const double floor_tol = std::pow(10.0, -o.inner_tol_exp);
@@ -765,7 +821,10 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
     bn.alloc(R, s);
     rn.alloc(R, s);
     mask.alloc(R, s);
-    launch_residual(ctx, d_cond, d_rhs, nullptr, Res.p, N, R);
+    if (B)
+        GPX_CUDA(cudaMemcpyAsync(Res.p, B, (size_t)NR * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    else
+        launch_residual(ctx, d_cond, d_rhs, nullptr, Res.p, N, R);
     launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, bn.p);
     std::vector<double> hb(R), hr(R);
     std::vector<int32_t> hm(R);
@@ -807,10 +866,70 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         st.iterations += in.iterations;
         launch_add(ctx, X.p, D.p, NR);
         op.apply(X.p, W.p);
-        launch_residual(ctx, d_cond, d_rhs, W.p, Res.p, N, R);
+        if (B)
+            launch_sub(ctx, B, W.p, Res.p, NR);
+        else
+            launch_residual(ctx, d_cond, d_rhs, W.p, Res.p, N, R);
         outer += 1;
     }
     op.check_tc();
+}
+
+// Solve op X = B (B null: the unit-conductor right-hand sides of d_rhs,
+// cap/solver.rs:55-63) with the options' precision.  The all-pairs path
+// stands in for the reference's dense LU (cap/solver.rs:114-117), so it is
+// solved to a tighter tolerance that matches a direct solve.
+void solve_columns(Ctx& ctx, Operator& op, const Opts& o, bool dense, const int32_t* d_cond, const int32_t* d_rhs,
+                   const double* B, int R, int64_t n, DBuf<double>& X, SolveStats& st, int& outer) {
+    const double tol = dense ? std::min(o.tol, 1e-12) : o.tol;
+    outer = 0;
+    if (o.precision == GPX_PREC_MIXED) {
+        Opts oi = o;
+        oi.tol = tol;
+        mixed_solve(ctx, op, d_cond, d_rhs, B, R, n, oi, X, st, outer);
+    } else {
+        const ApplyFn a64 = [&](const double* x, double* y) { op.apply(x, y); };
+        const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
+        gmres_multi(ctx, a64, pc, d_cond, d_rhs, B, R, n, tol, o.restart, o.max_restarts, X, st);
+    }
+}
+
+// Q[k][r] = a_k if panel k belongs to the conductor of column r, else 0.
+__global__ void k_rhs_areas(const int32_t* __restrict__ cond, const double* __restrict__ area,
+                            const int32_t* __restrict__ rhs, int64_t N, int R, double* __restrict__ Q) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * R) return;
+    const int64_t k = i / R;
+    const int r = (int)(i % R);
+    Q[i] = cond[k] == rhs[r] ? area[k] : 0.0;
+}
+
+// C (ncond x ncond) from the solved columns (R x ... device X); columns not
+// solved are filled by symmetry, the unsolved diagonal entry is NaN.
+void maxwell_from_columns(Ctx& ctx, const Prepared& pr, const DBuf<double>& X, int64_t n, int ncond, int Rn, int R,
+                          double* C) {
+    DBuf<double> dC;
+    dC.alloc((size_t)ncond * R, ctx.stream);
+    {
+        KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
+        k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, pr.dp.area.p, X.p, n, R, dC.p);
+        GPX_LAUNCH_CHECK();
+        ctx.launches += 1;
+    }
+    std::vector<double> hc((size_t)ncond * R);
+    dC.download(hc.data(), hc.size());
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+    for (int i = 0; i < ncond; ++i)
+        for (int j = 0; j < ncond; ++j) {
+            double v;
+            if (j < Rn)
+                v = hc[(size_t)i * R + j];
+            else if (i < Rn)
+                v = hc[(size_t)j * R + i];  // substrate column by symmetry
+            else
+                v = std::nan("");
+            C[(size_t)i * ncond + j] = v;
+        }
 }
 
 }  // namespace
@@ -845,7 +964,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     if (o.precision == GPX_PREC_MIXED) {
         Opts oi = o;
         oi.tol = tol;
-        mixed_solve(ctx, op, pr.dp.cond.p, d_rhs.p, R, n, oi, X, st, outer);
+        mixed_solve(ctx, op, pr.dp.cond.p, d_rhs.p, nullptr, R, n, oi, X, st, outer);
     } else {
         const ApplyFn a64 = [&](const double* x, double* y) { op.apply(x, y); };
         const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
@@ -950,6 +1069,119 @@ void potential_matrix(Ctx& ctx, int64_t ns, const double* sv, int64_t nt, const 
     launch_potential_matrix(ctx, a.p, ns, b.p, nt, c.p, kCoulomb);
     c.download(out, (size_t)ns * nt);
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+
+void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o,
+                     int np, const double* V, double* C, double* dCdp, gpx_solve_report* rep) {
+    const double t0 = now_s();
+    const int64_t l0 = ctx.launches;
+    check_problem(n, verts, cond, ncond, o);
+    if (np < 0 || np > 4096 || (np > 0 && !V)) throw Error(GPX_ERR_INVALID_ARG, "n_params must be in [0, 4096]");
+    for (int64_t i = 0; i < (int64_t)np * n * 12; ++i)
+        if (!std::isfinite(V[i])) throw Error(GPX_ERR_INVALID_ARG, "non-finite vertex velocity");
+    const int depth = choose_depth(o, n);
+    const bool dense = depth == 1;
+    const int Rn = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;
+    if (Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
+    const int R = (Rn + 3) & ~3;
+    cudaStream_t s = ctx.stream;
+    Prepared pr;
+    prepare(ctx, n, verts, cond, ncond, o, R, depth, pr);
+    Operator& op = *pr.op;
+    std::vector<int32_t> rhs_cond(R);
+    for (int r = 0; r < R; ++r) rhs_cond[r] = r < Rn ? r : -1;
+    DBuf<int32_t> d_rhs;
+    d_rhs.upload(rhs_cond, s);
+    // forward: P sigma_j = b_j
+    DBuf<double> X;
+    SolveStats st, stT;
+    int outer = 0, outerT = 0;
+    solve_columns(ctx, op, o, dense, pr.dp.cond.p, d_rhs.p, nullptr, R, n, X, st, outer);
+    if (!st.converged)
+        throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge (forward): max relative residual " +
+                                             std::to_string(st.max_resid));
+    maxwell_from_columns(ctx, pr, X, n, ncond, Rn, R, C);
+    // adjoint: P^T lambda_i = q_i
+    Operator opT(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get());
+    opT.precond = o.precond;
+    opT.mixed_near = o.mixed_near;
+    opT.tc32 = op.tc32;
+    opT.assemble(&op);
+    DBuf<double> Q, Lam;
+    Q.alloc((size_t)n * R, s);
+    {
+        KTimer kt(ctx, K_VEC, 16.0 * (double)n * R, 0.0);
+        k_rhs_areas<<<(unsigned)((n * R + 255) / 256), 256, 0, s>>>(pr.dp.cond.p, pr.dp.area.p, d_rhs.p, n, R, Q.p);
+        GPX_LAUNCH_CHECK();
+        ctx.launches += 1;
+    }
+    solve_columns(ctx, opT, o, dense, pr.dp.cond.p, d_rhs.p, Q.p, R, n, Lam, stT, outerT);
+    op.check_tc();
+    opT.check_tc();
+    if (!stT.converged)
+        throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge (adjoint): max relative residual " +
+                                             std::to_string(stT.max_resid));
+    // per parameter: dC = dq^T sigma - lambda^T (dP sigma)
+    const Plan& pl = pr.plan;
+    DBuf<double> dV, dcent, darea, dP, D, dW, dS, G;
+    dV.alloc((size_t)n * 12, s);
+    dcent.alloc((size_t)n * 3, s);
+    darea.alloc((size_t)n, s);
+    dP.alloc((size_t)pl.nnz(), s);
+    dP.zero();
+    D.alloc((size_t)n * R, s);
+    G.alloc((size_t)R * R, s);
+    if (op.has_far()) {
+        dW.alloc((size_t)n * pl.n3, s);
+        dS.alloc((size_t)n * pl.n3, s);
+    }
+    std::vector<double> vs((size_t)n * 12), hg((size_t)R * R);
+    for (int q = 0; q < np; ++q) {
+        const double* Vq = V + (size_t)q * n * 12;
+        for (int64_t k = 0; k < n; ++k)
+            std::memcpy(&vs[(size_t)k * 12], Vq + (size_t)pl.perm[k] * 12, 12 * sizeof(double));
+        dV.upload(vs, s);
+        launch_panel_dprops(ctx, pr.dp.v, dV.p, dcent.p, darea.p);
+        launch_near_assemble_dual(ctx, pr.dp.v, pl.nnz(), dV.p, dcent.p, dP.p, kCoulomb);
+        launch_near_apply(ctx, pr.dp.v, pl.nnz(), dP.p, X.p, D.p, R);
+        if (op.has_far()) {
+            launch_dsrc_weights(ctx, pr.dp.v, o.far_quad, dV.p, dW.p);
+            op.apply_far_with(X.p, D.p, FarWeights<double>{dW.p, false, nullptr, false});
+            launch_centroid_weights(ctx, pr.dp.v, dcent.p, dS.p);
+            op.apply_far_with(X.p, D.p, FarWeights<double>{pr.dp.wsrc.p, true, dS.p, false});
+        }
+        launch_grad_contract(ctx, pr.dp.cond.p, d_rhs.p, darea.p, X.p, Lam.p, D.p, n, R, G.p);
+        G.download(hg.data(), hg.size());
+        GPX_CUDA(cudaStreamSynchronize(s));
+        double* out = dCdp + (size_t)q * ncond * ncond;
+        for (int i = 0; i < ncond; ++i)
+            for (int j = 0; j < ncond; ++j)
+                out[(size_t)i * ncond + j] = (i < Rn && j < Rn) ? hg[(size_t)i * R + j] : std::nan("");
+    }
+    const double t1 = now_s();
+    if (rep) {
+        gpx_solve_report& r = *rep;
+        r.n_panels = n;
+        r.n_conductors = ncond;
+        r.n_rhs = Rn;
+        r.order = o.order;
+        r.max_level = depth;
+        r.n_boxes = pl.nbox();
+        r.n_leaves = pl.nleaf();
+        r.nnz_near = pl.near_pairs();
+        r.m2l_pairs = pl.m2l_pairs();
+        r.iterations = st.iterations + stT.iterations;
+        r.outer_iterations = outer + outerT;
+        r.operator_applies = op.applies + op.applies32 + opT.applies + opT.applies32;
+        r.max_rel_residual = std::max(st.max_resid, stT.max_resid);
+        r.converged = 1;
+        r.dense = dense ? 1 : 0;
+        r.t_solve_s = t1 - t0;
+        r.t_total_s = t1 - t0;
+        r.t_near_assembly_s = op.t_assembly_s;
+        r.kernel_launches = ctx.launches - l0;
+    }
 }
 
 }  // namespace gpx

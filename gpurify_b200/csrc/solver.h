@@ -31,6 +31,13 @@ int choose_depth(const Opts& o, int64_t n);
 void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, double* C,
                gpx_solve_report* rep);
 
+// Maxwell matrix C and its derivatives dC/dp for np vertex velocity fields V
+// (np x n x 12, caller panel order): one forward and one transposed solve
+// (all conductors at once), then one derivative apply per parameter.
+// dCdp: np x ncond x ncond; entries of conductors not solved are NaN.
+void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o,
+                     int np, const double* V, double* C, double* dCdp, gpx_solve_report* rep);
+
 // y = P sigma (sigma, y: n x R row-major in caller panel order).
 void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int R, const double* sigma, double* y,
                     gpx_solve_report* rep);

@@ -137,3 +137,47 @@ def run_pex_by_net_with_accuracy(store, deck, net_of_poly, accuracy=Accuracy.QUA
 def run_pex_by_net(store, deck, net_of_poly, **kw):
     acc = Accuracy.QUASISTATIC if deck.pex_method == "field_solver" else Accuracy.ANALYTICAL
     return run_pex_by_net_with_accuracy(store, deck, net_of_poly, acc, **kw)
+
+
+@dataclass
+class CapSensitivity:
+    """Maxwell matrix and its parameter derivatives of one layout.
+
+    ``nets``: net ids in conductor order (the substrate plate is the last
+    conductor).  ``maxwell_af``: k-scaled Maxwell matrix in aF.  ``grad``:
+    per parameter, dC/dp in aF per um for geometric parameters and aF per unit
+    of k for ``("k",)``."""
+    nets: List[int]
+    maxwell_af: np.ndarray
+    grad: Dict[tuple, np.ndarray]
+    report: dict = field(default_factory=dict)
+
+
+def run_pex_sensitivity_checked(store: GeometryStore, deck: Deck, net_of_poly: Sequence[int], params,
+                                ctx: Optional[_lib.Context] = None, **opts) -> CapSensitivity:
+    """Capacitance sensitivities beside the checked field-solver result
+    (fail-closed like ``run_pex_by_net_checked``): the layout is panelised as
+    the bridge does, the Maxwell matrix and dC/dp for every parameter of
+    ``params`` (see ``sensitivity.velocity_fields``) come from one forward and
+    one transposed solve on the GPU."""
+    from . import sensitivity
+
+    ctx = ctx or default_context()
+    panel_kw = {k: opts.pop(k) for k in ("mesh_max_edge_m", "max_panels") if k in opts}
+    try:
+        p = _lib.bridge_panelize(store.arrays(), deck.layer_table(), deck.dbu_nm, net_of_poly, **panel_kw)
+        if len(p["verts"]) == 0:
+            raise _lib.GpxError(15, "no panels in geometry")
+        eps = p["eps"]
+        if np.any(np.abs(eps - eps[0]) > 1e-12 * abs(eps[0])):
+            raise _lib.GpxError(15, "sensitivities need a homogeneous dielectric")
+        k = float(eps[0])
+        ncond = len(p["nets"]) + 1
+        V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params)
+        C, dC, rep = ctx.cap_sensitivity(p["verts"], p["cond"], ncond, V, **opts)
+    except _lib.GpxError as e:
+        raise _diagnostic(e) from None
+    grad = {}
+    for q, prm in enumerate(params):
+        grad[tuple(prm)] = C * 1e18 if prm[0] == "k" else k * dC[q] * 1e18 * 1e-6
+    return CapSensitivity([int(x) for x in p["nets"]], k * C * 1e18, grad, rep)

@@ -19,6 +19,8 @@
  *                            `fmm_solver::solve` and cap/solver.rs:100-134 `solve`
  *   gpx_cap_solve_batched    (no single reference function: many independent
  *                            windows; each window is one gpx_cap_solve)
+ *   gpx_cap_sensitivity      (no reference counterpart: adjoint dC/dp beside the
+ *                            capacitance result of cap/fmm_solver.rs:147-172)
  *   gpx_operator_apply       crates/pex/src/quasistatic/cap/fmm_solver.rs:109-129
  *                            `FmmCapOperator::apply`, for R right-hand sides
  *   gpx_potential_matrix     crates/pex/src/quasistatic/cap/solver.rs:81-97
@@ -97,9 +99,10 @@ typedef struct {
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
                                 (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
     int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05), 1 -> FP32 CUDA cores */
-    int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5, else the
-                                factored low-rank form on FP32 CUDA cores; 1 -> always the factored form
-                                (compressed operators) */
+    int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5 with centroid
+                                far-field sources, else the factored low-rank form on FP32 CUDA cores;
+                                1 -> always the factored form (compressed operators); 2 -> tensor cores
+                                at orders 4 and 5 also with Gauss-point sources */
     int32_t reserved[5];
 } gpx_solve_opts;
 
@@ -141,6 +144,21 @@ gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* problem, const g
 gpx_status gpx_cap_solve_batched(gpx_ctx* ctx, const gpx_panel_problem* problems, int32_t n_problems,
                                  const gpx_solve_opts* opts, double* const* maxwell_out,
                                  gpx_solve_report* reports);
+
+/* Adjoint sensitivities of the Maxwell matrix (north of the reference: it has
+ * no gradient path; the derivative is of the same discretised operator
+ * gpx_cap_solve solves).  Parameter q moves every panel vertex with velocity
+ * vert_velocity[q][panel][12] (same layout as problem->verts, metres per unit
+ * parameter).  maxwell_out: as gpx_cap_solve.  dmaxwell_out: n_params x
+ * n_conductors x n_conductors, dC_ij/dp_q in farads per unit parameter (no
+ * dielectric scaling; for a homogeneous dielectric dC_phys/dk = C).  Cost: one
+ * forward and one transposed solve for all conductors, then one derivative
+ * apply per parameter (Wilton near blocks differentiated exactly on dual
+ * numbers, far field with differentiated end weights).  With
+ * opts.skip_ground_rhs the substrate row and column of dmaxwell_out are NaN. */
+gpx_status gpx_cap_sensitivity(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
+                               int32_t n_params, const double* vert_velocity, double* maxwell_out,
+                               double* dmaxwell_out, gpx_solve_report* report);
 
 /* y = P sigma for `nrhs` columns (sigma, y: n_panels x nrhs row-major, panel
  * order of `problem`), P the precorrected operator the solver uses. */

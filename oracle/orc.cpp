@@ -1452,9 +1452,12 @@ int64_t orc_bridge_panelize(const int32_t* vx, const int32_t* vy, const uint32_t
             bestz = kv.second.z0;
             geps = kv.second.k;
         }
+    // reference rule (cap/mesh.rs:12-43 via bridge.rs:346-379): cells of 4 gap,
+    // 4..32 per side; target-edge mode: cells of at most 4 max_edge, no cap
     double plate_cap = me > 0.0 ? 4096.0 : 32.0;
-    size_t gnx = (size_t)std::fmin(std::fmax(std::ceil(lx / (4.0 * gap)), 4.0), plate_cap);
-    size_t gny = (size_t)std::fmin(std::fmax(std::ceil(ly / (4.0 * gap)), 4.0), plate_cap);
+    double cell = me > 0.0 ? std::fmin(4.0 * gap, 4.0 * me) : 4.0 * gap;
+    size_t gnx = (size_t)std::fmin(std::fmax(std::ceil(lx / cell), 4.0), plate_cap);
+    size_t gny = (size_t)std::fmin(std::fmax(std::ceil(ly / cell), 4.0), plate_cap);
     size_t before = s.size();
     plate(s, 0.5 * (b[0] + b[2]), 0.5 * (b[1] + b[3]), gz, lx, ly, gnx, gny, gid);
     s.eps.resize(s.size(), geps);

@@ -56,7 +56,8 @@ typedef struct {
  * Outputs the panels (grouped by (net, layer) in BTreeMap order + ground
  * plate), their conductor index and eps, and the sorted net list.
  * mesh_max_edge_m == 0 -> reference `subdivisions` rule; > 0 -> target-edge
- * mode (every face edge at most that long; plate cap lifted).
+ * mode (every face edge at most that long; substrate plate cells at most
+ * 4 x that long, no cap on their number).
  * max_panels: 0 = the reference's 20 000 limit; < 0 = unlimited.
  * Returns the panel count, or a negative error code; err_msg gets text. */
 int64_t orc_bridge_panelize(const int32_t* verts_x, const int32_t* verts_y,

@@ -128,3 +128,30 @@ def test_plan_covers_every_pair_once(depth):
     assert st["near_pairs"] + st["far_panel_pairs"] == n * n
     if depth == 1:
         assert st["m2l_box_pairs"] == 0
+
+
+def test_sensitivity_velocity_fields():
+    """Width stretches one wire across its axis (long sides +-1/2), spacing
+    translates the same-layer wires past it, thickness moves top faces by +1
+    and bottom faces not at all, height lifts the layer, k moves nothing."""
+    from gpurify_b200 import sensitivity
+
+    lay = layouts.bus_crossing(bits=3, wires=1, length_nm=6000, cross_pitch_nm=2000)
+    p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly, max_panels=-1)
+    z0, z1 = sensitivity.layer_span(lay.deck, "met2")
+    params = [("width", 1), ("spacing", 0), ("thickness", z0, z1), ("height", z0, z1), ("k",)]
+    V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params).reshape(len(params), -1, 4, 3)
+    pts = p["verts"].reshape(-1, 4, 3)
+    c = p["cond"]
+    w = V[0][c == 1]
+    assert np.allclose(np.unique(np.round(w[..., 1], 12)).min(), -0.5) and np.allclose(w[..., 1].max(), 0.5)
+    assert np.all(V[0][c != 1] == 0) and np.all(V[0][..., [0, 2]] == 0)
+    assert np.all(V[1][c == 0] == 0) and np.all(V[1][(c == 1) | (c == 2)][..., 1] == 1.0)
+    assert np.all(V[1][c >= 3] == 0)  # the crossing met3 wire and the substrate stay
+    th = V[2][c <= 2][..., 2]
+    zz = pts[c <= 2][..., 2]
+    assert np.allclose(th[np.isclose(zz, z1)], 1.0) and np.allclose(th[np.isclose(zz, z0)], 0.0)
+    assert np.all(V[3][c <= 2][..., 2] == 1.0) and np.all(V[3][c > 2] == 0)
+    assert np.all(V[4] == 0)
+    with pytest.raises(ValueError):
+        sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], [("length", 0)])
