@@ -374,21 +374,24 @@ __global__ void __launch_bounds__(256) k_m2l64(DevPlan p, int b0, double* __rest
 //     source's outgoing pairs, T[t_e][r][col(e,k)] = sum_l E_s[r][l] Vt_o[k][l];
 //   phase 2, per target box t: L_t[r][m] += scale * sum_c T_t[r][c] Ut[c][m],
 //     the contraction running over the concatenated ranks of t's pairs.
-// T is stored target-major (R rows x Kp_t columns per target, Kp_t = the
-// summed ranks rounded up to 4) so phase 2 reads contiguous rows.
+// T is stored target-major and column-major (Kp_t columns of R values per
+// target, Kp_t = the summed ranks rounded up to 4): phase 1 writes each column
+// as contiguous rows of R, phase 2 reads contiguous K-chunks.
 // Phase 1 as a transposed GEMM per work item (source box, up to
 // kFacItemCols of its columns): C[c][r] = sum_l Vt_c[l] E_s[r][l].  E_s^T (B)
-// is staged once per item; the gathered Vt rows (A) of each 64-column
-// sub-block stream through a cp.async double buffer over the ns nodes.
-template <class T>
-__global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __restrict__ item_src,
+// is staged once per item; the gathered Vt rows (A) of each CT-column
+// sub-block stream through a cp.async double buffer over the ns nodes.  CT
+// threads, 8 x 8 outputs per thread (columns ty + (CT/8) i, rows tx + 8 j).
+template <class T, int CT>
+__global__ void __launch_bounds__(CT) k_m2l_fac_v(FacM2L<T> f, const int32_t* __restrict__ item_src,
                                                   const int64_t* __restrict__ item_c0,
                                                   const int32_t* __restrict__ item_cnt, const T* __restrict__ E,
                                                   int R) {
     constexpr int V = 16 / sizeof(T);
     constexpr int KC = 128 / sizeof(T);
     constexpr int PP = KC + V;
-    constexpr int BP = 64 + V;
+    constexpr int BP = 64 + 1;  // odd pitch: the transposed staging stores hit distinct banks
+    constexpr int CS = CT / 8;  // column stride of a thread's tile
     const int ns = f.ns;
     const int it = blockIdx.x;
     const int rc = blockIdx.y * 64;
@@ -397,20 +400,20 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
     const int ncols = item_cnt[it];
     const int rows = min(64, R - rc);
     extern __shared__ __align__(16) unsigned char fac_smem[];
-    T(*As)[64][PP] = reinterpret_cast<T(*)[64][PP]>(fac_smem);                        // [2][64][PP]: [c][l]
-    T(*Bs)[BP] = reinterpret_cast<T(*)[BP]>(fac_smem + sizeof(T) * 2 * 64 * PP);      // [ns][BP]:  [l][r]
+    T(*As)[CT][PP] = reinterpret_cast<T(*)[CT][PP]>(fac_smem);                        // [2][CT][PP]: [c][l]
+    T(*Bs)[BP] = reinterpret_cast<T(*)[BP]>(fac_smem + sizeof(T) * 2 * CT * PP);      // [ns][BP]:  [l][r]
     const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
     const int nch = ns / KC;                      // node chunks per sub-block
-    const int nsub = (ncols + 63) / 64;           // 64-column sub-blocks
+    const int nsub = (ncols + CT - 1) / CT;       // CT-column sub-blocks
     const int nsteps = nsub * nch;
     auto issue = [&](int step) {
         const int sub = step / nch, ch = step % nch;
-        const int64_t c0 = cbase + 64 * sub;
-        const int nc = min(64, ncols - 64 * sub);
+        const int64_t c0 = cbase + (int64_t)CT * sub;
+        const int nc = min(CT, ncols - CT * sub);
         const int k0 = ch * KC, buf = step & 1;
 #pragma unroll
         for (int q = 0; q < KC / V; ++q) {
-            const int id = tid + 64 * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
+            const int id = tid + CT * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
             const bool ok = row < nc;
             cp16(&As[buf][row][kc], ok ? (const void*)(f.Vt + f.col_vt[c0 + row] + k0 + kc) : (const void*)f.Vt, ok);
         }
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
     };
     issue(0);
     const T* Es = E + ((int64_t)s * R + rc) * ns;
-    for (int e = tid; e < 64 * ns; e += 64) {
+    for (int e = tid; e < 64 * ns; e += CT) {
         const int r = e / ns, l = e % ns;
         Bs[l][r] = r < rows ? Es[(int64_t)r * ns + l] : (T)0;
     }
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
         for (int kk = 0; kk < KC; ++kk) {
             T a[8], b[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = As[buf][ty + 8 * i][kk];
+            for (int i = 0; i < 8; ++i) a[i] = As[buf][ty + CS * i][kk];
 #pragma unroll
             for (int j = 0; j < 8; ++j) b[j] = Bs[ch * KC + kk][tx + 8 * j];
 #pragma unroll
@@ -453,56 +456,59 @@ __global__ void __launch_bounds__(64) k_m2l_fac_v(FacM2L<T> f, const int32_t* __
                 for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
         }
         if (ch == nch - 1) {
-            const int64_t c0 = cbase + 64 * sub;
-            const int nc = min(64, ncols - 64 * sub);
+            const int64_t c0 = cbase + (int64_t)CT * sub;
+            const int nc = min(CT, ncols - CT * sub);
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const int c = ty + 8 * i;
+                const int c = ty + CS * i;
                 if (c >= nc) continue;
                 const int tg = f.col_tgt[c0 + c];
-                const int ld = (int)((f.tgt_col_off[tg + 1] - f.tgt_col_off[tg] + 3) & ~int64_t(3));
-                T* dst = f.Tm + f.tgt_base[tg] * R + (int64_t)rc * ld + f.col_pos[c0 + c];
+                T* dst = f.Tm + (f.tgt_base[tg] + f.col_pos[c0 + c]) * R + rc;
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int r = tx + 8 * j;
-                    if (r < rows) dst[(int64_t)r * ld] = acc[i][j];
+                    if (r < rows) dst[r] = acc[i][j];
                 }
             }
         }
     }
 }
 
-// Phase 2: CTA per (target box, 64 rows r, 64 nodes m).
-template <class T>
-__global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __restrict__ L, int R, double scale) {
+// Phase 2: CTA per (target box, 64 rows r, MW nodes m), MW threads, 8 x 8
+// outputs per thread (rows ty + 8 i, nodes tx + (MW/8) j); the contraction
+// over the target's concatenated ranks streams A = T rows and B = gathered Ut
+// rows through a cp.async double buffer.
+template <class T, int MW>
+__global__ void __launch_bounds__(MW) k_m2l_fac_u(FacM2L<T> f, int b0, T* __restrict__ L, int R, double scale) {
     constexpr int V = 16 / sizeof(T);
     constexpr int KC = 128 / sizeof(T);
     constexpr int PP = KC + V;
-    constexpr int XP = 64 + V;
+    constexpr int XP = MW + V;
+    constexpr int AP = 64 + V;
+    constexpr int TXN = MW / 8;
     const int ns = f.ns;
     const int t = b0 + blockIdx.x;
     const int rc = blockIdx.y * 64;
-    const int m0 = blockIdx.z * 64;
+    const int m0 = blockIdx.z * MW;
     const int64_t k0g = f.tgt_col_off[t], K = f.tgt_col_off[t + 1] - k0g;
     if (K == 0) return;
     const int Kp = (int)((K + 3) & ~int64_t(3));
-    const T* A = f.Tm + f.tgt_base[t] * R + (int64_t)rc * Kp;
+    const T* A = f.Tm + f.tgt_base[t] * R + rc;  // column-major: A[c][r] at c * R + r
     const int m = min(64, R - rc);
-    __shared__ __align__(16) T As[2][64][PP];
-    __shared__ __align__(16) T Bs[2][KC][XP];
-    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+    extern __shared__ __align__(16) unsigned char facu_smem[];
+    T(*As)[KC][AP] = reinterpret_cast<T(*)[KC][AP]>(facu_smem);                     // [2][KC][AP]: [c][r]
+    T(*Bs)[KC][XP] = reinterpret_cast<T(*)[KC][XP]>(facu_smem + sizeof(T) * 2 * KC * AP);  // [2][KC][XP]
+    const int tid = threadIdx.x, tx = tid % TXN, ty = tid / TXN;
     const int nchunk = (Kp + KC - 1) / KC;
     auto issue = [&](int cch) {
         const int k0 = cch * KC, buf = cch & 1;
-#pragma unroll
-        for (int q = 0; q < KC / V; ++q) {
-            const int id = tid + 64 * q, row = id / (KC / V), kc = (id % (KC / V)) * V;
-            const bool ok = row < m && k0 + kc < Kp;
-            cp16(&As[buf][row][kc], ok ? (const void*)(A + (int64_t)row * Kp + k0 + kc) : (const void*)f.Tm, ok);
+        for (int id = tid; id < KC * (64 / V); id += MW) {
+            const int kk = id / (64 / V), rr = (id % (64 / V)) * V;
+            const bool ok = k0 + kk < Kp && rr < m;
+            cp16(&As[buf][kk][rr], ok ? (const void*)(A + (int64_t)(k0 + kk) * R + rr) : (const void*)f.Tm, ok);
         }
-#pragma unroll
-        for (int q = 0; q < KC / V; ++q) {
-            const int id = tid + 64 * q, kk = id / (64 / V), cc = (id % (64 / V)) * V;
+        for (int id = tid; id < KC * (MW / V); id += MW) {
+            const int kk = id / (MW / V), cc = (id % (MW / V)) * V;
             const bool ok = k0 + kk < K && m0 + cc < ns;
             cp16(&Bs[buf][kk][cc], ok ? (const void*)(f.Ut + f.tgt_ut[k0g + k0 + kk] + m0 + cc) : (const void*)f.Ut,
                  ok);
@@ -529,9 +535,9 @@ __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
         for (int kk = 0; kk < KC; ++kk) {
             T a[8], b[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = As[buf][ty + 8 * i][kk];
+            for (int i = 0; i < 8; ++i) a[i] = As[buf][kk][ty + 8 * i];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) b[j] = Bs[buf][kk][tx + 8 * j];
+            for (int j = 0; j < 8; ++j) b[j] = Bs[buf][kk][tx + TXN * j];
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -544,7 +550,7 @@ __global__ void __launch_bounds__(64) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
         if (r >= m) continue;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const int mm = m0 + tx + 8 * j;
+            const int mm = m0 + tx + TXN * j;
             if (mm >= ns) continue;
             T* dst = L + ((int64_t)t * R + rc + r) * ns + mm;
             *dst += (T)scale * acc[i][j];
@@ -627,14 +633,25 @@ template <class T>
 void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int nb, T* L, const T* E, int R,
                     double scale) {
     constexpr int V = 16 / sizeof(T), KC = 128 / sizeof(T);
-    const int smem = (int)(sizeof(T) * (2 * 64 * (KC + V) + f.ns * (64 + V)));
+    constexpr int CT = 128;
+    const int smem_v = (int)(sizeof(T) * (2 * CT * (KC + V) + f.ns * (64 + 1)));
     if (lv.nitems > 0) {
-        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_v<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        k_m2l_fac_v<T><<<dim3(lv.nitems, cdiv(R, 64)), 64, smem, c.stream>>>(f, lv.item_src, lv.item_c0, lv.item_cnt,
-                                                                              E, R);
+        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_v<T, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_v));
+        k_m2l_fac_v<T, CT><<<dim3(lv.nitems, cdiv(R, 64)), CT, smem_v, c.stream>>>(f, lv.item_src, lv.item_c0,
+                                                                                    lv.item_cnt, E, R);
     }
     GPX_LAUNCH_CHECK();
-    k_m2l_fac_u<T><<<dim3(nb, cdiv(R, 64), cdiv(f.ns, 64)), 64, 0, c.stream>>>(f, b0, L, R, scale);
+    if (f.ns >= 128) {
+        constexpr int MW = 128;
+        const int smem_u = (int)(sizeof(T) * (2 * KC * (64 + V) + 2 * KC * (MW + V)));
+        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_u<T, MW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_u));
+        k_m2l_fac_u<T, MW><<<dim3(nb, cdiv(R, 64), cdiv(f.ns, MW)), MW, smem_u, c.stream>>>(f, b0, L, R, scale);
+    } else {
+        constexpr int MW = 64;
+        const int smem_u = (int)(sizeof(T) * (2 * KC * (64 + V) + 2 * KC * (MW + V)));
+        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_u<T, MW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_u));
+        k_m2l_fac_u<T, MW><<<dim3(nb, cdiv(R, 64), cdiv(f.ns, MW)), MW, smem_u, c.stream>>>(f, b0, L, R, scale);
+    }
     GPX_LAUNCH_CHECK();
     c.launches += 1;  // the caller counts the other one
 }

@@ -51,7 +51,7 @@ struct FacM2L {
     const int64_t* tgt_col_off = nullptr;  // nbox + 1: phase-2 contraction range of each target
     const int64_t* tgt_ut = nullptr;    // per contraction index: offset of its Ut row
     const int64_t* tgt_base = nullptr;  // nbox: sum of padded block widths of earlier boxes
-    T* Tm = nullptr;                    // target-major intermediate (R rows x Kp per target)
+    T* Tm = nullptr;                    // target-major intermediate (Kp columns of R values per target)
 };
 // Phase-1 work items of one level: (source box, first column, column count <= kFacItemCols).
 constexpr int kFacItemCols = 512;
