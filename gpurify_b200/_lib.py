@@ -49,7 +49,8 @@ class SolveOpts(C.Structure):
         ("tol", C.c_double), ("restart", C.c_int32), ("max_restarts", C.c_int32), ("dense_below", C.c_int32),
         ("precond", C.c_int32), ("skip_ground_rhs", C.c_int32), ("inner_tol_exp", C.c_int32),
         ("mesh_max_edge_m", C.c_double), ("max_panels", C.c_int64), ("far_quad", C.c_int32),
-        ("mixed_near", C.c_int32), ("mixed_m2l", C.c_int32), ("reserved", C.c_int32 * 5),
+        ("mixed_near", C.c_int32), ("mixed_m2l", C.c_int32), ("no_graphs", C.c_int32), ("batch_streams", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -214,6 +215,24 @@ class Context:
         rep = SolveReport()
         self._check(self.L.gpx_cap_solve(self.h, C.byref(pb), C.byref(opts(**kw)), Cm.ctypes.data, C.byref(rep)))
         return Cm, rep.as_dict()
+
+    def cap_solve_batched(self, problems, **kw):
+        """Many independent windows in one call (gpx_cap_solve_batched).
+        ``problems``: sequence of (verts, cond, ncond).  Returns a list of
+        (C, report) in input order."""
+        keep, pbs = [], (PanelProblem * max(1, len(problems)))()
+        outs = []
+        for i, (verts, cond, ncond) in enumerate(problems):
+            v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)
+            c = np.ascontiguousarray(cond, dtype=np.int32)
+            keep += [v, c]
+            pbs[i] = PanelProblem(len(v), v.ctypes.data, c.ctypes.data, ncond)
+            outs.append(np.zeros((ncond, ncond)))
+        ptrs = (C.c_void_p * max(1, len(outs)))(*[o.ctypes.data for o in outs])
+        reps = (SolveReport * max(1, len(outs)))()
+        self._check(self.L.gpx_cap_solve_batched(self.h, C.cast(pbs, C.c_void_p), len(outs), C.byref(opts(**kw)),
+                                                 C.cast(ptrs, C.c_void_p), C.cast(reps, C.c_void_p)))
+        return [(outs[i], reps[i].as_dict()) for i in range(len(outs))]
 
     def cap_sensitivity(self, verts, cond, ncond, velocities, **kw):
         """Maxwell matrix and its derivatives along vertex velocity fields

@@ -2,7 +2,9 @@
 // exceptions to a gpx_status and records the message on the context; nothing
 // throws across the ABI.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstring>
 
@@ -27,11 +29,11 @@ gpx_status fail(gpx_ctx* ctx, gpx_status s, const std::string& msg) {
 struct CopyMeter {
     gpx_solve_report* r;
     int64_t h0, d0;
-    explicit CopyMeter(gpx_solve_report* rep) : r(rep), h0(h2d_counter().load()), d0(d2h_counter().load()) {}
+    explicit CopyMeter(gpx_solve_report* rep) : r(rep), h0(h2d_counter()), d0(d2h_counter()) {}
     ~CopyMeter() {
         if (r) {
-            r->h2d_bytes = h2d_counter().load() - h0;
-            r->d2h_bytes = d2h_counter().load() - d0;
+            r->h2d_bytes = h2d_counter() - h0;
+            r->d2h_bytes = d2h_counter() - d0;
         }
     }
 };
@@ -154,17 +156,70 @@ gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* pb, const gpx_so
     });
 }
 
+// Windows are independent: a work queue, largest estimated cost first, is
+// drained by batch_streams worker threads, each with its own stream (a
+// private context on the same device), so small and large windows overlap on
+// the GPU.  Every window runs the same code path as gpx_cap_solve, so its
+// result is identical to a separate call.
 gpx_status gpx_cap_solve_batched(gpx_ctx* ctx, const gpx_panel_problem* pbs, int32_t n, const gpx_solve_opts* opts,
                                  double* const* maxwell_out, gpx_solve_report* reports) {
-    if (!ctx || (n > 0 && (!pbs || !maxwell_out))) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
+    if (!ctx || n < 0 || (n > 0 && (!pbs || !maxwell_out))) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
     return guarded(ctx, [&] {
         Opts o = normalize(opts);
         for (int32_t i = 0; i < n; ++i) {
-            gpx_solve_report* r = reports ? &reports[i] : nullptr;
-            if (r) std::memset(r, 0, sizeof(*r));
-            cap_solve(ctx->impl, pbs[i].n_panels, pbs[i].verts, pbs[i].conductor, pbs[i].n_conductors, o,
-                      maxwell_out[i], r);
+            if (reports) std::memset(&reports[i], 0, sizeof(reports[i]));
+            if (!maxwell_out[i]) throw Error(GPX_ERR_INVALID_ARG, "window " + std::to_string(i) + ": null output");
         }
+        const int workers = std::max(1, std::min<int>(n, o.batch_streams > 0 ? std::min(o.batch_streams, 32) : 8));
+        if (workers == 1 || ctx->impl.profile) {
+            for (int32_t i = 0; i < n; ++i) {
+                try {
+                    cap_solve(ctx->impl, pbs[i].n_panels, pbs[i].verts, pbs[i].conductor, pbs[i].n_conductors, o,
+                              maxwell_out[i], reports ? &reports[i] : nullptr);
+                } catch (const Error& e) {
+                    throw Error(e.status, "window " + std::to_string(i) + ": " + e.what(), e.polygon);
+                }
+            }
+            return;
+        }
+        std::vector<int32_t> order(n);
+        for (int32_t i = 0; i < n; ++i) order[i] = i;
+        auto cost = [&](int32_t i) { return (double)pbs[i].n_panels * std::max(1, pbs[i].n_conductors); };
+        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cost(a) > cost(b); });
+        std::atomic<int32_t> next{0};
+        std::atomic<int64_t> launches{0};
+        std::vector<gpx_status> st(n, GPX_OK);
+        std::vector<std::string> msg(n);
+        const int device = ctx->impl.device;
+        auto work = [&] {
+            gpx_ctx* sub = nullptr;
+            if (gpx_ctx_create(&sub, device) != GPX_OK) {
+                for (int32_t k; (k = next.fetch_add(1)) < n;) {
+                    st[order[k]] = GPX_ERR_CUDA;
+                    msg[order[k]] = "could not create a worker stream";
+                }
+                return;
+            }
+            for (int32_t k; (k = next.fetch_add(1)) < n;) {
+                const int32_t i = order[k];
+                gpx_solve_report* r = reports ? &reports[i] : nullptr;
+                CopyMeter meter(r);
+                st[i] = guarded(sub, [&] {
+                    cap_solve(sub->impl, pbs[i].n_panels, pbs[i].verts, pbs[i].conductor, pbs[i].n_conductors, o,
+                              maxwell_out[i], r);
+                });
+                if (st[i] != GPX_OK) msg[i] = sub->impl.last_error;
+            }
+            launches += sub->impl.launches;
+            gpx_ctx_destroy(sub);
+        };
+        std::vector<std::thread> pool;
+        for (int w = 0; w < workers; ++w) pool.emplace_back(work);
+        for (auto& t : pool) t.join();
+        ctx->impl.launches += launches.load();
+        GPX_CUDA(cudaSetDevice(device));
+        for (int32_t i = 0; i < n; ++i)
+            if (st[i] != GPX_OK) throw Error(st[i], "window " + std::to_string(i) + ": " + msg[i]);
     });
 }
 

@@ -578,8 +578,8 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
         c.launches += 1;
     }
     if (smem > 48 * 1024) {
-        GPX_CUDA(cudaFuncSetAttribute(k_m2m_tree<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        GPX_CUDA(cudaFuncSetAttribute(k_l2l_tree<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        set_smem_once(k_m2m_tree<T, N>, (int)smem);
+        set_smem_once(k_l2l_tree<T, N>, (int)smem);
     }
     for (int l = Lv; l >= 3; --l) {
         const int pb0 = f.lvl_off[l - 1], npb = f.lvl_off[l] - pb0, nch = f.lvl_off[l + 1] - f.lvl_off[l];
@@ -636,7 +636,7 @@ void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int 
     constexpr int CT = 128;
     const int smem_v = (int)(sizeof(T) * (2 * CT * (KC + V) + f.ns * (64 + 1)));
     if (lv.nitems > 0) {
-        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_v<T, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_v));
+        set_smem_once(k_m2l_fac_v<T, CT>, smem_v);
         k_m2l_fac_v<T, CT><<<dim3(lv.nitems, cdiv(R, 64)), CT, smem_v, c.stream>>>(f, lv.item_src, lv.item_c0,
                                                                                     lv.item_cnt, E, R);
     }
@@ -644,12 +644,12 @@ void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int 
     if (f.ns >= 128) {
         constexpr int MW = 128;
         const int smem_u = (int)(sizeof(T) * (2 * KC * (64 + V) + 2 * KC * (MW + V)));
-        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_u<T, MW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_u));
+        set_smem_once(k_m2l_fac_u<T, MW>, smem_u);
         k_m2l_fac_u<T, MW><<<dim3(nb, cdiv(R, 64), cdiv(f.ns, MW)), MW, smem_u, c.stream>>>(f, b0, L, R, scale);
     } else {
         constexpr int MW = 64;
         const int smem_u = (int)(sizeof(T) * (2 * KC * (64 + V) + 2 * KC * (MW + V)));
-        GPX_CUDA(cudaFuncSetAttribute(k_m2l_fac_u<T, MW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_u));
+        set_smem_once(k_m2l_fac_u<T, MW>, smem_u);
         k_m2l_fac_u<T, MW><<<dim3(nb, cdiv(R, 64), cdiv(f.ns, MW)), MW, smem_u, c.stream>>>(f, b0, L, R, scale);
     }
     GPX_LAUNCH_CHECK();

@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include <cstdint>
 #include <cstdio>
@@ -39,13 +42,15 @@ struct Error : std::runtime_error {
                                std::string(#call) + ": " + cudaGetErrorString(e_));           \
     } while (0)
 
-// Host<->device bytes copied by the library (all contexts of the process).
-inline std::atomic<int64_t>& h2d_counter() {
-    static std::atomic<int64_t> c{0};
+// Host<->device bytes copied by the library on the calling thread (a call's
+// copies all happen on the thread that made it, so a per-thread count gives
+// each call's own bytes even while other threads solve concurrently).
+inline int64_t& h2d_counter() {
+    static thread_local int64_t c = 0;
     return c;
 }
-inline std::atomic<int64_t>& d2h_counter() {
-    static std::atomic<int64_t> c{0};
+inline int64_t& d2h_counter() {
+    static thread_local int64_t c = 0;
     return c;
 }
 
@@ -185,6 +190,23 @@ struct KTimer {
 };
 
 inline void count_launch(Ctx& c, int k = 1) { c.launches += k; }
+
+// Raises a kernel's dynamic shared-memory limit on the current device, once
+// per (kernel, device, size) in the process: the attribute call is a host
+// API call that must not run while a stream is being captured into a graph,
+// so launches inside a capture find it already set.
+template <class K>
+inline void set_smem_once(K* kernel, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    GPX_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    int& have = done[{reinterpret_cast<const void*>(kernel), dev}];
+    if (have >= bytes) return;
+    GPX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    have = bytes;
+}
 
 #define GPX_LAUNCH_CHECK() GPX_CUDA(cudaGetLastError())
 

@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
 template <int NS>
 void launch_ns(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale, int* err) {
     using Cf = TcCfg<NS>;
-    GPX_CUDA(cudaFuncSetAttribute(k_m2l_tc<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::kSmem));
+    set_smem_once(k_m2l_tc<NS>, (int)Cf::kSmem);
     k_m2l_tc<NS><<<dim3(lv.nitems, R / 64), kThreads, Cf::kSmem, c.stream>>>(lv, E, L, K32, R, scale, err);
     GPX_LAUNCH_CHECK();
 }

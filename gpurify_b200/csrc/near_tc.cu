@@ -289,7 +289,7 @@ void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, con
     if (nitems == 0) return;
     if (R % 4 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core near apply needs R a multiple of 4");
     KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 12.0 * (double)p.N * R, 2.0 * (double)nnz * R);
-    GPX_CUDA(cudaFuncSetAttribute(k_near_apply_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+    set_smem_once(k_near_apply_tc, (int)kSmemBytes);
     k_near_apply_tc<<<dim3(nitems, (R + 63) / 64), kThreads, kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, X, Y, R,
                                                                                      err);
     GPX_LAUNCH_CHECK();

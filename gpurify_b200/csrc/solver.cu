@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <mutex>
 
 #include "adjoint.cuh"
 #include "farfield.cuh"
@@ -44,11 +45,24 @@ double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Host M2L tables, built once per (order, mode) in the process and shared by
+// every context (their compression is the costly part).
+std::shared_ptr<const M2LTable> host_m2l(int n, int mode) {
+    static std::mutex mu;
+    static std::vector<std::shared_ptr<const M2LTable>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& t : cache)
+        if (t->n == n && t->mode == mode) return t;
+    auto t = std::make_shared<M2LTable>();
+    build_m2l_table(*t, n, mode);
+    cache.push_back(t);
+    return t;
+}
+
 std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
     for (auto& t : ctx.m2l_cache)
         if (t->n == n && t->mode == mode) return t;
-    M2LTable host;
-    build_m2l_table(host, n, mode);
+    const M2LTable& host = *host_m2l(n, mode);
     auto d = std::make_shared<DevM2L>();
     d->n = n;
     d->mode = mode;
@@ -308,6 +322,20 @@ struct Operator {
     FarWeights<double> w64;
     FarWeights<float> w32;
     bool transposed = false;
+    // Operator applies captured into CUDA graphs, one per (input, output,
+    // kind): the first call with a pair runs directly (it also performs the
+    // one-time per-kernel attribute set-up), the second captures and every
+    // later call replays the graph.
+    bool use_graphs = true;
+    struct GraphEntry {
+        const void* x;
+        void* y;
+        int kind;
+        int seen;
+        cudaGraphExec_t exec;
+        int64_t nlaunch;
+    };
+    std::vector<GraphEntry> graphs;
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
@@ -330,6 +358,59 @@ struct Operator {
 
     Operator(Ctx& c, const Plan& p, DevPlanBufs& dd, int r, int fq, bool mx, const DevM2L* m)
         : ctx(c), pl(p), d(dd), R(r), far_quad(fq), mixed(mx), m2l(m) {}
+    Operator(const Operator&) = delete;
+    Operator& operator=(const Operator&) = delete;
+    ~Operator() {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
+
+    template <class F>
+    void run_captured(int kind, const void* x, void* y, F&& body) {
+        if (!use_graphs || ctx.profile) {
+            body();
+            return;
+        }
+        GraphEntry* ge = nullptr;
+        for (auto& g : graphs)
+            if (g.x == x && g.y == y && g.kind == kind) ge = &g;
+        if (!ge) {
+            if (graphs.size() >= 16) {  // many distinct buffers: not worth capturing
+                body();
+                return;
+            }
+            graphs.push_back({x, y, kind, 0, nullptr, 0});
+            ge = &graphs.back();
+        }
+        if (ge->exec) {
+            GPX_CUDA(cudaGraphLaunch(ge->exec, ctx.stream));
+            ctx.launches += ge->nlaunch;
+            return;
+        }
+        if (ge->seen++ == 0) {
+            body();
+            return;
+        }
+        const int64_t l0 = ctx.launches;
+        GPX_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t g = nullptr;
+        try {
+            body();
+        } catch (...) {
+            cudaStreamEndCapture(ctx.stream, &g);
+            if (g) cudaGraphDestroy(g);
+            ctx.launches = l0;
+            throw;
+        }
+        GPX_CUDA(cudaStreamEndCapture(ctx.stream, &g));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        GPX_CUDA(e);
+        ge->exec = exec;
+        ge->nlaunch = ctx.launches - l0;
+        GPX_CUDA(cudaGraphLaunch(exec, ctx.stream));
+    }
 
     bool has_far() const { return pl.far && pl.m2l_pairs() > 0; }
 
@@ -511,6 +592,10 @@ struct Operator {
 
     // Y = A X in FP64 (X, Y: N x R, leaf-sorted panel order).
     void apply(const double* X, double* Y) {
+        run_captured(0, X, Y, [&] { apply_direct(X, Y); });
+        applies += 1;
+    }
+    void apply_direct(const double* X, double* Y) {
         launch_near_apply(ctx, d.v, pl.nnz(), P.p, X, Y, R);
         if (has_far()) {
             M2LLevelFn<double> m2l_fn = [&](int level, int b0, int nb, double scale) {
@@ -521,7 +606,6 @@ struct Operator {
             };
             launch_far_field<double>(ctx, d.v, d.far, X, w64, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
         }
-        applies += 1;
     }
 
     // Y += far field of X with the given end weights (FP64).
@@ -538,6 +622,10 @@ struct Operator {
 
     // Y = A32 X: FP32 near field, FP32 far field with TF32 tensor-core M2L.
     void apply32(const double* X, double* Y) {
+        run_captured(1, X, Y, [&] { apply32_direct(X, Y); });
+        applies32 += 1;
+    }
+    void apply32_direct(const double* X, double* Y) {
         launch_to_f32(ctx, X, X32.p, pl.N * R);
         if (mixed_near == 0)
             launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, X32.p, Y,
@@ -554,7 +642,6 @@ struct Operator {
             };
             launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
         }
-        applies32 += 1;
     }
 
     // Z (+)= M^-1 V with the chosen right preconditioner.
@@ -741,6 +828,8 @@ Opts normalize(const gpx_solve_opts* o) {
     r.far_quad = o->far_quad;
     r.mixed_near = o->mixed_near;
     r.mixed_m2l = o->mixed_m2l;
+    r.graphs = o->no_graphs ? 0 : 1;
+    r.batch_streams = o->batch_streams;
     return r;
 }
 
@@ -794,6 +883,7 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     pr.op.reset(new Operator(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get()));
     pr.op->precond = o.precond;
     pr.op->mixed_near = o.mixed_near;
+    pr.op->use_graphs = o.graphs != 0;
     // TF32 M2L only with centroid sources: with 2x2 Gauss sources the leaf
     // expansions carry large alternating node values (sources slightly outside
     // their leaf box) and the TF32 inputs lose 1e-2 of the far field.
@@ -1106,6 +1196,7 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
     Operator opT(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get());
     opT.precond = o.precond;
     opT.mixed_near = o.mixed_near;
+    opT.use_graphs = o.graphs != 0;
     opT.tc32 = op.tc32;
     opT.assemble(&op);
     DBuf<double> Q, Lam;

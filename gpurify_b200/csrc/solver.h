@@ -20,6 +20,8 @@ struct Opts {
     int far_quad = 0;
     int mixed_near = 0;
     int mixed_m2l = 0;
+    int graphs = 1;         // capture operator applies into CUDA graphs
+    int batch_streams = 0;  // batched solves: concurrent streams (0 -> default)
 };
 Opts normalize(const gpx_solve_opts* o);
 

@@ -103,7 +103,11 @@ typedef struct {
                                 far-field sources, else the factored low-rank form on FP32 CUDA cores;
                                 1 -> always the factored form (compressed operators); 2 -> tensor cores
                                 at orders 4 and 5 also with Gauss-point sources */
-    int32_t reserved[5];
+    int32_t no_graphs;       /* 1: launch every operator apply directly instead of replaying it as a
+                                captured CUDA graph (results are identical) */
+    int32_t batch_streams;   /* gpx_cap_solve_batched: windows solved concurrently, one stream each;
+                                0 -> 8 */
+    int32_t reserved[3];
 } gpx_solve_opts;
 
 typedef struct {
