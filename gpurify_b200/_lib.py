@@ -29,7 +29,7 @@ EXPORTS = (
     "gpx_cap_solve_batched", "gpx_operator_apply", "gpx_potential_matrix", "gpx_cap_solve_groups",
     "gpx_extract_quasistatic", "gpx_bridge_panelize", "gpx_plan_check", "gpx_ctx_stream",
     "gpx_ctx_set_profiling", "gpx_ctx_kernel_stats", "gpx_ctx_reset_stats", "gpx_cap_solve_small_static",
-    "gpx_cap_sensitivity",
+    "gpx_cap_sensitivity", "gpx_autotune",
 )
 KERNEL_CLASSES = ("near_assemble", "near_apply", "p2m", "m2m", "m2l", "l2l", "l2p", "gs_dot", "gs_axpy", "vec",
                   "small")
@@ -64,6 +64,14 @@ class SolveReport(C.Structure):
         ("t_total_s", C.c_double), ("t_near_assembly_s", C.c_double), ("kernel_launches", C.c_int64),
         ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
     ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("est_rel_err", C.c_double), ("apply_ms", C.c_double), ("setup_ms", C.c_double),
+                ("candidates", C.c_int32), ("from_cache", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -145,6 +153,8 @@ def load(build_if_missing: bool = True):
                                            C.POINTER(C.c_double), C.POINTER(i64)]
         L.gpx_ctx_reset_stats.argtypes = [vp]
         L.gpx_cap_solve_small_static.argtypes = [vp, i64, vp, vp, i32, vp]
+        L.gpx_autotune.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), C.c_double, C.c_char_p,
+                                   C.POINTER(SolveOpts), C.POINTER(TuneReport)]
         L.gpx_cap_sensitivity.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), i32, vp, vp, vp,
                                           C.POINTER(SolveReport)]
         for name in EXPORTS:
@@ -215,6 +225,22 @@ class Context:
         rep = SolveReport()
         self._check(self.L.gpx_cap_solve(self.h, C.byref(pb), C.byref(opts(**kw)), Cm.ctypes.data, C.byref(rep)))
         return Cm, rep.as_dict()
+
+    def autotune(self, verts, cond, ncond, target=1e-4, cache_path=None, **kw):
+        """gpx_autotune: returns (options dict to pass to cap_solve, report)."""
+        v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)
+        c = np.ascontiguousarray(cond, dtype=np.int32)
+        pb = PanelProblem(len(v), v.ctypes.data, c.ctypes.data, ncond)
+        base = opts(**kw)
+        tuned = SolveOpts()
+        rep = TuneReport()
+        path = cache_path.encode() if cache_path else None
+        self._check(self.L.gpx_autotune(self.h, C.byref(pb), C.byref(base), float(target), path, C.byref(tuned),
+                                        C.byref(rep)))
+        out = dict(kw)
+        for k in ("order", "max_level", "far_quad", "mixed_near", "dense_below"):
+            out[k] = getattr(tuned, k)
+        return out, rep.as_dict()
 
     def cap_solve_batched(self, problems, **kw):
         """Many independent windows in one call (gpx_cap_solve_batched).

@@ -237,6 +237,26 @@ gpx_status gpx_cap_sensitivity(gpx_ctx* ctx, const gpx_panel_problem* pb, const 
     });
 }
 
+gpx_status gpx_autotune(gpx_ctx* ctx, const gpx_panel_problem* pb, const gpx_solve_opts* base, double target_rel_err,
+                        const char* cache_path, gpx_solve_opts* tuned, gpx_tune_report* report) {
+    if (!ctx || !pb || !tuned) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
+    if (report) std::memset(report, 0, sizeof(*report));
+    return guarded(ctx, [&] {
+        Opts o = normalize(base);
+        Opts t;
+        autotune(ctx->impl, pb->n_panels, pb->verts, pb->conductor, pb->n_conductors, o, target_rel_err, cache_path,
+                 t, report);
+        gpx_solve_opts res{};
+        if (base) res = *base;
+        res.order = t.order;
+        res.max_level = t.max_level;
+        res.far_quad = t.far_quad;
+        res.mixed_near = t.mixed_near;
+        res.dense_below = -1;
+        *tuned = res;
+    });
+}
+
 gpx_status gpx_operator_apply(gpx_ctx* ctx, const gpx_panel_problem* pb, const gpx_solve_opts* opts, int32_t nrhs,
                               const double* sigma, double* y, gpx_solve_report* report) {
     if (!ctx || !pb || !sigma || !y) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");

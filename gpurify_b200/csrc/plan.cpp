@@ -25,27 +25,6 @@ inline P3 scl(P3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
 inline P3 crs(P3 a, P3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
 inline double len(P3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
 
-// Area-weighted fan centroid and area of a quad whose 4th vertex may repeat
-// the 3rd (integrals/panel.rs:29-67).
-void panel_centroid_area(const double* v, double* c, double* a) {
-    P3 q[4];
-    for (int i = 0; i < 4; ++i) q[i] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
-    int nv = (q[3].x == q[2].x && q[3].y == q[2].y && q[3].z == q[2].z) ? 3 : 4;
-    double asum = 0.0;
-    P3 acc{0.0, 0.0, 0.0};
-    for (int i = 1; i < nv - 1; ++i) {
-        double t = len(crs(sub(q[i], q[0]), sub(q[i + 1], q[0]))) * 0.5;
-        P3 tc = scl(add(add(q[0], q[i]), q[i + 1]), 1.0 / 3.0);
-        acc = add(acc, scl(tc, t));
-        asum += t;
-    }
-    P3 r = asum == 0.0 ? q[0] : scl(acc, 1.0 / asum);
-    c[0] = r.x;
-    c[1] = r.y;
-    c[2] = r.z;
-    *a = asum;
-}
-
 inline uint64_t spread3(uint32_t v) {
     uint64_t x = v & 0x1fffff;
     x = (x | x << 32) & 0x1f00000000ffffull;
@@ -134,6 +113,28 @@ void qr_truncate_product(const std::vector<double>& g, int m, double eps, double
 }
 
 }  // namespace
+
+// Area-weighted fan centroid and area of a quad whose 4th vertex may repeat
+// the 3rd (integrals/panel.rs:29-67).
+void panel_centroid_area(const double* v, double* c, double* a) {
+    P3 q[4];
+    for (int i = 0; i < 4; ++i) q[i] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    int nv = (q[3].x == q[2].x && q[3].y == q[2].y && q[3].z == q[2].z) ? 3 : 4;
+    double asum = 0.0;
+    P3 acc{0.0, 0.0, 0.0};
+    for (int i = 1; i < nv - 1; ++i) {
+        double t = len(crs(sub(q[i], q[0]), sub(q[i + 1], q[0]))) * 0.5;
+        P3 tc = scl(add(add(q[0], q[i]), q[i + 1]), 1.0 / 3.0);
+        acc = add(acc, scl(tc, t));
+        asum += t;
+    }
+    P3 r = asum == 0.0 ? q[0] : scl(acc, 1.0 / asum);
+    c[0] = r.x;
+    c[1] = r.y;
+    c[2] = r.z;
+    *a = asum;
+}
+
 
 std::vector<double> cheb_roots(int n) {
     std::vector<double> v(n);

@@ -73,6 +73,9 @@ struct Plan {
 // Build the plan.  depth >= 1; depth 1 makes every pair near.
 void build_plan(Plan& p, int64_t n, const double* verts, const int32_t* cond, int ncond, int order, int depth);
 
+// Area-weighted fan centroid and area of one panel (integrals/panel.rs:29-67).
+void panel_centroid_area(const double* v, double* c, double* a);
+
 // Chebyshev roots and 1-D interpolation weights (fmm/chebyshev.rs:11-74).
 std::vector<double> cheb_roots(int n);
 void cheb_weights(double x, int n, const double* roots, double* out);

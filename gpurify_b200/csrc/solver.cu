@@ -1275,4 +1275,228 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
     }
 }
 
+
+namespace {
+
+// y[s] = sum_l M[s][l] * sigma[l][r] for the sampled rows (one block per row
+// and probe column).
+__global__ void k_rows_apply(const double* __restrict__ M, int64_t N, const double* __restrict__ sigma, int R,
+                             double* __restrict__ y) {
+    const int s = blockIdx.x, r = blockIdx.y;
+    double acc = 0.0;
+    for (int64_t l = threadIdx.x; l < N; l += blockDim.x) acc += M[(int64_t)s * N + l] * sigma[l * R + r];
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) y[(int64_t)s * R + r] = red[0];
+}
+
+std::string tune_signature(int64_t n, const double* verts, int ncond, const Opts& o, double target) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, edge = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double* v = verts + 12 * i;
+        for (int k = 0; k < 4; ++k)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], v[3 * k + d]);
+                hi[d] = std::max(hi[d], v[3 * k + d]);
+            }
+        double e = 0.0;
+        for (int d = 0; d < 3; ++d) e += (v[3 + d] - v[d]) * (v[3 + d] - v[d]);
+        edge += std::sqrt(e);
+    }
+    edge /= (double)n;
+    const double side = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "p%d_n%d_c%d_a%.1f_%.1f_%.1f_e%d_t%d", o.precision, (int)std::lround(std::log2((double)n) * 2),
+                  (int)std::lround(std::log2((double)ncond + 1.0) * 2), (hi[0] - lo[0]) / side, (hi[1] - lo[1]) / side,
+                  (hi[2] - lo[2]) / side, (int)std::lround(std::log2(side / std::max(edge, 1e-300)) * 2),
+                  (int)std::lround(-std::log10(target) * 4));
+    return buf;
+}
+
+}  // namespace
+
+void autotune(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& base,
+              double target, const char* cache_path, Opts& out, gpx_tune_report* rep) {
+    check_problem(n, verts, cond, ncond, base);
+    if (!(target > 0.0) || target >= 1.0) throw Error(GPX_ERR_INVALID_ARG, "target relative error must be in (0, 1)");
+    gpx_tune_report r{};
+    out = base;
+    const std::string sig = tune_signature(n, verts, ncond, base, target);
+    if (cache_path && *cache_path) {
+        if (FILE* f = std::fopen(cache_path, "r")) {
+            char key[256];
+            int order, depth, fq, mn;
+            double err, ams, sms;
+            while (std::fscanf(f, "%255s %d %d %d %d %lf %lf %lf", key, &order, &depth, &fq, &mn, &err, &ams, &sms) == 8)
+                if (sig == key) {
+                    out.order = order;
+                    out.max_level = depth;
+                    out.far_quad = fq;
+                    out.mixed_near = mn;
+                    out.dense_below = -1;
+                    r.est_rel_err = err;
+                    r.apply_ms = ams;
+                    r.setup_ms = sms;
+                    r.from_cache = 1;
+                }
+            std::fclose(f);
+            if (r.from_cache) {
+                if (rep) *rep = r;
+                return;
+            }
+        }
+    }
+    cudaStream_t s = ctx.stream;
+    const bool mixed = base.precision == GPX_PREC_MIXED;
+    // sampled target rows (evenly spaced in caller order) and their exact
+    // all-pairs rows of the potential-coefficient matrix
+    const int ns = (int)std::min<int64_t>(n, 512);
+    std::vector<double> pts((size_t)ns * 3);
+    std::vector<int64_t> rows(ns);
+    for (int k = 0; k < ns; ++k) {
+        rows[k] = (int64_t)((double)k * (double)n / (double)ns);
+        double c[3], a;
+        panel_centroid_area(verts + 12 * rows[k], c, &a);
+        for (int d = 0; d < 3; ++d) pts[3 * k + d] = c[d];
+    }
+    // probe charge densities: constant, two smooth patterns, seeded random signs
+    const int R = 4;
+    std::vector<double> sig_h((size_t)n * R);
+    uint64_t lcg = 0x9E3779B97F4A7C15ull;
+    for (int64_t i = 0; i < n; ++i) {
+        double c[3], a;
+        panel_centroid_area(verts + 12 * i, c, &a);
+        lcg = lcg * 6364136223846793005ull + 1442695040888963407ull;
+        sig_h[(size_t)i * R + 0] = 1.0;
+        sig_h[(size_t)i * R + 1] = 1.0 + 0.5 * std::sin(1e6 * c[0]) * std::cos(1e6 * c[1]);
+        sig_h[(size_t)i * R + 2] = 1.0 + 0.5 * std::cos(7e5 * (c[0] + c[1]) + 3e6 * c[2]);
+        sig_h[(size_t)i * R + 3] = (lcg >> 63) ? 1.0 : -1.0;
+    }
+    DBuf<double> dv, dpts, M, dsig, yex;
+    dv.upload(verts, (size_t)n * 12, s);
+    dpts.upload(pts, s);
+    M.alloc((size_t)ns * n, s);
+    dsig.upload(sig_h, s);
+    yex.alloc((size_t)ns * R, s);
+    launch_potential_matrix(ctx, dv.p, n, dpts.p, ns, M.p, kCoulomb);
+    k_rows_apply<<<dim3(ns, R), 256, 0, s>>>(M.p, n, dsig.p, R, yex.p);
+    GPX_LAUNCH_CHECK();
+    ctx.launches += 1;
+    std::vector<double> yexact((size_t)ns * R);
+    yex.download(yexact.data(), yexact.size());
+    GPX_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> ymax(R, 0.0);
+    for (int k = 0; k < ns; ++k)
+        for (int q = 0; q < R; ++q) ymax[q] = std::max(ymax[q], std::fabs(yexact[(size_t)k * R + q]));
+
+    Opts probe = base;
+    probe.dense_below = -1;
+    Opts autodepth = base;
+    autodepth.max_level = -1;
+    autodepth.dense_below = -1;
+    const int d0 = std::max(2, choose_depth(autodepth, n));
+    struct Cand {
+        int order, depth, fq, mn;
+    };
+    std::vector<Cand> cands;
+    for (int order : {4, 5, 6})
+        for (int depth = std::max(2, d0 - 1); depth <= d0 + 1; ++depth)
+            for (int fq : {0, 1})
+                for (int mn : (mixed ? std::vector<int>{0, 1} : std::vector<int>{0})) cands.push_back({order, depth, fq, mn});
+    double best_score = INFINITY;
+    bool found = false;
+    cudaEvent_t e0, e1;
+    GPX_CUDA(cudaEventCreate(&e0));
+    GPX_CUDA(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{e0, e1};
+    for (const Cand& c : cands) {
+        Opts o = probe;
+        o.order = c.order;
+        o.max_level = c.depth;
+        o.far_quad = c.fq;
+        o.mixed_near = c.mn;
+        o.precond = base.precond;
+        Prepared pr;
+        const double t0 = now_s();
+        prepare(ctx, n, verts, cond, ncond, o, R, c.depth, pr);
+        GPX_CUDA(cudaStreamSynchronize(s));
+        const double setup_ms = (now_s() - t0) * 1e3;
+        r.candidates += 1;
+        // FP64 apply for the discretisation error (the mixed path converges to
+        // the FP64 operator's solution), in the plan's panel order
+        std::vector<double> xs((size_t)n * R);
+        for (int64_t k = 0; k < n; ++k)
+            for (int q = 0; q < R; ++q) xs[(size_t)k * R + q] = sig_h[(size_t)pr.plan.perm[k] * R + q];
+        DBuf<double> X, Y;
+        X.upload(xs, s);
+        Y.alloc(xs.size(), s);
+        pr.op->apply(X.p, Y.p);
+        std::vector<double> ys(xs.size());
+        Y.download(ys.data(), ys.size());
+        GPX_CUDA(cudaStreamSynchronize(s));
+        std::vector<int64_t> inv(n);
+        for (int64_t k = 0; k < n; ++k) inv[pr.plan.perm[k]] = k;
+        // error of the smooth probes (the fourth, random-sign probe cancels
+        // and is not scored); the Maxwell matrix's error measures about 1.7x
+        // this, so the target is met with a factor of 2 to spare
+        double err = 0.0;
+        for (int k = 0; k < ns; ++k)
+            for (int q = 0; q < 3; ++q)
+                err = std::max(err, std::fabs(ys[(size_t)inv[rows[k]] * R + q] - yexact[(size_t)k * R + q]) / ymax[q]);
+        if (2.0 * err > target) continue;
+        // time the applies the solve iterates (two warm, three timed)
+        auto one = [&] {
+            if (mixed)
+                pr.op->apply32(X.p, Y.p);
+            else
+                pr.op->apply(X.p, Y.p);
+        };
+        one();
+        one();
+        GPX_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < 3; ++k) one();
+        GPX_CUDA(cudaEventRecord(e1, s));
+        GPX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        GPX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const double apply_ms = ms / 3.0;
+        if (mixed) pr.op->check_tc();
+        // a solve: setup plus about 100 applies (inner iterations of a 1e-8 solve)
+        const double score = setup_ms + 100.0 * apply_ms;
+        if (score < best_score) {
+            best_score = score;
+            found = true;
+            out.order = c.order;
+            out.max_level = c.depth;
+            out.far_quad = c.fq;
+            out.mixed_near = c.mn;
+            out.dense_below = -1;
+            r.est_rel_err = err;
+            r.apply_ms = apply_ms;
+            r.setup_ms = setup_ms;
+        }
+    }
+    if (!found)
+        throw Error(GPX_ERR_CAPACITANCE, "no far-field configuration reaches the target error " + std::to_string(target));
+    if (cache_path && *cache_path) {
+        if (FILE* f = std::fopen(cache_path, "a")) {
+            std::fprintf(f, "%s %d %d %d %d %.6e %.6e %.6e\n", sig.c_str(), out.order, out.max_level, out.far_quad,
+                         out.mixed_near, r.est_rel_err, r.apply_ms, r.setup_ms);
+            std::fclose(f);
+        }
+    }
+    if (rep) *rep = r;
+}
+
 }  // namespace gpx

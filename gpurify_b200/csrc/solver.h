@@ -40,6 +40,13 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
 void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o,
                      int np, const double* V, double* C, double* dCdp, gpx_solve_report* rep);
 
+// Autotuner: the fastest far-field configuration (order, depth, far-field
+// source model, near-apply engine) whose sampled operator error against the
+// all-pairs rows is at most `target`; cached by problem signature in
+// cache_path (one line per signature) when given.
+void autotune(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& base,
+              double target, const char* cache_path, Opts& out, gpx_tune_report* rep);
+
 // y = P sigma (sigma, y: n x R row-major in caller panel order).
 void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int R, const double* sigma, double* y,
                     gpx_solve_report* rep);

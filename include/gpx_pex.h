@@ -21,6 +21,8 @@
  *                            windows; each window is one gpx_cap_solve)
  *   gpx_cap_sensitivity      (no reference counterpart: adjoint dC/dp beside the
  *                            capacitance result of cap/fmm_solver.rs:147-172)
+ *   gpx_autotune             (no reference counterpart: replaces the fixed order 4 /
+ *                            depth 4 of bridge.rs:403 by a measured choice)
  *   gpx_operator_apply       crates/pex/src/quasistatic/cap/fmm_solver.rs:109-129
  *                            `FmmCapOperator::apply`, for R right-hand sides
  *   gpx_potential_matrix     crates/pex/src/quasistatic/cap/solver.rs:81-97
@@ -163,6 +165,32 @@ gpx_status gpx_cap_solve_batched(gpx_ctx* ctx, const gpx_panel_problem* problems
 gpx_status gpx_cap_sensitivity(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
                                int32_t n_params, const double* vert_velocity, double* maxwell_out,
                                double* dmaxwell_out, gpx_solve_report* report);
+
+/* ---- autotuner (no reference counterpart: the reference hard-codes order 4,
+ * depth 4, bridge.rs:403) ----
+ * Chooses the far-field configuration for a representative panel problem: for
+ * every candidate (Chebyshev order 4..6, octree depth around the automatic
+ * choice, centroid or Gauss-point far-field sources, and in mixed precision
+ * the tensor-core or FP32 near apply) it measures the operator's error on 512
+ * sampled rows against the exact all-pairs rows (three smooth probe charge
+ * densities) and times the operator apply on the device; the fastest
+ * candidate whose error is at most target_rel_err / 2 wins (score: set-up +
+ * 100 applies; the Maxwell matrix's error measures about 1.7x the sampled
+ * operator error).
+ * `tuned` receives `base` with order, max_level, far_quad, mixed_near and
+ * dense_below (-1) replaced.  With cache_path (may be NULL) the choice is
+ * looked up in / appended to that text file, keyed by a signature of the
+ * problem (size, conductor count, aspect, mesh scale, precision, target). */
+typedef struct {
+    double est_rel_err;  /* sampled operator error of the chosen configuration */
+    double apply_ms;     /* its operator apply, device milliseconds */
+    double setup_ms;     /* its plan + near-field assembly, milliseconds */
+    int32_t candidates;  /* configurations evaluated (0 when taken from the cache) */
+    int32_t from_cache;
+} gpx_tune_report;
+gpx_status gpx_autotune(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* base,
+                        double target_rel_err, const char* cache_path, gpx_solve_opts* tuned,
+                        gpx_tune_report* report);
 
 /* y = P sigma for `nrhs` columns (sigma, y: n_panels x nrhs row-major, panel
  * order of `problem`), P the precorrected operator the solver uses. */
