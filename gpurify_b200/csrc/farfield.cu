@@ -493,6 +493,7 @@ __global__ void __launch_bounds__(MW) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
     const int64_t k0g = f.tgt_col_off[t], K = f.tgt_col_off[t + 1] - k0g;
     if (K == 0) return;
     const int Kp = (int)((K + 3) & ~int64_t(3));
+    const T sc = (T)(f.box_scale ? f.box_scale[t] : scale);
     const T* A = f.Tm + f.tgt_base[t] * R + rc;  // column-major: A[c][r] at c * R + r
     const int m = min(64, R - rc);
     extern __shared__ __align__(16) unsigned char facu_smem[];
@@ -553,7 +554,7 @@ __global__ void __launch_bounds__(MW) k_m2l_fac_u(FacM2L<T> f, int b0, T* __rest
             const int mm = m0 + tx + TXN * j;
             if (mm >= ns) continue;
             T* dst = L + ((int64_t)t * R + rc + r) * ns + mm;
-            *dst += (T)scale * acc[i][j];
+            *dst += sc * acc[i][j];
         }
     }
 }
@@ -562,7 +563,7 @@ inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b);
 
 template <class T, int N>
 void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y, int R,
-                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
+                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all) {
     cudaStream_t s = c.stream;
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>();
     constexpr size_t smem = tree_smem<T, N>();
@@ -589,14 +590,24 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
-    for (int l = 2; l <= Lv; ++l) {
-        const int b0 = f.lvl_off[l], nb = f.lvl_off[l + 1] - b0;
-        if (nb == 0) continue;
+    if (m2l_all && Lv >= 2) {
+        const int b0 = f.lvl_off[2], nb = f.lvl_off[Lv + 1] - b0;
         const double pairs = (double)(f.m2l_off[b0 + nb] - f.m2l_off[b0]);
-        if (pairs == 0) continue;
-        KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
-        m2l(l, b0, nb, 1.0 / f.lvl_half[l]);
-        c.launches += 1;
+        if (pairs > 0) {
+            KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
+            m2l(-1, b0, nb, 0.0);
+            c.launches += 1;
+        }
+    } else {
+        for (int l = 2; l <= Lv; ++l) {
+            const int b0 = f.lvl_off[l], nb = f.lvl_off[l + 1] - b0;
+            if (nb == 0) continue;
+            const double pairs = (double)(f.m2l_off[b0 + nb] - f.m2l_off[b0]);
+            if (pairs == 0) continue;
+            KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
+            m2l(l, b0, nb, 1.0 / f.lvl_half[l]);
+            c.launches += 1;
+        }
     }
     for (int l = 2; l < Lv; ++l) {
         const int pb0 = f.lvl_off[l], npb = f.lvl_off[l + 1] - pb0, ncb = f.lvl_off[l + 2] - f.lvl_off[l + 1];
@@ -618,13 +629,13 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
 
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
-                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l) {
+                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all) {
     switch (p.n) {
-        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
-        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
-        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
-        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
-        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l); break;
+        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
+        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
+        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
+        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
+        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
         default: throw Error(GPX_ERR_INVALID_ARG, "far field runs Chebyshev orders 2 to 6");
     }
 }
@@ -667,8 +678,8 @@ void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const dou
 
 template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*,
                                        const FarWeights<double>&, double*, int, int, double*, double*, double,
-                                       const M2LLevelFn<double>&);
+                                       const M2LLevelFn<double>&, bool);
 template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, const FarWeights<float>&,
-                                      double*, int, int, float*, float*, double, const M2LLevelFn<float>&);
+                                      double*, int, int, float*, float*, double, const M2LLevelFn<float>&, bool);
 
 }  // namespace gpx

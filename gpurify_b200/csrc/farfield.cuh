@@ -28,9 +28,11 @@ struct FarWeights {
 // nbox x Rb x ns each (Rb >= R rows per box, node stride ns); E is written in
 // full by P2M and M2M (zero padding rows and nodes), L is zeroed here.  M2L is
 // supplied per level.
+// m2l_all_levels: the M2L callback runs once for every level (level -1,
+// first box of level 2, box count of levels 2..L) instead of once per level.
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
-                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l);
+                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all_levels = false);
 
 // FP64 M2L of one level with CUDA-core FMAs (dense operators).
 void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale);
@@ -52,6 +54,7 @@ struct FacM2L {
     const int64_t* tgt_ut = nullptr;    // per contraction index: offset of its Ut row
     const int64_t* tgt_base = nullptr;  // nbox: sum of padded block widths of earlier boxes
     T* Tm = nullptr;                    // target-major intermediate (Kp columns of R values per target)
+    const double* box_scale = nullptr;  // per box: 1 / half-width of its level (all-levels launches)
 };
 // Phase-1 work items of one level: (source box, first column, column count <= kFacItemCols).
 constexpr int kFacItemCols = 512;
@@ -79,8 +82,9 @@ struct TcLevel {
 // L[t][r][m] = scale * sum K[m][l] E[s][r][l] for order-4 (node stride 64)
 // or order-5 (node stride 128) expansions; K32: 343 x ns x ns TF32-rounded
 // operators; R a multiple of 64.  err receives a nonzero code if a bounded
-// wait on the tensor-core pipeline expired.
+// wait on the tensor-core pipeline expired.  box_scale (per box, may be null):
+// each target box's own scale, for launches that cover several levels.
 void launch_m2l_tc(Ctx& c, const TcLevel& lv, int ns, const float* E, float* L, const float* K32, int R, float scale,
-                   int* err);
+                   const double* box_scale, int* err);
 
 }  // namespace gpx

@@ -92,7 +92,7 @@ struct TcCfg {
 template <int NS>
 __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __restrict__ E, float* __restrict__ L,
                                                      const float* __restrict__ K32, int R, float scale,
-                                                     int* __restrict__ err) {
+                                                     const double* __restrict__ box_scale, int* __restrict__ err) {
     using C = TcCfg<NS>;
     constexpr int S = C::kStages;
     extern __shared__ uint8_t smem_raw[];
@@ -200,6 +200,7 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
         const int row = warp * 32 + lane;
         const int t = row < 64 ? tA : tB;
         float* dst = (t >= 0) ? L + ((int64_t)t * R + r0 + (row & 63)) * NS : nullptr;
+        const float sc = (t >= 0 && box_scale) ? (float)box_scale[t] : scale;
 #pragma unroll
         for (int cb = 0; cb < NS / 16; ++cb) {
             uint32_t v[16];
@@ -208,8 +209,8 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
             if (dst) {
 #pragma unroll
                 for (int k = 0; k < 16; k += 4) {
-                    const float4 o = make_float4(scale * __uint_as_float(v[k]), scale * __uint_as_float(v[k + 1]),
-                                                 scale * __uint_as_float(v[k + 2]), scale * __uint_as_float(v[k + 3]));
+                    const float4 o = make_float4(sc * __uint_as_float(v[k]), sc * __uint_as_float(v[k + 1]),
+                                                 sc * __uint_as_float(v[k + 2]), sc * __uint_as_float(v[k + 3]));
                     *reinterpret_cast<float4*>(dst + cb * 16 + k) = o;
                 }
             }
@@ -222,23 +223,25 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
 }
 
 template <int NS>
-void launch_ns(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale, int* err) {
+void launch_ns(Ctx& c, const TcLevel& lv, const float* E, float* L, const float* K32, int R, float scale,
+               const double* box_scale, int* err) {
     using Cf = TcCfg<NS>;
     set_smem_once(k_m2l_tc<NS>, (int)Cf::kSmem);
-    k_m2l_tc<NS><<<dim3(lv.nitems, R / 64), kThreads, Cf::kSmem, c.stream>>>(lv, E, L, K32, R, scale, err);
+    k_m2l_tc<NS><<<dim3(lv.nitems, R / 64), kThreads, Cf::kSmem, c.stream>>>(lv, E, L, K32, R, scale, box_scale,
+                                                                             err);
     GPX_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 void launch_m2l_tc(Ctx& c, const TcLevel& lv, int ns, const float* E, float* L, const float* K32, int R, float scale,
-                   int* err) {
+                   const double* box_scale, int* err) {
     if (lv.nitems == 0) return;
     if (R % 64 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core M2L needs R a multiple of 64");
     if (ns == 64)
-        launch_ns<64>(c, lv, E, L, K32, R, scale, err);
+        launch_ns<64>(c, lv, E, L, K32, R, scale, box_scale, err);
     else if (ns == 128)
-        launch_ns<128>(c, lv, E, L, K32, R, scale, err);
+        launch_ns<128>(c, lv, E, L, K32, R, scale, box_scale, err);
     else
         throw Error(GPX_ERR_INTERNAL, "tensor-core M2L runs node strides 64 and 128 (orders 4 and 5)");
 }

@@ -245,6 +245,7 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
 // same octant class in Morton order sharing one offset loop).
 struct TcLists {
     std::vector<TcLevel> level;  // per level (empty below 2)
+    TcLevel all;                 // levels 2..L in one list
     DBuf<int32_t> item_t, item_off, slot, srcA, srcB;
 };
 
@@ -304,6 +305,14 @@ void build_tc_lists(Ctx& ctx, const Plan& pl, TcLists& out) {
         v.srcA = out.srcA.p;
         v.srcB = out.srcB.p;
     }
+    // every level in one launch (the per-level item lists are contiguous)
+    out.all = TcLevel();
+    if (pl.L >= 2) {
+        out.all = out.level[2];
+        int n = 0;
+        for (int l = 2; l <= pl.L; ++l) n += ranges[l].n;
+        out.all.nitems = n;
+    }
 }
 
 // The precorrected potential operator of one plan for R right-hand sides, in
@@ -350,6 +359,8 @@ struct Operator {
     DBuf<double> T64;
     DBuf<float> T32;
     std::vector<FacLevel> fac_level;
+    FacLevel fac_all;
+    DBuf<double> box_scale;
     DBuf<int32_t> fi_src, fi_cnt;
     DBuf<int64_t> fi_c0;
     int Rb32 = 0;
@@ -454,6 +465,13 @@ struct Operator {
             }
             E64.alloc((size_t)pl.nbox() * ns * R, s);
             L64.alloc((size_t)pl.nbox() * ns * R, s);
+            {
+                // M2L scale 1/half of each box's level, for launches covering all levels
+                std::vector<double> sc(pl.nbox(), 0.0);
+                for (int l = 0; l <= pl.L; ++l)
+                    for (int32_t b = pl.lvl_off[l]; b < pl.lvl_off[l + 1]; ++b) sc[b] = 1.0 / pl.lvl_half[l];
+                box_scale.upload(sc, s);
+            }
             if (m2l && m2l->factored_ok) setup_factored();
         }
         if (mixed) {
@@ -555,6 +573,14 @@ struct Operator {
             fl.item_c0 = fi_c0.p + lvl_first[l];
             fl.item_cnt = fi_cnt.p + lvl_first[l];
         }
+        // all levels in one launch: the phase-1 items of levels 2..L, and the
+        // M2L scale 1/half of each box's level
+        const int lf = std::min(2, pl.L + 1);
+        fac_all.nitems = lvl_first[pl.L + 1] - lvl_first[lf];
+        fac_all.item_src = fi_src.p + lvl_first[lf];
+        fac_all.item_c0 = fi_c0.p + lvl_first[lf];
+        fac_all.item_cnt = fi_cnt.p + lvl_first[lf];
+
         src_col_off.upload(scol, s);
         col_vt.upload(cvt, s);
         col_tgt.upload(ctg, s);
@@ -564,6 +590,7 @@ struct Operator {
         tgt_base.upload(base, s);
         auto wire = [&](auto& f) {
             f.ns = ns;
+            f.box_scale = box_scale.p;
             f.src_col_off = src_col_off.p;
             f.col_vt = col_vt.p;
             f.col_tgt = col_tgt.p;
@@ -600,11 +627,12 @@ struct Operator {
         if (has_far()) {
             M2LLevelFn<double> m2l_fn = [&](int level, int b0, int nb, double scale) {
                 if (factored)
-                    launch_m2l_fac<double>(ctx, fac64, fac_level[level], b0, nb, L64.p, E64.p, R, scale);
+                    launch_m2l_fac<double>(ctx, fac64, level < 0 ? fac_all : fac_level[level], b0, nb, L64.p, E64.p,
+                                           R, scale);
                 else
                     launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
             };
-            launch_far_field<double>(ctx, d.v, d.far, X, w64, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
+            launch_far_field<double>(ctx, d.v, d.far, X, w64, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn, factored);
         }
     }
 
@@ -613,11 +641,12 @@ struct Operator {
         if (!has_far()) return;
         M2LLevelFn<double> m2l_fn = [&](int level, int b0, int nb, double scale) {
             if (factored)
-                launch_m2l_fac<double>(ctx, fac64, fac_level[level], b0, nb, L64.p, E64.p, R, scale);
+                launch_m2l_fac<double>(ctx, fac64, level < 0 ? fac_all : fac_level[level], b0, nb, L64.p, E64.p, R,
+                                       scale);
             else
                 launch_m2l64(ctx, d.v, b0, nb, L64.p, E64.p, R, scale);
         };
-        launch_far_field<double>(ctx, d.v, d.far, X, w, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn);
+        launch_far_field<double>(ctx, d.v, d.far, X, w, Y, R, R, E64.p, L64.p, kCoulomb, m2l_fn, factored);
     }
 
     // Y = A32 X: FP32 near field, FP32 far field with TF32 tensor-core M2L.
@@ -635,12 +664,13 @@ struct Operator {
         if (has_far()) {
             M2LLevelFn<float> m2l_fn = [&](int level, int b0, int nb, double scale) {
                 if (tc32)
-                    launch_m2l_tc(ctx, tc.level[level], node_stride(pl.n), E32.p, L32.p, m2l->K32.p, Rb32,
-                                  (float)scale, tc_err.p);
+                    launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], node_stride(pl.n), E32.p, L32.p,
+                                  m2l->K32.p, Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
                 else
-                    launch_m2l_fac<float>(ctx, fac32, fac_level[level], b0, nb, L32.p, E32.p, Rb32, scale);
+                    launch_m2l_fac<float>(ctx, fac32, level < 0 ? fac_all : fac_level[level], b0, nb, L32.p, E32.p,
+                                          Rb32, scale);
             };
-            launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn);
+            launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true);
         }
     }
 
