@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--inner-tol-exp", type=int, default=0, help="mixed: inner GMRES tolerance 10^-x (0: default)")
     ap.add_argument("--mixed-near", type=int, default=0, help="mixed near apply: 0 TF32 tensor cores, 1 FP32 CUDA cores")
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 QR-compressed M2L operators (reference), 1 exact")
+    ap.add_argument("--mixed-m2l", type=int, default=2,
+                    help="mixed M2L: 0 auto, 1 factored on CUDA cores, 2 tensor cores also with Gauss sources")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     return ap.parse_args()
@@ -126,6 +128,17 @@ def load_peaks():
         return d["hbm_gbs"], d["bf16_tflops"], "measured"
     except Exception:
         return 6650.0, 1590.0, "fallback"
+
+
+def max_over_ranks(x: float, dist, device: str = "cuda") -> float:
+    """The job's time is the slowest rank's: all-reduce MAX (no-op alone)."""
+    if not dist:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def workload(rank: int, nets: int, side: float = 40.0):
@@ -208,10 +221,7 @@ def time_solves(ctx, verts, cond, ncond, solve_kw, steps, warmup, stream, dist, 
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     clocks = sampler.stop()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     ctx.set_profiling(True)
     ctx.reset_stats()
     t0 = time.perf_counter()
@@ -272,7 +282,7 @@ def main():
     ctx = _lib.Context(local)
     base_kw = dict(order=args.order, max_level=args.depth, skip_ground_rhs=1, tol=1e-8, restart=args.restart,
                    far_quad=args.far_quad, precond=args.precond, inner_tol_exp=args.inner_tol_exp,
-                   mixed_near=args.mixed_near, m2l_mode=args.m2l_mode)
+                   mixed_near=args.mixed_near, m2l_mode=args.m2l_mode, mixed_m2l=args.mixed_m2l)
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     lay = workload(rank, args.nets, args.side)
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
@@ -304,10 +314,7 @@ def main():
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = min(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
 
     accuracy = None
     if args.accuracy and rank == 0:
@@ -326,7 +333,8 @@ def main():
                                                / np.abs(np.diag(runs["fp64"]["C"][:R, :R]))[:, None]).max())
 
     if rank == 0:
-        tc_m2l = head == "mixed" and args.order in (4, 5) and (args.far_quad == 0 or args.m2l_mode == 1)
+        tc_m2l = head == "mixed" and args.order in (4, 5) and args.mixed_m2l != 1 and (
+            args.far_quad == 0 or args.m2l_mode == 1 or args.mixed_m2l == 2)
         roof = roofline_of(hr["ks"], hr["ms_prof"], "tcgen05 TF32" if tc_m2l else
                            ("FP32 CUDA cores, factored low-rank operators" if head == "mixed" else
                             "FP64 CUDA cores, factored low-rank operators"))
@@ -355,6 +363,7 @@ def main():
                                    f"panels, {N} panels, {R} RHS, GMRES tol 1e-8",
                        "panels": N, "rhs": R, "precision": head, "order": args.order, "depth": args.depth,
                        "far_quad": args.far_quad, "restart": args.restart, "precond": args.precond,
+                       "mixed_m2l": args.mixed_m2l,
                        "parallelism": f"replicas x{world}", "l2": "working set (Krylov basis > 1 GB) >> L2"},
             "panel_rhs_per_s": world * N * R / (ms_step * 1e-3),
             "precisions": per_prec,
