@@ -57,7 +57,9 @@ def parse():
     ap.add_argument("--side", type=float, default=40.0, help="window side in um")
     ap.add_argument("--restart", type=int, default=200, help="GMRES restart length")
     ap.add_argument("--far-quad", type=int, default=1, help="0 centroid lumping (reference), 1 Gauss points")
-    ap.add_argument("--precond", type=int, default=1, help="0 diagonal Jacobi (reference), 1 leaf block-Jacobi")
+    ap.add_argument("--precond", type=int, default=-1,
+                    help="0 diagonal Jacobi (reference), 1 / 2 leaf block-Jacobi with 48- / 96-panel blocks; "
+                         "-1: 2 for the FP64 path, 1 for the mixed path (fastest of each, measured)")
     ap.add_argument("--accuracy", type=int, default=1, help="1: report errors against the FP64 all-pairs solve")
     ap.add_argument("--inner-tol-exp", type=int, default=0, help="mixed: inner GMRES tolerance 10^-x (0: default)")
     ap.add_argument("--mixed-near", type=int, default=0, help="mixed near apply: 0 TF32 tensor cores, 1 FP32 CUDA cores")
@@ -296,6 +298,8 @@ def main():
     runs = {}
     for prec in precisions:
         kw = dict(base_kw, precision=_lib.PREC_MIXED if prec == "mixed" else _lib.PREC_FP64)
+        if args.precond < 0:
+            kw["precond"] = 1 if prec == "mixed" else 2
         ms, reps, ks, clocks, C, launches, ms_prof = time_solves(ctx, verts, cond, ncond, kw, args.steps,
                                                                  args.warmup, stream, dist, local)
         runs[prec] = dict(ms=ms, reps=reps, ks=ks, clocks=clocks, C=C, kw=kw, launches=launches, ms_prof=ms_prof)
@@ -321,7 +325,7 @@ def main():
         # FP64 all-pairs reference (every entry by the exact Wilton integral),
         # GMRES to 1e-10; errors normalised by the row's diagonal entry.
         Cd, _ = ctx.cap_solve(verts, cond, ncond, dense_below=2**31 - 1, skip_ground_rhs=1, tol=1e-10,
-                              precond=args.precond)
+                              precond=max(args.precond, 1))
         Cn = Cd[:R, :R]
         dg = np.abs(np.diag(Cn))
         accuracy = {"reference": "FP64 all-pairs Wilton operator, GMRES tol 1e-10",
@@ -362,7 +366,8 @@ def main():
             "config": {"workload": f"routing window {args.nets} nets {args.side:g}x{args.side:g}um 3 layers, 0.25um "
                                    f"panels, {N} panels, {R} RHS, GMRES tol 1e-8",
                        "panels": N, "rhs": R, "precision": head, "order": args.order, "depth": args.depth,
-                       "far_quad": args.far_quad, "restart": args.restart, "precond": args.precond,
+                       "far_quad": args.far_quad, "restart": args.restart,
+                       "precond": {pr: runs[pr]["kw"]["precond"] for pr in runs},
                        "mixed_m2l": args.mixed_m2l,
                        "parallelism": f"replicas x{world}", "l2": "working set (Krylov basis > 1 GB) >> L2"},
             "panel_rhs_per_s": world * N * R / (ms_step * 1e-3),

@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X,
 //   Y[j][r] += coef * sum_m S_j[m] L[leaf][r][m],  S_j[m] = wx[a] wy[b] wz[c]
 // (the centroid's separable weights), or S_j = Wt[j] (times a_j if mul_area)
 // when explicit weights are given.
-// 256 threads; thread (tj, tr) holds panels tj + 16 i and rows tr + 16 q.
+// 256 threads, 32 panels per chunk; thread (tj, tr) holds panels tj + 16 i
+// (i < 2) and rows tr + 16 q (q < 4).
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L, const T* __restrict__ Wt,
                                              bool mul_area, double* __restrict__ Y, int R, int Rb, double coef) {
@@ -106,25 +107,26 @@ __global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L,
     const int rc = blockIdx.y * 64;
     const int64_t j0 = p.leaf_begin[t], j1 = p.leaf_begin[t + 1];
     const T* src = L + ((int64_t)(p.leaf_box0 + t) * Rb + rc) * NS;
-    __shared__ T wv[64][3 * N];
-    __shared__ T Ss[64][33];
+    constexpr int JP = 32;  // panels per chunk (leaves hold a few tens of panels)
+    __shared__ T wv[JP][3 * N];
+    __shared__ T Ss[JP][33];
     __shared__ T Ls[32][65];
     const int tid = threadIdx.x, tj = tid >> 4, tr = tid & 15;
-    for (int64_t jb = j0; jb < j1; jb += 64) {
-        const int cnt = (int)min((int64_t)64, j1 - jb);
+    for (int64_t jb = j0; jb < j1; jb += JP) {
+        const int cnt = (int)min((int64_t)JP, j1 - jb);
         __syncthreads();
-        for (int e = tid; e < 64 * 3 * N; e += 256) {
+        for (int e = tid; e < JP * 3 * N; e += 256) {
             const int jj = e / (3 * N);
             wv[jj][e % (3 * N)] = jj < cnt ? (T)p.w1d[jb * 3 * N + e] : (T)0;
         }
-        T acc[4][4];
+        T acc[2][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][q] = (T)0;
         for (int m0 = 0; m0 < N3; m0 += 32) {
             __syncthreads();
-            for (int e = tid; e < 64 * 32; e += 256) {
+            for (int e = tid; e < JP * 32; e += 256) {
                 const int jj = e >> 5, mm = e & 31, m = m0 + mm;
                 T v = (T)0;
                 if (m < N3 && jj < cnt) {
@@ -141,19 +143,19 @@ __global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L,
             __syncthreads();
 #pragma unroll 8
             for (int k = 0; k < 32; ++k) {
-                T a[4], b[4];
+                T a[2], b[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = Ss[tj + 16 * i][k];
+                for (int i = 0; i < 2; ++i) a[i] = Ss[tj + 16 * i][k];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) b[q] = Ls[k][tr + 16 * q];
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 2; ++i)
 #pragma unroll
                     for (int q = 0; q < 4; ++q) acc[i][q] += a[i] * b[q];
             }
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < 2; ++i) {
             const int jj = tj + 16 * i;
             if (jj >= cnt) continue;
 #pragma unroll
@@ -216,41 +218,73 @@ __global__ void __launch_bounds__(256) k_m2m_tree(DevPlan p, int pb0, const int3
         }
     }
     __syncthreads();
+    // Each stage runs one 1-D line per thread (the n values along the
+    // contracted axis), so the index arithmetic is per line, not per value.
     // z: B[q][r][(a,b,c')] = sum_oz sum_c Z_oz[c'][c] A[q|oz<<2][r][(a,b,c)]
-    for (int e = threadIdx.x; e < 4 * RC * N3; e += blockDim.x) {
-        const int q = e / (RC * N3), r = (e / N3) % RC, m = e % N3, ab = m / N, cp = m % N;
+    for (int e = threadIdx.x; e < 4 * RC * NN; e += blockDim.x) {
+        const int q = e / (RC * NN), r = (e / NN) % RC, ab = e % NN;
         const T* a0 = A + (q * RC + r) * N3 + ab * N;
         const T* a1 = A + ((q | 4) * RC + r) * N3 + ab * N;
-        T s = (T)0;
+        T x0[N], x1[N];
 #pragma unroll
-        for (int c = 0; c < N; ++c) s += M1[2][0][cp * N + c] * a0[c] + M1[2][1][cp * N + c] * a1[c];
-        B[e] = s;
+        for (int c = 0; c < N; ++c) {
+            x0[c] = a0[c];
+            x1[c] = a1[c];
+        }
+        T* out = B + (q * RC + r) * N3 + ab * N;
+#pragma unroll
+        for (int cp = 0; cp < N; ++cp) {
+            T s = (T)0;
+#pragma unroll
+            for (int c = 0; c < N; ++c) s += M1[2][0][cp * N + c] * x0[c] + M1[2][1][cp * N + c] * x1[c];
+            out[cp] = s;
+        }
     }
     __syncthreads();
     // y: C[ox][r][(a,b',c)] = sum_oy sum_b Y_oy[b'][b] B[ox|oy<<1][r][(a,b,c)]
-    for (int e = threadIdx.x; e < 2 * RC * N3; e += blockDim.x) {
-        const int ox = e / (RC * N3), r = (e / N3) % RC, m = e % N3, a = m / NN, bp = (m / N) % N, c = m % N;
+    for (int e = threadIdx.x; e < 2 * RC * NN; e += blockDim.x) {
+        const int ox = e / (RC * NN), r = (e / NN) % RC, ac = e % NN, a = ac / N, c = ac % N;
         const T* b0 = B + (ox * RC + r) * N3 + a * NN + c;
         const T* b1 = B + ((ox | 2) * RC + r) * N3 + a * NN + c;
-        T s = (T)0;
+        T x0[N], x1[N];
 #pragma unroll
-        for (int b = 0; b < N; ++b) s += M1[1][0][bp * N + b] * b0[b * N] + M1[1][1][bp * N + b] * b1[b * N];
-        C[e] = s;
+        for (int b = 0; b < N; ++b) {
+            x0[b] = b0[b * N];
+            x1[b] = b1[b * N];
+        }
+        T* out = C + (ox * RC + r) * N3 + a * NN + c;
+#pragma unroll
+        for (int bp = 0; bp < N; ++bp) {
+            T s = (T)0;
+#pragma unroll
+            for (int b = 0; b < N; ++b) s += M1[1][0][bp * N + b] * x0[b] + M1[1][1][bp * N + b] * x1[b];
+            out[bp * N] = s;
+        }
     }
     __syncthreads();
-    // x: E_par[r][(a',b,c)] = sum_ox sum_a X_ox[a'][a] C[ox][r][(a,b,c)]
+    // x: E_par[r][(a',b,c)] = sum_ox sum_a X_ox[a'][a] C[ox][r][(a,b,c)]; padding nodes zero
     T* dst = E + ((int64_t)pb * Rb + r0) * NS;
-    for (int e = threadIdx.x; e < rc * NS; e += blockDim.x) {
-        const int r = e / NS, m = e % NS;
-        T s = (T)0;
-        if (m < N3) {
-            const int ap = m / NN, bc = m % NN;
-            const T* c0 = C + r * N3 + bc;
-            const T* c1 = C + (RC + r) * N3 + bc;
+    for (int e = threadIdx.x; e < rc * NN; e += blockDim.x) {
+        const int r = e / NN, bc = e % NN;
+        const T* c0 = C + r * N3 + bc;
+        const T* c1 = C + (RC + r) * N3 + bc;
+        T x0[N], x1[N];
 #pragma unroll
-            for (int a = 0; a < N; ++a) s += M1[0][0][ap * N + a] * c0[a * NN] + M1[0][1][ap * N + a] * c1[a * NN];
+        for (int a = 0; a < N; ++a) {
+            x0[a] = c0[a * NN];
+            x1[a] = c1[a * NN];
         }
-        dst[(int64_t)r * NS + m] = s;
+#pragma unroll
+        for (int ap = 0; ap < N; ++ap) {
+            T s = (T)0;
+#pragma unroll
+            for (int a = 0; a < N; ++a) s += M1[0][0][ap * N + a] * x0[a] + M1[0][1][ap * N + a] * x1[a];
+            dst[(int64_t)r * NS + ap * NN + bc] = s;
+        }
+    }
+    for (int e = threadIdx.x; e < rc * (NS - N3); e += blockDim.x) {
+        const int r = e / (NS - N3), m = N3 + e % (NS - N3);
+        dst[(int64_t)r * NS + m] = (T)0;
     }
 }
 
@@ -276,39 +310,63 @@ __global__ void __launch_bounds__(256) k_l2l_tree(DevPlan p, int pb0, const int3
         P[e] = r < rc ? src[(int64_t)r * NS + m] : (T)0;
     }
     __syncthreads();
-    // x: C[ox][r][(a,b,c)] = sum_a' X_ox[a'][a] P[r][(a',b,c)]
-    for (int e = threadIdx.x; e < 2 * RC * N3; e += blockDim.x) {
-        const int ox = e / (RC * N3), r = (e / N3) % RC, m = e % N3, a = m / NN, bc = m % NN;
+    // x: C[ox][r][(a,b,c)] = sum_a' X_ox[a'][a] P[r][(a',b,c)]  (one line per thread)
+    for (int e = threadIdx.x; e < RC * NN; e += blockDim.x) {
+        const int r = e / NN, bc = e % NN;
         const T* pr = P + r * N3 + bc;
-        T s = (T)0;
+        T x[N];
 #pragma unroll
-        for (int ap = 0; ap < N; ++ap) s += M1[0][ox][ap * N + a] * pr[ap * NN];
-        C[e] = s;
+        for (int ap = 0; ap < N; ++ap) x[ap] = pr[ap * NN];
+#pragma unroll
+        for (int ox = 0; ox < 2; ++ox) {
+            T* out = C + (ox * RC + r) * N3 + bc;
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                T s = (T)0;
+#pragma unroll
+                for (int ap = 0; ap < N; ++ap) s += M1[0][ox][ap * N + a] * x[ap];
+                out[a * NN] = s;
+            }
+        }
     }
     __syncthreads();
     // y: B[q][r][(a,b,c)] = sum_b' Y_oy[b'][b] C[ox][r][(a,b',c)],  q = ox | oy<<1
-    for (int e = threadIdx.x; e < 4 * RC * N3; e += blockDim.x) {
-        const int q = e / (RC * N3), r = (e / N3) % RC, m = e % N3, a = m / NN, b = (m / N) % N, c = m % N;
-        const T* cr = C + ((q & 1) * RC + r) * N3 + a * NN + c;
-        const int oy = q >> 1;
-        T s = (T)0;
+    for (int e = threadIdx.x; e < 2 * RC * NN; e += blockDim.x) {
+        const int ox = e / (RC * NN), r = (e / NN) % RC, ac = e % NN, a = ac / N, c = ac % N;
+        const T* cr = C + (ox * RC + r) * N3 + a * NN + c;
+        T x[N];
 #pragma unroll
-        for (int bp = 0; bp < N; ++bp) s += M1[1][oy][bp * N + b] * cr[bp * N];
-        B[e] = s;
+        for (int bp = 0; bp < N; ++bp) x[bp] = cr[bp * N];
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+            T* out = B + ((ox | (oy << 1)) * RC + r) * N3 + a * NN + c;
+#pragma unroll
+            for (int b = 0; b < N; ++b) {
+                T s = (T)0;
+#pragma unroll
+                for (int bp = 0; bp < N; ++bp) s += M1[1][oy][bp * N + b] * x[bp];
+                out[b * N] = s;
+            }
+        }
     }
     __syncthreads();
     // z, straight into each existing child: L_child[r][(a,b,c)] += sum_c' Z_oz[c'][c] B[oct&3][r][(a,b,c')]
     const int cf = child_first[pb], cc = child_count[pb];
-    for (int ch = cf; ch < cf + cc; ++ch) {
+    for (int e = threadIdx.x; e < cc * rc * NN; e += blockDim.x) {
+        const int k = e / (rc * NN), r = (e / NN) % rc, ab = e % NN;
+        const int ch = cf + k;
         const int oc = p.box_octant[ch], q = oc & 3, oz = oc >> 2;
-        T* dst = L + ((int64_t)ch * Rb + r0) * NS;
-        for (int e = threadIdx.x; e < rc * N3; e += blockDim.x) {
-            const int r = e / N3, m = e % N3, ab = m / N, c = m % N;
-            const T* br = B + (q * RC + r) * N3 + ab * N;
+        const T* br = B + (q * RC + r) * N3 + ab * N;
+        T x[N];
+#pragma unroll
+        for (int cp = 0; cp < N; ++cp) x[cp] = br[cp];
+        T* dst = L + ((int64_t)ch * Rb + r0 + r) * NS + ab * N;
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
             T s = (T)0;
 #pragma unroll
-            for (int cp = 0; cp < N; ++cp) s += M1[2][oz][cp * N + c] * br[cp];
-            dst[(int64_t)r * NS + m] += s;
+            for (int cp = 0; cp < N; ++cp) s += M1[2][oz][cp * N + c] * x[cp];
+            dst[c] += s;
         }
     }
 }

@@ -1,4 +1,4 @@
-// Leaf block-Jacobi preconditioner.  Blocks are runs of up to 48
+// Leaf block-Jacobi preconditioner.  Blocks are runs of up to KB (48 or 96)
 // consecutive panels inside one leaf; each block's matrix is the exact
 // (Wilton) self-interaction sub-block of the near field, inverted once by
 // Gauss-Jordan elimination with partial pivoting in FP64 and applied as a
@@ -14,9 +14,9 @@ namespace gpx {
 
 namespace {
 
-constexpr int kB = 48;
-
-// One CTA per block: invert A (b x b) read from the leaf's near block.
+// One CTA per block: invert A (b x b) read from the leaf's near block.  A and
+// its inverse I live in dynamic shared memory (2 x KB x (KB+1) doubles).
+template <int kB>
 __global__ void __launch_bounds__(256) k_block_invert(DevPlan p, const double* __restrict__ P,
                                                       const int32_t* __restrict__ blk_leaf,
                                                       const int32_t* __restrict__ blk_row0,
@@ -26,7 +26,9 @@ __global__ void __launch_bounds__(256) k_block_invert(DevPlan p, const double* _
     const int t = blk_leaf[bi], r0 = blk_row0[bi], b = blk_size[bi];
     const int Sp = (p.near_S[t] + 3) & ~3;
     const double* Pt = P + p.nval_off[t];
-    __shared__ double A[kB][kB + 1], I[kB][kB + 1];
+    extern __shared__ double bj_smem[];
+    double(*A)[kB + 1] = reinterpret_cast<double(*)[kB + 1]>(bj_smem);
+    double(*I)[kB + 1] = reinterpret_cast<double(*)[kB + 1]>(bj_smem + kB * (kB + 1));
     __shared__ int piv;
     __shared__ double pval;
     for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) {
@@ -82,17 +84,23 @@ __global__ void __launch_bounds__(256) k_block_invert(DevPlan p, const double* _
     for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) out[e] = I[e / kB][e % kB];
 }
 
-// One CTA per (block, 64-column chunk): Z[rows] = Minv V[rows].
+// One CTA per (block, 64-column chunk): Z[rows] = Minv V[rows].  256
+// threads; thread (ty, tx) holds rows ty + 16 a (a < KB/16) and columns
+// tx + 16 q (q < 4) in registers, so each shared-memory read feeds several
+// multiply-adds.
+template <int kB>
 __global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ Minv,
                                                      const int64_t* __restrict__ blk_start,
                                                      const int32_t* __restrict__ blk_size, const double* __restrict__ V,
                                                      double* __restrict__ Z, int R, int add) {
+    constexpr int RA = kB / 16;
     const int bi = blockIdx.x;
     const int rc = blockIdx.y * 64;
     const int64_t s0 = blk_start[bi];
     const int b = blk_size[bi];
-    __shared__ double Ms[kB][kB + 1];
-    __shared__ double Vs[kB][65];
+    extern __shared__ double bj_smem[];
+    double(*Ms)[kB + 1] = reinterpret_cast<double(*)[kB + 1]>(bj_smem);
+    double(*Vs)[65] = reinterpret_cast<double(*)[65]>(bj_smem + kB * (kB + 1));
     const double* M = Minv + (int64_t)bi * kB * kB;
     for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) Ms[e / kB][e % kB] = M[e];
     for (int e = threadIdx.x; e < kB * 64; e += blockDim.x) {
@@ -100,19 +108,41 @@ __global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ 
         Vs[i][c] = (i < b && rc + c < R) ? V[(s0 + i) * R + rc + c] : 0.0;
     }
     __syncthreads();
-    const int c = threadIdx.x & 63, rg = threadIdx.x >> 6;  // 4 row groups
-    for (int i = rg; i < b; i += 4) {
-        if (rc + c >= R) break;
-        double acc = 0.0;
-        for (int k = 0; k < b; ++k) acc += Ms[i][k] * Vs[k][c];
-        double* z = Z + (s0 + i) * R + rc + c;
-        *z = add ? *z + acc : acc;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[RA][4];
+#pragma unroll
+    for (int a = 0; a < RA; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+    for (int k = 0; k < b; ++k) {
+        double m[RA], v[4];
+#pragma unroll
+        for (int a = 0; a < RA; ++a) m[a] = Ms[ty + 16 * a][k];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = Vs[k][tx + 16 * q];
+#pragma unroll
+        for (int a = 0; a < RA; ++a)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[a][q] += m[a] * v[q];
+    }
+#pragma unroll
+    for (int a = 0; a < RA; ++a) {
+        const int i = ty + 16 * a;
+        if (i >= b) continue;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = tx + 16 * q;
+            if (rc + c >= R) continue;
+            double* z = Z + (s0 + i) * R + rc + c;
+            *z = add ? *z + acc[a][q] : acc[a][q];
+        }
     }
 }
 
 }  // namespace
 
 void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double* P) {
+    const int kB = block;
     std::vector<int32_t> leaf, row0, size;
     std::vector<int64_t> start;
     for (int64_t k = 0; k + 1 < (int64_t)pl.leaf_begin.size(); ++k) {
@@ -134,7 +164,14 @@ void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double*
     d_sing.zero();
     {
         KTimer t(c, K_SMALL, 8.0 * nblk * kB * kB * 2, 2.0 * nblk * (double)kB * kB * kB);
-        k_block_invert<<<nblk, 256, 0, c.stream>>>(dp, P, d_leaf.p, d_row0.p, d_size.p, Minv.p, d_sing.p);
+        const int smem = (int)(sizeof(double) * 2 * kB * (kB + 1));
+        if (kB == 96) {
+            set_smem_once(k_block_invert<96>, smem);
+            k_block_invert<96><<<nblk, 256, smem, c.stream>>>(dp, P, d_leaf.p, d_row0.p, d_size.p, Minv.p, d_sing.p);
+        } else {
+            set_smem_once(k_block_invert<48>, smem);
+            k_block_invert<48><<<nblk, 256, smem, c.stream>>>(dp, P, d_leaf.p, d_row0.p, d_size.p, Minv.p, d_sing.p);
+        }
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
@@ -145,8 +182,17 @@ void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double*
 }
 
 void BlockJacobi::apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add) const {
+    const int kB = block;
     KTimer t(c, K_VEC, 8.0 * (2.0 * N * R + (double)nblk * kB * kB), 2.0 * (double)N * kB * R);
-    k_block_apply<<<dim3(nblk, (R + 63) / 64), 256, 0, c.stream>>>(Minv.p, d_start.p, d_size.p, V, Z, R, add ? 1 : 0);
+    const int smem = (int)(sizeof(double) * (kB * (kB + 1) + kB * 65));
+    const dim3 g(nblk, (R + 63) / 64);
+    if (kB == 96) {
+        set_smem_once(k_block_apply<96>, smem);
+        k_block_apply<96><<<g, 256, smem, c.stream>>>(Minv.p, d_start.p, d_size.p, V, Z, R, add ? 1 : 0);
+    } else {
+        set_smem_once(k_block_apply<48>, smem);
+        k_block_apply<48><<<g, 256, smem, c.stream>>>(Minv.p, d_start.p, d_size.p, V, Z, R, add ? 1 : 0);
+    }
     GPX_LAUNCH_CHECK();
     c.launches += 1;
     (void)N;

@@ -5,9 +5,10 @@
 
 namespace gpx {
 
-// Leaf block-Jacobi: blocks of up to 48 consecutive panels of one leaf,
-// inverted from the exact near-field self block.
+// Leaf block-Jacobi: blocks of up to `block` (48 or 96) consecutive panels
+// of one leaf, inverted from the exact near-field self block.
 struct BlockJacobi {
+    int block = 48;
     int nblk = 0;
     DBuf<int32_t> d_leaf, d_row0, d_size, d_sing;
     DBuf<int64_t> d_start;

@@ -444,7 +444,10 @@ struct Operator {
             launch_near_assemble(ctx, d.v, pl.nnz(), P.p, kCoulomb);
         GPX_CUDA(cudaEventRecord(e1, s));
         launch_diag_inv(ctx, d.v, P.p, inv_diag.p);
-        if (precond == 1) bj.build(ctx, pl, d.v, P.p);
+        if (precond >= 1) {
+            bj.block = precond == 2 ? 96 : 48;
+            bj.build(ctx, pl, d.v, P.p);
+        }
         GPX_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         GPX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -676,7 +679,7 @@ struct Operator {
 
     // Z (+)= M^-1 V with the chosen right preconditioner.
     void precondition(const double* V, double* Z, bool add) {
-        if (precond == 1)
+        if (precond >= 1)
             bj.apply(ctx, V, Z, pl.N, R, add);
         else
             launch_diag_scale(ctx, V, inv_diag.p, Z, pl.N, R, add);
@@ -884,7 +887,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
                     "the mixed-precision path runs exact M2L operators on the tensor cores, at orders 4 and 5 "
                     "with centroid far-field sources (far_quad 0)");
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
-    if (o.precond != 0 && o.precond != 1) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0 or 1");
+    if (o.precond < 0 || o.precond > 2) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0, 1 or 2");
     if (o.mixed_near != 0 && o.mixed_near != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0 or 1");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1 or 2");
     for (int64_t i = 0; i < n; ++i) {

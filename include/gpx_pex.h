@@ -91,7 +91,8 @@ typedef struct {
     int32_t max_restarts;    /* 0 -> 50 */
     int32_t dense_below;     /* all-pairs (no far field) below this many panels;
                                 0 -> 500 (bridge.rs:30), -1 -> never */
-    int32_t precond;         /* 0 diagonal Jacobi (fmm_solver.rs:133-162), 1 leaf block-Jacobi */
+    int32_t precond;         /* 0 diagonal Jacobi (fmm_solver.rs:133-162), 1 leaf block-Jacobi (48-panel
+                                blocks), 2 leaf block-Jacobi (96-panel blocks) */
     int32_t skip_ground_rhs; /* 1: do not solve the substrate column (the reference solves it);
                                 the per-net result needs only the nets' columns */
     int32_t inner_tol_exp;   /* mixed: floor of the adaptive inner tolerance, 10^-x; 0 -> 3 with the

@@ -184,8 +184,8 @@ def test_reference_known_answers_on_gpu(ctx, orc):
     assert abs(cf[0, 0] - FOUR_PI_EPS0) / FOUR_PI_EPS0 < 0.03
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_block_jacobi_matches_diagonal(ctx, orc, precision):
+@pytest.mark.parametrize("precision,block", [(0, 1), (1, 1), (0, 2), (1, 2)])
+def test_block_jacobi_matches_diagonal(ctx, orc, precision, block):
     """The leaf block-Jacobi preconditioner changes the iteration, not the
     solution: same Maxwell matrix within the GMRES tolerance, fewer iterations."""
     lay = layouts.routing_window(12, 15.0, seed=11)
@@ -194,7 +194,7 @@ def test_block_jacobi_matches_diagonal(ctx, orc, precision):
     nc = len(p["nets"]) + 1
     kw = dict(order=4, max_level=5, dense_below=-1, precision=precision)
     C0, r0 = ctx.cap_solve(p["verts"], p["cond"], nc, precond=0, **kw)
-    C1, r1 = ctx.cap_solve(p["verts"], p["cond"], nc, precond=1, **kw)
+    C1, r1 = ctx.cap_solve(p["verts"], p["cond"], nc, precond=block, **kw)
     assert r1["converged"] == 1
     assert r1["iterations"] < r0["iterations"]
     d = np.abs(np.diag(C0))
