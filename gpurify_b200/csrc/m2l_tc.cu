@@ -12,22 +12,26 @@
 // so every A row (one right-hand side) and every B row (one target node) is a
 // contiguous K-major row: the contraction over source nodes runs in chunks of
 // 32 TF32 (one 128-byte swizzle atom per row), and each chunk is one pipeline
-// stage: A (128 rows x 128 B) and B (NS rows x 128 B) copied with cp.async
-// straight into the 128-byte-swizzled layout the MMA descriptors name, kStages
-// stages in a ring, loads running kStages - 2 chunks ahead of the MMAs.  One
-// thread issues the four K=8 MMAs of a chunk and commits them to the stage's
-// mbarrier; a stage is refilled only after the MMAs that read it completed.
+// stage: A (128 rows x 128 B) and B (NS rows x 128 B).
+// Warp-specialised: four producer warps copy each stage with cp.async
+// straight into the 128-byte-swizzled layout the MMA descriptors name and
+// signal the stage's `full` mbarrier with cp.async.mbarrier.arrive (128
+// arrivals); one thread of the fifth warp waits on `full`, issues the four
+// K=8 MMAs of the chunk and commits them to the stage's `empty` mbarrier,
+// which the producers wait on before refilling the stage.  kStages stages
+// are in flight, with no block-wide barrier in the main loop.
 // The tensor cores read FP32 operands as TF32 (the operator table is stored
 // rounded to TF32, the expansions are truncated by the hardware).
 // Every mbarrier wait is bounded; on expiry the kernel records an error code,
-// drains (bounded) its own MMAs, frees its TMEM and returns.
+// drains (bounded) its own MMAs and copies, frees its TMEM and returns.
 #include "farfield.cuh"
 
 namespace gpx {
 
 namespace {
 
-constexpr int kThreads = 128;
+constexpr int kProducers = 128;            // four producer warps
+constexpr int kThreads = kProducers + 32;  // + the MMA warp
 constexpr int kWaitLimit = 1 << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -81,7 +85,7 @@ struct TcCfg {
     static constexpr uint32_t kATile = 128 * 128;              // 128 rows x 128 B
     static constexpr uint32_t kBTile = NS * 128;               // NS rows x 128 B
     static constexpr uint32_t kStage = kATile + kBTile;        // multiple of 1024
-    static constexpr uint32_t kSmem = kStages * kStage + 1024 + 128;  // + alignment slack + barriers
+    static constexpr uint32_t kSmem = kStages * kStage + 1024 + 256;  // + alignment slack + barriers
     static constexpr uint32_t kTmemCols = NS;                  // 64 or 128 FP32 columns
     static constexpr int kChunks = NS / 32;                    // contraction chunks per entry
     // Instruction descriptor: D F32, A/B TF32, both K-major, N = NS, M = 128.
@@ -99,8 +103,8 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* sbase = smem_raw + (base - raw);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S * C::kStage);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S * C::kStage);  // full[S], empty[S]
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * S);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int item = blockIdx.x;
     const int r0 = blockIdx.y * 64;
@@ -108,11 +112,18 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     const int e0 = lv.item_off[item], e1 = lv.item_off[item + 1];
     const int total = (e1 - e0) * C::kChunks;
 
+    uint64_t* full = bars;
+    uint64_t* empty = bars + S;
+    __shared__ int s_bad;
     if (tid == 0) {
-        for (int k = 0; k < S; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[k])));
+        for (int k = 0; k < S; ++k) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[k])), "r"(kProducers));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[k])));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_bad = 0;
     }
-    if (warp == 0) {
+    if (warp == 4) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(C::kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -122,81 +133,84 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tslot;
 
-    // Copy chunk q (entry q / kChunks, source nodes 32 (q % kChunks) ..) into
-    // its stage: A rows 0..63 from tA's source, 64..127 from tB's source
-    // (zero-filled where the target has no source at this offset), B rows =
-    // the operator's target nodes.  Every thread copies 8 A and NS/16 B
-    // 16-byte pieces; 8 consecutive threads read one 128-byte row segment.
+    // Copies of chunk q (entry q / kChunks, source nodes 32 (q % kChunks) ..)
+    // into stage q % S: A rows 0..63 from tA's source, 64..127 from tB's
+    // source (zero-filled where the target has no source at this offset), B
+    // rows = the operator's target nodes.  Every producer thread copies 8 A and
+    // NS/16 B 16-byte pieces; 8 consecutive threads read one 128-byte row
+    // segment.
     auto issue = [&](int q) {
-        if (q < total) {
-            const int e = e0 + q / C::kChunks, kc = q % C::kChunks;
-            const int sa = lv.srcA[e], sb = lv.srcB[e];
-            const uint32_t a = base + (uint32_t)(q % S) * C::kStage;
-            const uint32_t b = a + C::kATile;
+        const int e = e0 + q / C::kChunks, kc = q % C::kChunks;
+        const int sa = lv.srcA[e], sb = lv.srcB[e];
+        const uint32_t a = base + (uint32_t)(q % S) * C::kStage;
+        const uint32_t b = a + C::kATile;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int id = tid + kThreads * i, row = id >> 3, pc = id & 7;
-                const int src = row < 64 ? sa : sb;
-                const float* g = src >= 0 ? E + ((int64_t)src * R + r0 + (row & 63)) * NS + kc * 32 + pc * 4 : E;
-                cp16(a + swz(row, pc), g, src >= 0);
-            }
-            const float* Ko = K32 + (int64_t)lv.slot[e] * NS * NS + kc * 32;
-#pragma unroll
-            for (int i = 0; i < NS / 16; ++i) {
-                const int id = tid + kThreads * i, row = id >> 3, pc = id & 7;
-                cp16(b + swz(row, pc), Ko + (int64_t)row * NS + pc * 4, true);
-            }
+        for (int i = 0; i < 8; ++i) {
+            const int id = tid + kProducers * i, row = id >> 3, pc = id & 7;
+            const int src = row < 64 ? sa : sb;
+            const float* g = src >= 0 ? E + ((int64_t)src * R + r0 + (row & 63)) * NS + kc * 32 + pc * 4 : E;
+            cp16(a + swz(row, pc), g, src >= 0);
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
+        const float* Ko = K32 + (int64_t)lv.slot[e] * NS * NS + kc * 32;
+#pragma unroll
+        for (int i = 0; i < NS / 16; ++i) {
+            const int id = tid + kProducers * i, row = id >> 3, pc = id & 7;
+            cp16(b + swz(row, pc), Ko + (int64_t)row * NS + pc * 4, true);
+        }
     };
 
-    bool bad = false;
-    int issued = 0;
-    for (int q = 0; q < S - 2; ++q) issue(q);
-    for (int q = 0; q < total; ++q) {
-        if (q >= 2) {  // the stage of chunk q + S - 2 was last read by the MMAs of chunk q - 2
-            const bool ok = mbar_wait(smem_u32(&bars[(q - 2) % S]), (uint32_t)(((q - 2) / S) & 1));
-            if (__syncthreads_or(!ok)) {
-                bad = true;
+    int issued = 0;  // chunks whose MMAs were committed (MMA thread)
+    if (tid < kProducers) {
+        for (int q = 0; q < total; ++q) {
+            const int st = q % S;
+            if (q >= S && !mbar_wait(smem_u32(&empty[st]), (uint32_t)(((q / S) - 1) & 1))) {
+                atomicExch(&s_bad, 1);
                 break;
             }
+            if (*(volatile int*)&s_bad) break;
+            issue(q);
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st]))
+                         : "memory");
         }
-        issue(q + S - 2);
-        asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (tid == kProducers) {
+        for (int q = 0; q < total; ++q) {
+            const int st = q % S;
+            if (!mbar_wait(smem_u32(&full[st]), (uint32_t)((q / S) & 1))) {
+                atomicExch(&s_bad, 1);
+                break;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t abase = base + (uint32_t)(q % S) * C::kStage, bbase = abase + C::kATile;
+            const uint32_t abase = base + (uint32_t)st * C::kStage, bbase = abase + C::kATile;
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const uint64_t ad = desc_sw128(abase + (uint32_t)s * 32u);
-                const uint64_t bd = desc_sw128(bbase + (uint32_t)s * 32u);
-                const uint32_t acc = (q > 0 || s > 0) ? 1u : 0u;
+            for (int k = 0; k < 4; ++k) {
+                const uint64_t ad = desc_sw128(abase + (uint32_t)k * 32u);
+                const uint64_t bd = desc_sw128(bbase + (uint32_t)k * 32u);
+                const uint32_t acc = (q > 0 || k > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
                     "l"(ad), "l"(bd), "r"(C::kIdesc), "r"(acc));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&bars[q % S]))
+                             smem_u32(&empty[st]))
                          : "memory");
+            issued = q + 1;
         }
-        issued = q + 1;
+        // Drain: the last commit covers every MMA issued before it (after an
+        // expired wait too, so the TMEM is idle before it is freed).
+        if (issued > 0) {
+            const int last = issued - 1;
+            if (!mbar_wait(smem_u32(&empty[last % S]), (uint32_t)((last / S) & 1))) atomicExch(&s_bad, 1);
+        }
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // Drain: the last commit covers every MMA issued before it (after an
-    // expired wait too, so the TMEM is idle before it is freed).
-    if (issued > 0) {
-        const int last = issued - 1;
-        const bool ok = mbar_wait(smem_u32(&bars[last % S]), (uint32_t)((last / S) & 1));
-        if (__syncthreads_or(!ok)) bad = true;
-    }
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (bad) {
+    if (s_bad) {
         if (tid == 0) atomicExch(err, 1);
-    } else if (issued > 0) {
-        // Epilogue: warp w reads TMEM lanes 32w..32w+31 = rows of D.
+    } else if (tid < kProducers && total > 0) {
+        // Epilogue: warp w (0..3) reads TMEM lanes 32w..32w+31 = rows of D.
         const int row = warp * 32 + lane;
         const int t = row < 64 ? tA : tB;
         float* dst = (t >= 0) ? L + ((int64_t)t * R + r0 + (row & 63)) * NS : nullptr;
@@ -218,7 +232,7 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 4)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::kTmemCols));
 }
 
