@@ -81,7 +81,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 template <int NS>
 struct TcCfg {
-    static constexpr int kStages = 6;
+    static constexpr int kStages = 2;
     static constexpr uint32_t kATile = 128 * 128;              // 128 rows x 128 B
     static constexpr uint32_t kBTile = NS * 128;               // NS rows x 128 B
     static constexpr uint32_t kStage = kATile + kBTile;        // multiple of 1024
