@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 QR-compressed M2L operators (reference), 1 exact")
     ap.add_argument("--mixed-m2l", type=int, default=2,
                     help="mixed M2L: 0 auto, 1 factored on CUDA cores, 2 tensor cores also with Gauss sources")
+    ap.add_argument("--workload", default="window64", choices=["window64", "twowires", "batch", "bus"],
+                    help="window64: the headline 64-net window; twowires: two met1 wires on a 0.05 um mesh; "
+                         "batch: many uneven windows in one batched call; bus: met2 bus sensitivities")
+    ap.add_argument("--windows", type=int, default=256, help="batch workload: number of windows")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     return ap.parse_args()
@@ -260,8 +264,95 @@ def roofline_of(ks, ms_total, m2l_engine):
                 flops_per_s=k["flops"] / max(1, k["launches"]) / (per_launch_ms * 1e-3), **common)
 
 
+def run_workload(args):
+    """The survey's other workloads, one JSON line each (not the headline
+    line): two wires on a 0.05 um mesh, a batch of uneven windows through
+    gpx_cap_solve_batched, and the met2-bus sensitivities."""
+    import numpy as np
+    import torch
+
+    from gpurify_b200 import _lib, layouts, pex, sensitivity
+
+    torch.cuda.set_device(0)
+    ctx = _lib.Context(0)
+    base = dict(order=args.order, max_level=-1, far_quad=args.far_quad, skip_ground_rhs=1, mixed_m2l=args.mixed_m2l)
+    out = {"workload": args.workload, "data": "synthetic (seeded layouts)"}
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps, r
+
+    if args.workload == "twowires":
+        lay = layouts.two_wires()
+        p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                 mesh_max_edge_m=0.05e-6, max_panels=-1)
+        nc = len(p["nets"]) + 1
+        Cd, _ = ctx.cap_solve(p["verts"], p["cond"], nc, dense_below=2**31 - 1, skip_ground_rhs=1, tol=1e-10,
+                              precond=1)
+        out.update(panels=len(p["verts"]), rhs=nc - 1)
+        for prec, pc in (("fp64", 2), ("mixed", 1)):
+            kw = dict(base, precision=_lib.PREC_MIXED if prec == "mixed" else _lib.PREC_FP64, precond=pc)
+            kw, trep = ctx.autotune(p["verts"], p["cond"], nc, target=1e-4, **kw)
+            dt, (C, rep) = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), max(1, args.steps))
+            d = np.abs(np.diag(Cd[:2, :2]))
+            out[prec] = {"solves_per_s": 1.0 / dt, "ms": dt * 1e3, "iterations": rep["iterations"],
+                         "tuned": {k: kw[k] for k in ("order", "max_level", "far_quad", "mixed_near")},
+                         "err_vs_all_pairs": float((np.abs(C[:2, :2] - Cd[:2, :2]) / d[:, None]).max()),
+                         "cap_af": [float(C[i, i] * 3.9e18) for i in range(2)]}
+    elif args.workload == "batch":
+        ws = layouts.window_batch(args.windows, seed=7)
+        probs = []
+        for w in ws:
+            p = _lib.bridge_panelize(w.store.arrays(), w.deck.layer_table(), 1.0, w.net_of_poly,
+                                     mesh_max_edge_m=EDGE_M, max_panels=-1)
+            probs.append((p["verts"], p["cond"], len(p["nets"]) + 1))
+        N = sum(len(v) for v, _, _ in probs)
+        RR = sum(nc - 1 for _, _, nc in probs)
+        NR = sum(len(v) * (nc - 1) for v, _, nc in probs)
+        out.update(windows=len(probs), panels=N, rhs=RR, panel_rhs=NR)
+        kw = dict(base, precision=_lib.PREC_MIXED, precond=1, batch_streams=8)
+        dt, res = timed(lambda: ctx.cap_solve_batched(probs, **kw), 1)
+        out["mixed"] = {"windows_per_s": len(probs) / dt, "s": dt, "panel_rhs_per_s": NR / dt,
+                        "max_iterations": max(r["iterations"] for _, r in res),
+                        "timing": "wall clock around the synchronous batched call (8 streams)"}
+    else:  # bus
+        lay = layouts.bus_crossing()
+        z0, z1 = sensitivity.layer_span(lay.deck, "met2")
+        params = [("width", b) for b in range(8)] + [("spacing", b) for b in range(7)] + \
+                 [("thickness", z0, z1), ("height", z0, z1), ("k",)]
+        p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                 mesh_max_edge_m=0.14e-6, max_panels=-1)
+        V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params)
+        nc = len(p["nets"]) + 1
+        out.update(panels=len(p["verts"]), rhs=nc - 1, params=len(params))
+        grads = {}
+        for prec, pc in (("fp64", 2), ("mixed", 1)):
+            kw = dict(base, precision=_lib.PREC_MIXED if prec == "mixed" else _lib.PREC_FP64, precond=pc)
+            kw, trep = ctx.autotune(p["verts"], p["cond"], nc, target=1e-4, **kw)
+            dt, (C, dC, rep) = timed(lambda: ctx.cap_sensitivity(p["verts"], p["cond"], nc, V, **kw),
+                                     max(1, args.steps))
+            dt0, _ = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), max(1, args.steps))
+            grads[prec] = dC
+            out[prec] = {"ms_capacitance_plus_gradients": dt * 1e3, "ms_capacitance_only": dt0 * 1e3,
+                         "tuned": {k: kw[k] for k in ("order", "max_level", "far_quad", "mixed_near")},
+                         "iterations_forward_plus_adjoint": rep["iterations"]}
+        R = nc - 1
+        a, b = grads["mixed"][:, :R, :R], grads["fp64"][:, :R, :R]
+        out["mixed_vs_fp64_gradient"] = float(np.abs(a - b).max() / np.abs(b).max())
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.workload != "window64":
+        run_workload(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -609,7 +609,7 @@ struct Operator {
         fac64.Tm = T64.p;
         fac64.Ut = m2l->Ut64.p;
         fac64.Vt = m2l->Vt64.p;
-        if (mixed && !tc32) {
+        if (mixed) {  // also with the tensor-core M2L: the stall guard may switch to this form
             Rb32 = (R + 63) / 64 * 64;
             T32.alloc((size_t)acc * Rb32, s);
             T32.zero();
@@ -683,6 +683,23 @@ struct Operator {
             bj.apply(ctx, V, Z, pl.N, R, add);
         else
             launch_diag_scale(ctx, V, inv_diag.p, Z, pl.N, R, add);
+    }
+
+    // Switch the FP32 M2L from the tensor cores to the factored form (kept
+    // ready whenever the operators are compressed); drops captured graphs of
+    // the FP32 apply.  Returns false when no factored form exists.
+    bool drop_tc_m2l() {
+        if (!tc32 || !factored) return false;
+        tc32 = false;
+        for (auto& g : graphs)
+            if (g.kind == 1) {
+                if (g.exec) cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+                g.seen = 0;
+                g.x = nullptr;
+                g.y = nullptr;
+            }
+        return true;
     }
 
     void check_tc() {
@@ -866,12 +883,33 @@ Opts normalize(const gpx_solve_opts* o) {
     return r;
 }
 
-int choose_depth(const Opts& o, int64_t n) {
+int choose_depth(const Opts& o, int64_t n, const double* verts) {
     if (o.dense_below > 0 && n < o.dense_below) return 1;
     if (o.max_level > 0) return o.max_level;
-    // auto: about 32 panels per occupied leaf for surface meshes (~n^(1/2) leaves per level step)
+    // auto: about 32 panels per occupied leaf for surface meshes (~n^(1/2)
+    // leaves per level step), but no leaf smaller than the largest panel: the
+    // far field interpolates each panel's sources in its leaf's box, which
+    // breaks down when panels reach far outside it
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, ext = 0.0;
+    if (verts)
+        for (int64_t i = 0; i < n; ++i) {
+            const double* v = verts + 12 * i;
+            double plo[3] = {INFINITY, INFINITY, INFINITY}, phi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (int k = 0; k < 4; ++k)
+                for (int dd = 0; dd < 3; ++dd) {
+                    plo[dd] = std::min(plo[dd], v[3 * k + dd]);
+                    phi[dd] = std::max(phi[dd], v[3 * k + dd]);
+                }
+            for (int dd = 0; dd < 3; ++dd) {
+                ext = std::max(ext, phi[dd] - plo[dd]);
+                const double c = 0.5 * (plo[dd] + phi[dd]);
+                lo[dd] = std::min(lo[dd], c);
+                hi[dd] = std::max(hi[dd], c);
+            }
+        }
+    const double side = verts ? std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2])) : 0.0;
     int d = 2;
-    while (d < 10 && (double)n / std::pow(4.0, d) > 32.0) ++d;
+    while (d < 10 && (double)n / std::pow(4.0, d) > 32.0 && (!verts || side / std::pow(2.0, d + 1) >= ext)) ++d;
     return d;
 }
 
@@ -957,11 +995,13 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
     st = SolveStats();
     outer = 0;
     const ApplyFn a32 = [&](const double* x, double* y) { op.apply32(x, y); };
+    double prev_resid = INFINITY;
     for (int it = 0; it <= 12; ++it) {
         launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, rn.p);
         rn.download(hr.data(), R);
         GPX_CUDA(cudaStreamSynchronize(s));
         bool all = true;
+        prev_resid = it == 0 ? INFINITY : st.max_resid;
         st.max_resid = 0.0;
         for (int r = 0; r < R; ++r) {
             const double rel = hr[r] / hb[r];
@@ -974,6 +1014,10 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
             break;
         }
         if (it == 12) break;
+        // Stall guard: a refinement step must cut the residual tenfold; if it
+        // did not, the TF32 M2L (forced with Gauss-point sources) is too far
+        // from the FP64 operator here, so continue with the factored FP32 M2L.
+        if (st.max_resid > 0.1 * prev_resid) op.drop_tc_m2l();
         mask.upload(hm, s);
         launch_zero_cols(ctx, Res.p, mask.p, N, R);
         // Adaptive inner tolerance: ask each inner solve for no more than the
@@ -985,7 +1029,8 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         // Inner solves stop at 1e-3..1e-5: one classical Gram-Schmidt pass (FP64) keeps the
         // basis orthogonal far below that, so the re-orthogonalisation pass is skipped.
         const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
-        gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, o.max_restarts, D, in, false);
+        gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, std::min(o.max_restarts, 3), D, in,
+                    false);
         st.iterations += in.iterations;
         launch_add(ctx, X.p, D.p, NR);
         op.apply(X.p, W.p);
@@ -1062,56 +1107,61 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     const double t0 = now_s();
     const int64_t l0 = ctx.launches;
     check_problem(n, verts, cond, ncond, o);
-    const int depth = choose_depth(o, n);
+    const int depth = choose_depth(o, n, verts);
     const bool dense = depth == 1;
     const int Rn = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;  // conductors solved
-    if (Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
+    // Conductors are solved in chunks of at most kMaxChunk columns sharing one
+    // operator (its expansion and Krylov buffers are sized for one chunk).
     // Columns are padded to a multiple of 4 (16-byte rows); padding columns
     // have a zero right-hand side and converge at once.
-    const int R = (Rn + 3) & ~3;
+    constexpr int kMaxChunk = 128;
+    const int Rc = std::min(Rn, kMaxChunk);
+    const int R = (Rc + 3) & ~3;
     Prepared pr;
     prepare(ctx, n, verts, cond, ncond, o, R, depth, pr);
     Operator& op = *pr.op;
-    std::vector<int32_t> rhs_cond(R);
-    for (int r = 0; r < R; ++r) rhs_cond[r] = r < Rn ? r : -1;
-    DBuf<int32_t> d_rhs;
-    d_rhs.upload(rhs_cond, ctx.stream);
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     const double t1 = now_s();
-    DBuf<double> X;
     SolveStats st;
+    st.converged = true;
     int outer = 0;
-    // The all-pairs path stands in for the reference's dense LU (cap/solver.rs:114-117):
-    // solve it to a tighter tolerance so it matches a direct solve.
-    const double tol = dense ? std::min(o.tol, 1e-12) : o.tol;
-    if (o.precision == GPX_PREC_MIXED) {
-        Opts oi = o;
-        oi.tol = tol;
-        mixed_solve(ctx, op, pr.dp.cond.p, d_rhs.p, nullptr, R, n, oi, X, st, outer);
-    } else {
-        const ApplyFn a64 = [&](const double* x, double* y) { op.apply(x, y); };
-        const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
-        gmres_multi(ctx, a64, pc, pr.dp.cond.p, d_rhs.p, nullptr, R, n, tol, o.restart, o.max_restarts, X, st);
+    std::vector<double> hc((size_t)ncond * Rn);  // C[i][j] for the solved columns j
+    for (int c0 = 0; c0 < Rn; c0 += Rc) {
+        const int nc = std::min(Rc, Rn - c0);
+        std::vector<int32_t> rhs_cond(R);
+        for (int r = 0; r < R; ++r) rhs_cond[r] = r < nc ? c0 + r : -1;
+        DBuf<int32_t> d_rhs;
+        d_rhs.upload(rhs_cond, ctx.stream);
+        DBuf<double> X;
+        SolveStats sc;
+        int oc = 0;
+        solve_columns(ctx, op, o, dense, pr.dp.cond.p, d_rhs.p, nullptr, R, n, X, sc, oc);
+        st.iterations = std::max(st.iterations, sc.iterations);
+        st.max_resid = std::max(st.max_resid, sc.max_resid);
+        st.converged = st.converged && sc.converged;
+        outer = std::max(outer, oc);
+        DBuf<double> dC;
+        dC.alloc((size_t)ncond * R, ctx.stream);
+        {
+            KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
+            k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, pr.dp.area.p, X.p, n, R, dC.p);
+            GPX_LAUNCH_CHECK();
+            ctx.launches += 1;
+        }
+        std::vector<double> part((size_t)ncond * R);
+        dC.download(part.data(), part.size());
+        GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+        for (int i = 0; i < ncond; ++i)
+            for (int r = 0; r < nc; ++r) hc[(size_t)i * Rn + c0 + r] = part[(size_t)i * R + r];
     }
-    DBuf<double> dC;
-    dC.alloc((size_t)ncond * R, ctx.stream);
-    {
-        KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
-        k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, pr.dp.area.p, X.p, n, R, dC.p);
-        GPX_LAUNCH_CHECK();
-        ctx.launches += 1;
-    }
-    std::vector<double> hc((size_t)ncond * R);
-    dC.download(hc.data(), hc.size());
-    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     const double t2 = now_s();
     for (int i = 0; i < ncond; ++i)
         for (int j = 0; j < ncond; ++j) {
             double v;
             if (j < Rn)
-                v = hc[(size_t)i * R + j];
+                v = hc[(size_t)i * Rn + j];
             else if (i < Rn)
-                v = hc[(size_t)j * R + i];  // substrate column by symmetry
+                v = hc[(size_t)j * Rn + i];  // substrate column by symmetry
             else
                 v = std::nan("");
             C[(size_t)i * ncond + j] = v;
@@ -1150,7 +1200,7 @@ void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int
     check_problem(n, verts, nullptr, 1, o);
     if (Rn <= 0 || Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "nrhs must be in [1, 256]");
     const int R = (Rn + 3) & ~3;
-    const int depth = choose_depth(o, n);
+    const int depth = choose_depth(o, n, verts);
     Prepared pr;
     prepare(ctx, n, verts, nullptr, 1, o, R, depth, pr);
     const Plan& plan = pr.plan;
@@ -1203,7 +1253,7 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
     if (np < 0 || np > 4096 || (np > 0 && !V)) throw Error(GPX_ERR_INVALID_ARG, "n_params must be in [0, 4096]");
     for (int64_t i = 0; i < (int64_t)np * n * 12; ++i)
         if (!std::isfinite(V[i])) throw Error(GPX_ERR_INVALID_ARG, "non-finite vertex velocity");
-    const int depth = choose_depth(o, n);
+    const int depth = choose_depth(o, n, verts);
     const bool dense = depth == 1;
     const int Rn = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;
     if (Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
@@ -1432,7 +1482,7 @@ void autotune(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int
     Opts autodepth = base;
     autodepth.max_level = -1;
     autodepth.dense_below = -1;
-    const int d0 = std::max(2, choose_depth(autodepth, n));
+    const int d0 = std::max(2, choose_depth(autodepth, n, verts));
     struct Cand {
         int order, depth, fq, mn;
     };

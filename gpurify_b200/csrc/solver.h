@@ -25,8 +25,10 @@ struct Opts {
 };
 Opts normalize(const gpx_solve_opts* o);
 
-// Depth the solver uses for n panels under the options (1 = all pairs).
-int choose_depth(const Opts& o, int64_t n);
+// Depth the solver uses for n panels under the options (1 = all pairs);
+// the automatic rule looks at the panels (may be null) to keep every leaf at
+// least as large as the largest panel.
+int choose_depth(const Opts& o, int64_t n, const double* verts);
 
 // Solve the Maxwell matrix of a panel problem (farads, not k-scaled) into C
 // (ncond x ncond row-major).  Columns not solved are filled by symmetry.

@@ -90,3 +90,30 @@ def test_mixed_two_wire_small_rhs(ctx):
     C32, rep = ctx.cap_solve(p["verts"], p["cond"], 3, order=4, max_level=4, precision=1)
     assert rep["converged"] == 1
     assert rel_max(C32, C64) < 1e-6
+
+
+def test_refinement_stall_guard_recovers(ctx):
+    """A small window whose substrate-plate panels are twice its depth-5 leaf
+    size: the TF32 M2L forced with Gauss-point sources is far from the FP64
+    operator there, the refinement stalls, and the stall guard continues with
+    the factored FP32 M2L; the result matches the FP64 solve."""
+    w = layouts.window_batch(93, seed=7)[92]
+    p = _lib.bridge_panelize(w.store.arrays(), w.deck.layer_table(), 1.0, w.net_of_poly, mesh_max_edge_m=0.25e-6,
+                             max_panels=-1)
+    nc = len(p["nets"]) + 1
+    kw = dict(order=5, max_level=5, dense_below=-1, far_quad=1, skip_ground_rhs=1, precond=1)
+    C64, _ = ctx.cap_solve(p["verts"], p["cond"], nc, precision=0, **kw)
+    C32, rep = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, mixed_m2l=2, **kw)
+    assert rep["converged"] == 1
+    R = nc - 1
+    d = np.abs(np.diag(C64[:R, :R]))
+    assert (np.abs(C32[:R, :R] - C64[:R, :R]) / d[:, None]).max() < 1e-6
+
+
+def test_auto_depth_keeps_leaves_larger_than_panels(ctx):
+    w = layouts.window_batch(93, seed=7)[92]
+    p = _lib.bridge_panelize(w.store.arrays(), w.deck.layer_table(), 1.0, w.net_of_poly, mesh_max_edge_m=0.25e-6,
+                             max_panels=-1)
+    _, rep = ctx.cap_solve(p["verts"], p["cond"], len(p["nets"]) + 1, order=5, max_level=-1, dense_below=-1,
+                           skip_ground_rhs=1, precision=1, mixed_m2l=2)
+    assert rep["converged"] == 1 and rep["max_level"] <= 4

@@ -199,3 +199,22 @@ def test_block_jacobi_matches_diagonal(ctx, orc, precision, block):
     assert r1["iterations"] < r0["iterations"]
     d = np.abs(np.diag(C0))
     assert (np.abs(C1 - C0) / d[:, None]).max() < 1e-6
+
+
+def test_many_conductors_in_column_chunks(ctx, orc):
+    """More conductors than one column chunk (128): the columns are solved in
+    chunks sharing one operator; the Maxwell matrix equals the oracle's dense
+    LU solve."""
+    verts, cond = [], []
+    k = 0
+    for i in range(12):
+        for j in range(12):
+            v, c = orc.plate(i * 0.3, j * 0.3, 0.05 * ((i + j) % 3), 0.2, 0.2, 2, 2, k)
+            verts.append(v)
+            cond.append(c)
+            k += 1
+    verts, cond = np.vstack(verts), np.concatenate(cond)
+    C, rep = ctx.cap_solve(verts, cond, k, dense_below=2**31 - 1)
+    assert rep["n_rhs"] == k == 144 and rep["converged"] == 1
+    ref = orc.cap_dense(verts, cond, k)
+    assert rel_max(C, ref) < 1e-9
