@@ -754,6 +754,9 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
                  DBuf<double>& X, SolveStats& st, bool reorth = true) {
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
+    // Krylov basis within a memory budget (16 GB per solve), restart >= 20
+    constexpr double kBasisBudget = 16.0 * (1ull << 30);
+    m = (int)std::max<int64_t>(std::min<int64_t>(20, m), std::min<int64_t>(m, (int64_t)(kBasisBudget / (8.0 * NR)) - 1));
     DBuf<double> V, W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
     DBuf<int32_t> act, done, kused, cnt;
     V.alloc((size_t)(m + 1) * NR, s);
