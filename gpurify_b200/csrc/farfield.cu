@@ -28,27 +28,39 @@ __device__ __forceinline__ void cp16(void* dst, const void* src, bool valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
 
+// Panels per near-field work item (the plan's kRowsPerItem).
+constexpr int kItemPanels = 64;
+
 template <int N>
 struct Ord {
     static constexpr int n3 = N * N * N;
     static constexpr int ns = (n3 + 31) & ~31;
 };
 
-// P2M as a GEMM per (leaf, 64-wide chunk of rows r):
-//   E[leaf][r][m] = sum_j W[j][m] * (a_j X[j][r])
-// 256 threads; thread (tm, tr) holds nodes tm + 32 i and rows tr + 8 j.
-// Panels are staged 32 (FP32) or 16 (FP64) at a time.  Every row r < Rb and node m < ns of the
-// chunk is written (zeros outside r < R, m < n3).
+// P2M as a GEMM per (work item = leaf and <= 64 of its panels, 64-wide chunk
+// of rows r):  E[leaf][r][m] = sum_j W[j][m] * (a_j X[j][r]).
+// The work items are the near-field items (64 panels each), so a leaf of a few
+// hundred panels spreads over several CTAs instead of serialising one: the
+// first item of a leaf writes E[leaf], each further item writes a partial
+// expansion at box index nbox + slot, and k_p2m_fix adds the partials in item
+// order (deterministic).
+// 256 threads; thread (tm, tr) holds nodes MI tm .. MI tm + MI - 1 and rows
+// 8 tr .. 8 tr + 7.  Panels are staged KP at a time.  Every row r < Rb and node
+// m < ns of the chunk is written (zeros outside r < R, m < n3).
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X, const T* __restrict__ W,
-                                             bool mul_area, T* __restrict__ E, int R, int Rb) {
+__global__ void __launch_bounds__(256) k_p2m(DevPlan p, const int32_t* __restrict__ slot, const T* __restrict__ X,
+                                             const T* __restrict__ W, bool mul_area, T* __restrict__ E, int R,
+                                             int Rb) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, MI = NS / 32;
     constexpr int KP = sizeof(T) == 8 ? 16 : 32;  // panels per staged chunk (static shared memory <= 48 KB)
-    const int t = blockIdx.x;
+    constexpr int QW = 64 + 16 / (int)sizeof(T);  // Qs row stride: 16-byte aligned rows
+    const int it = blockIdx.x;
+    const int t = p.item_leaf[it], r0 = p.item_row0[it];
     const int rc = blockIdx.y * 64;
-    const int64_t j0 = p.leaf_begin[t], j1 = p.leaf_begin[t + 1];
+    const int64_t lb = p.leaf_begin[t];
+    const int64_t j0 = lb + r0, j1 = min(lb + r0 + kItemPanels, p.leaf_begin[t + 1]);
     __shared__ T Ws[KP][NS + 1];
-    __shared__ T Qs[KP][65];
+    __shared__ __align__(16) T Qs[KP][QW];
     const int tid = threadIdx.x, tm = tid >> 3, tr = tid & 7;
     T acc[MI][8];
 #pragma unroll
@@ -71,98 +83,143 @@ __global__ void __launch_bounds__(256) k_p2m(DevPlan p, const T* __restrict__ X,
         for (int k = 0; k < cnt; ++k) {
             T a[MI], b[8];
 #pragma unroll
-            for (int i = 0; i < MI; ++i) a[i] = Ws[k][tm + 32 * i];
+            for (int i = 0; i < MI; ++i) a[i] = Ws[k][MI * tm + i];
+            if constexpr (sizeof(T) == 4) {
+                const float4 b0 = *reinterpret_cast<const float4*>(&Qs[k][8 * tr]);
+                const float4 b1 = *reinterpret_cast<const float4*>(&Qs[k][8 * tr + 4]);
+                b[0] = b0.x, b[1] = b0.y, b[2] = b0.z, b[3] = b0.w, b[4] = b1.x, b[5] = b1.y, b[6] = b1.z, b[7] = b1.w;
+            } else {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) b[j] = Qs[k][tr + 8 * j];
+                for (int q = 0; q < 4; ++q) {
+                    const double2 v = *reinterpret_cast<const double2*>(&Qs[k][8 * tr + 2 * q]);
+                    b[2 * q] = v.x, b[2 * q + 1] = v.y;
+                }
+            }
 #pragma unroll
             for (int i = 0; i < MI; ++i)
 #pragma unroll
                 for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
         }
     }
-    T* out = E + ((int64_t)(p.leaf_box0 + t) * Rb + rc) * NS;
+    const int64_t box = slot[it] < 0 ? (int64_t)p.leaf_box0 + t : (int64_t)p.nbox + slot[it];
+    T* out = E + (box * Rb + rc) * NS;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        const int r = tr + 8 * j;
+        const int r = 8 * tr + j;
         if (rc + r >= Rb) continue;
 #pragma unroll
         for (int i = 0; i < MI; ++i) {
-            const int m = tm + 32 * i;
+            const int m = MI * tm + i;
             out[(int64_t)r * NS + m] = (m < N3 && rc + r < R) ? acc[i][j] : (T)0;
         }
     }
 }
 
-// L2P as a GEMM per (leaf, 64-wide chunk of r):
-//   Y[j][r] += coef * sum_m S_j[m] L[leaf][r][m],  S_j[m] = wx[a] wy[b] wz[c]
-// (the centroid's separable weights), or S_j = Wt[j] (times a_j if mul_area)
-// when explicit weights are given.
-// 256 threads, 32 panels per chunk; thread (tj, tr) holds panels tj + 16 i
-// (i < 2) and rows tr + 16 q (q < 4).
+// E[leaf] += the partial expansions of its further work items, in item order.
+// One CTA per (leaf with several items, 1024-value chunk of its Rb x ns block).
+template <class T>
+__global__ void __launch_bounds__(256) k_p2m_fix(int nbox, int leaf_box0, const int32_t* __restrict__ fix_leaf,
+                                                 const int32_t* __restrict__ fix_first,
+                                                 const int32_t* __restrict__ fix_cnt, T* __restrict__ E,
+                                                 int64_t block) {
+    const int f = blockIdx.x;
+    const int64_t e = ((int64_t)blockIdx.y * 256 + threadIdx.x) * 4;
+    if (e >= block) return;
+    T* dst = E + ((int64_t)leaf_box0 + fix_leaf[f]) * block + e;
+    T v0 = dst[0], v1 = dst[1], v2 = dst[2], v3 = dst[3];
+    const int s0 = fix_first[f], cnt = fix_cnt[f];
+    for (int q = 0; q < cnt; ++q) {
+        const T* src = E + ((int64_t)nbox + s0 + q) * block + e;
+        v0 += src[0], v1 += src[1], v2 += src[2], v3 += src[3];
+    }
+    dst[0] = v0, dst[1] = v1, dst[2] = v2, dst[3] = v3;
+}
+
+// L2P as a GEMM per (work item = leaf and <= 64 of its panels, 64-wide chunk
+// of r):  Y[j][r] += coef * sum_m S_j[m] L[leaf][r][m],  S_j[m] = wx[a] wy[b]
+// wz[c] (the centroid's separable weights), or S_j = Wt[j] (times a_j if
+// mul_area) when explicit weights are given.
+// 256 threads; thread (tj, tr) holds panels 4 tj .. 4 tj + 3 and rows
+// 4 tr .. 4 tr + 3; nodes are staged 32 at a time.
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L, const T* __restrict__ Wt,
                                              bool mul_area, double* __restrict__ Y, int R, int Rb, double coef) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns;
-    const int t = blockIdx.x;
+    constexpr int JP = kItemPanels, MK = 32, SW = 64 + 16 / (int)sizeof(T);
+    const int it = blockIdx.x;
+    const int t = p.item_leaf[it], r0 = p.item_row0[it];
     const int rc = blockIdx.y * 64;
-    const int64_t j0 = p.leaf_begin[t], j1 = p.leaf_begin[t + 1];
+    const int64_t lb = p.leaf_begin[t];
+    const int64_t jb = lb + r0;
+    const int cnt = (int)min((int64_t)JP, p.leaf_begin[t + 1] - jb);
     const T* src = L + ((int64_t)(p.leaf_box0 + t) * Rb + rc) * NS;
-    constexpr int JP = 32;  // panels per chunk (leaves hold a few tens of panels)
     __shared__ T wv[JP][3 * N];
-    __shared__ T Ss[JP][33];
-    __shared__ T Ls[32][65];
+    __shared__ __align__(16) T Ss[MK][SW];  // [node][panel]
+    __shared__ __align__(16) T Ls[MK][SW];  // [node][row]
     const int tid = threadIdx.x, tj = tid >> 4, tr = tid & 15;
-    for (int64_t jb = j0; jb < j1; jb += JP) {
-        const int cnt = (int)min((int64_t)JP, j1 - jb);
-        __syncthreads();
+    if (!Wt)
         for (int e = tid; e < JP * 3 * N; e += 256) {
             const int jj = e / (3 * N);
             wv[jj][e % (3 * N)] = jj < cnt ? (T)p.w1d[jb * 3 * N + e] : (T)0;
         }
-        T acc[2][4];
+    T acc[4][4];
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][q] = (T)0;
-        for (int m0 = 0; m0 < N3; m0 += 32) {
-            __syncthreads();
-            for (int e = tid; e < JP * 32; e += 256) {
-                const int jj = e >> 5, mm = e & 31, m = m0 + mm;
-                T v = (T)0;
-                if (m < N3 && jj < cnt) {
-                    v = Wt ? Wt[(jb + jj) * N3 + m]
-                           : wv[jj][m / (N * N)] * wv[jj][N + (m / N) % N] * wv[jj][2 * N + m % N];
-                    if (mul_area) v *= (T)p.area[jb + jj];
-                }
-                Ss[jj][mm] = v;
+        for (int q = 0; q < 4; ++q) acc[i][q] = (T)0;
+    for (int m0 = 0; m0 < N3; m0 += MK) {
+        __syncthreads();
+        for (int e = tid; e < JP * MK; e += 256) {
+            const int jj = e / MK, mm = e % MK, m = m0 + mm;
+            T v = (T)0;
+            if (m < N3 && jj < cnt) {
+                v = Wt ? Wt[(jb + jj) * N3 + m] : wv[jj][m / (N * N)] * wv[jj][N + (m / N) % N] * wv[jj][2 * N + m % N];
+                if (mul_area) v *= (T)p.area[jb + jj];
             }
-            for (int e = tid; e < 32 * 64; e += 256) {
-                const int mm = e & 31, r = e >> 5;
-                Ls[mm][r] = (m0 + mm < N3 && rc + r < R) ? src[(int64_t)r * NS + m0 + mm] : (T)0;
-            }
-            __syncthreads();
-#pragma unroll 8
-            for (int k = 0; k < 32; ++k) {
-                T a[2], b[4];
-#pragma unroll
-                for (int i = 0; i < 2; ++i) a[i] = Ss[tj + 16 * i][k];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) b[q] = Ls[k][tr + 16 * q];
-#pragma unroll
-                for (int i = 0; i < 2; ++i)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[i][q] += a[i] * b[q];
-            }
+            Ss[mm][jj] = v;
         }
+        for (int e = tid; e < 64 * MK; e += 256) {
+            const int mm = e % MK, r = e / MK;
+            Ls[mm][r] = (m0 + mm < N3 && rc + r < R) ? src[(int64_t)r * NS + m0 + mm] : (T)0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < MK; ++k) {
+            T a[4], b[4];
+            if constexpr (sizeof(T) == 4) {
+                const float4 av = *reinterpret_cast<const float4*>(&Ss[k][4 * tj]);
+                const float4 bv = *reinterpret_cast<const float4*>(&Ls[k][4 * tr]);
+                a[0] = av.x, a[1] = av.y, a[2] = av.z, a[3] = av.w;
+                b[0] = bv.x, b[1] = bv.y, b[2] = bv.z, b[3] = bv.w;
+            } else {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int jj = tj + 16 * i;
-            if (jj >= cnt) continue;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = rc + tr + 16 * q;
-                if (r < R) Y[(jb + jj) * R + r] += coef * (double)acc[i][q];
+                for (int h = 0; h < 2; ++h) {
+                    const double2 av = *reinterpret_cast<const double2*>(&Ss[k][4 * tj + 2 * h]);
+                    const double2 bv = *reinterpret_cast<const double2*>(&Ls[k][4 * tr + 2 * h]);
+                    a[2 * h] = av.x, a[2 * h + 1] = av.y, b[2 * h] = bv.x, b[2 * h + 1] = bv.y;
+                }
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[i][q] += a[i] * b[q];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int jj = 4 * tj + i;
+        if (jj >= cnt) continue;
+        double* y = Y + (jb + jj) * R + rc + 4 * tr;
+        if ((R & 1) == 0 && rc + 4 * tr + 3 < R) {  // 16-byte aligned pairs
+            double2 y0 = *reinterpret_cast<double2*>(y), y1 = *reinterpret_cast<double2*>(y + 2);
+            y0.x += coef * (double)acc[i][0], y0.y += coef * (double)acc[i][1];
+            y1.x += coef * (double)acc[i][2], y1.y += coef * (double)acc[i][3];
+            *reinterpret_cast<double2*>(y) = y0;
+            *reinterpret_cast<double2*>(y + 2) = y1;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (rc + 4 * tr + q < R) y[q] += coef * (double)acc[i][q];
         }
     }
 }
@@ -631,10 +688,18 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     const unsigned rchunks64 = cdiv(Rb, 64), rchunks_tree = cdiv(Rb, RC);
     GPX_CUDA(cudaMemsetAsync(L, 0, (size_t)p.nbox * NS * Rb * sizeof(T), s));
     {
-        KTimer t(c, K_P2M, (double)p.N * (wb * R + wb * N3 + 8.0) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
-        k_p2m<T, N><<<dim3(p.nleaf, rchunks64), 256, 0, s>>>(p, X, w.src, w.src_area, E, R, Rb);
+        KTimer t(c, K_P2M, (double)p.N * (wb * R + wb * N3 + 8.0) + (p.nleaf + 2.0 * f.npart) * box_bytes,
+                 2.0 * (double)p.N * N3 * R);
+        k_p2m<T, N><<<dim3(p.nitems, rchunks64), 256, 0, s>>>(p, f.p2m_slot, X, w.src, w.src_area, E, R, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
+        if (f.nfix > 0) {
+            const int64_t block = (int64_t)Rb * NS;
+            k_p2m_fix<T><<<dim3(f.nfix, cdiv(block, 1024)), 256, 0, s>>>(p.nbox, p.leaf_box0, f.fix_leaf, f.fix_first,
+                                                                         f.fix_cnt, E, block);
+            GPX_LAUNCH_CHECK();
+            c.launches += 1;
+        }
     }
     if (smem > 48 * 1024) {
         set_smem_once(k_m2m_tree<T, N>, (int)smem);
@@ -677,7 +742,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     }
     {
         KTimer t(c, K_L2P, (double)p.N * (16.0 * R + 24.0 * N) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
-        k_l2p<T, N><<<dim3(p.nleaf, cdiv(R, 64)), 256, 0, s>>>(p, L, w.tgt, w.tgt_area, Y, R, Rb, coef);
+        k_l2p<T, N><<<dim3(p.nitems, cdiv(R, 64)), 256, 0, s>>>(p, L, w.tgt, w.tgt_area, Y, R, Rb, coef);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }

@@ -85,6 +85,14 @@ struct FarLaunch {
     const int32_t* child_count;  // device, per box
     const int32_t* leaf_of;      // device, per sorted panel
     const int64_t* m2l_off;      // host, per box (pair counts per level)
+    // P2M over the near-field work items: each item's expansion slot (-1:
+    // the item writes its leaf's expansion; k >= 0: partial at box nbox + k),
+    // and per leaf with several items the partials k_p2m_fix adds to it.
+    const int32_t* p2m_slot;     // device, per near item
+    const int32_t* fix_leaf;     // device, per leaf with several items
+    const int32_t* fix_first;    // device: its first partial slot
+    const int32_t* fix_cnt;      // device: its number of partials
+    int nfix = 0, npart = 0;
 };
 // Y = P_near X with an FP32 copy of P, FP32 input and arithmetic (Y is FP64).
 // R must be a multiple of 4 (16-byte aligned rows).

@@ -121,7 +121,8 @@ std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
 struct DevPlanBufs {
     DBuf<double> verts, cent, area, w1d, m2m1d;
     DBuf<int32_t> cond, near_off, near_src, near_S, box_parent, box_octant, m2l_src, m2l_slot, child_first,
-        child_count, leaf_of, item_leaf, item_row0, item128_leaf, item128_row0, near_rev, near_pre;
+        child_count, leaf_of, item_leaf, item_row0, item128_leaf, item128_row0, near_rev, near_pre, p2m_slot,
+        fix_leaf, fix_first, fix_cnt;
     DBuf<int64_t> leaf_begin, nval_off, m2l_off;
     DBuf<double> leaf_ctr, wsrc;
     int nitems128 = 0;
@@ -161,6 +162,34 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
     }
     d.item_leaf.upload(p.item_leaf, s);
     d.item_row0.upload(p.item_row0, s);
+    {
+        // P2M runs over the near items: the first item of a leaf writes the
+        // leaf's expansion, further items write partials that k_p2m_fix adds
+        static_assert(Plan::kRowsPerItem == 64, "far-field kernels take 64-panel items");
+        std::vector<int32_t> slot(p.item_leaf.size(), -1), fl, ff, fc;
+        int32_t np = 0;
+        for (size_t i = 0; i < p.item_leaf.size(); ++i) {
+            if (p.item_row0[i] == 0) continue;
+            const int32_t k = p.item_leaf[i];
+            if (fl.empty() || fl.back() != k) {
+                fl.push_back(k);
+                ff.push_back(np);
+                fc.push_back(0);
+            }
+            slot[i] = np++;
+            fc.back() += 1;
+        }
+        d.p2m_slot.upload(slot, s);
+        d.fix_leaf.upload(fl, s);
+        d.fix_first.upload(ff, s);
+        d.fix_cnt.upload(fc, s);
+        d.far.p2m_slot = d.p2m_slot.p;
+        d.far.fix_leaf = d.fix_leaf.p;
+        d.far.fix_first = d.fix_first.p;
+        d.far.fix_cnt = d.fix_cnt.p;
+        d.far.nfix = (int)fl.size();
+        d.far.npart = np;
+    }
     {
         // per near entry (t, e): its column offset in t's concatenated source
         // list, and the index of t in the near list of leaf near_src[e]
@@ -466,7 +495,7 @@ struct Operator {
                 launch_centroid_weights(ctx, d.v, nullptr, Sc.p);
                 w64 = FarWeights<double>{Sc.p, false, d.wsrc.p, true};
             }
-            E64.alloc((size_t)pl.nbox() * ns * R, s);
+            E64.alloc((size_t)(pl.nbox() + d.far.npart) * ns * R, s);  // + P2M partials
             L64.alloc((size_t)pl.nbox() * ns * R, s);
             {
                 // M2L scale 1/half of each box's level, for launches covering all levels
@@ -489,7 +518,7 @@ struct Operator {
             if (has_far()) {
                 const int ns = node_stride(pl.n);
                 Rb32 = (R + 63) / 64 * 64;
-                E32.alloc((size_t)pl.nbox() * ns * Rb32, s);
+                E32.alloc((size_t)(pl.nbox() + d.far.npart) * ns * Rb32, s);
                 L32.alloc((size_t)pl.nbox() * ns * Rb32, s);
                 W32.alloc((size_t)pl.N * pl.n3, s);
                 launch_to_f32(ctx, d.wsrc.p, W32.p, pl.N * pl.n3);
