@@ -14,38 +14,64 @@ namespace {
 constexpr int kRedThreads = 256;
 
 // partial[b][i][r] = sum over rows of block b of A_i[n][r] * B[n][r].
+// Four vectors A_i per pass over the block's rows: B is read once per four,
+// and each thread keeps four independent loads in flight per row.  Each
+// partial sums the same rows in the same order as a one-vector pass.
 __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restrict__ A, int64_t strideA, int ni,
                                                           const double* __restrict__ B, int64_t N, int R,
                                                           double* __restrict__ partial) {
+    constexpr int kV = 4;
     const int nsub = kRedThreads / R;
     const int r = threadIdx.x % R, sub = threadIdx.x / R;
     const int64_t per = (N + gridDim.x - 1) / gridDim.x;
     const int64_t n0 = (int64_t)blockIdx.x * per, n1 = min(N, n0 + per);
-    __shared__ double red[kRedThreads];
-    for (int i = 0; i < ni; ++i) {
-        const double* Ai = A + i * strideA;
-        double acc = 0.0;
-        if (sub < nsub)
-            for (int64_t n = n0 + sub; n < n1; n += nsub) acc += Ai[n * R + r] * B[n * R + r];
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        if (sub == 0) {
-            double s = red[r];
-            for (int k = 1; k < nsub; ++k) s += red[k * R + r];
-            partial[((int64_t)blockIdx.x * ni + i) * R + r] = s;
+    __shared__ double red[kV][kRedThreads];
+    for (int i0 = 0; i0 < ni; i0 += kV) {
+        const int nv = min(kV, ni - i0);
+        const double* A0 = A + i0 * strideA;
+        double acc[kV] = {0.0, 0.0, 0.0, 0.0};
+        if (sub < nsub) {
+            if (nv == kV) {
+#pragma unroll 2
+                for (int64_t n = n0 + sub; n < n1; n += nsub) {
+                    const int64_t o = n * R + r;
+                    const double b = B[o];
+#pragma unroll
+                    for (int q = 0; q < kV; ++q) acc[q] += A0[q * strideA + o] * b;
+                }
+            } else {
+                for (int64_t n = n0 + sub; n < n1; n += nsub) {
+                    const int64_t o = n * R + r;
+                    const double b = B[o];
+                    for (int q = 0; q < nv; ++q) acc[q] += A0[q * strideA + o] * b;
+                }
+            }
         }
+#pragma unroll
+        for (int q = 0; q < kV; ++q) red[q][threadIdx.x] = acc[q];
+        __syncthreads();
+        if (sub == 0)
+            for (int q = 0; q < nv; ++q) {
+                double s = red[q][r];
+                for (int k = 1; k < nsub; ++k) s += red[q][k * R + r];
+                partial[((int64_t)blockIdx.x * ni + i0 + q) * R + r] = s;
+            }
         __syncthreads();
     }
 }
 
-// out[i][r] (+)= sum_b partial[b][i][r]; one thread per (i, r).
+// out[i][r] (+)= sum_b partial[b][i][r]; one warp per (i, r): lane l sums
+// blocks l, l + 32, ... and the lanes combine in a fixed shuffle tree.
 __global__ void k_reduce_blocks(const double* __restrict__ partial, int nblk, int ni, int R, double* __restrict__ out,
                                 int accumulate) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (o >= ni * R) return;
+    const int64_t stride = (int64_t)ni * R;
     double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += partial[(int64_t)b * ni * R + o];
-    out[o] = accumulate ? out[o] + s : s;
+    for (int b = lane; b < nblk; b += 32) s += partial[b * stride + o];
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+    if (lane == 0) out[o] = accumulate ? out[o] + s : s;
 }
 
 // W[n][r] -= sum_{i<ni} h[i][r] * V_i[n][r]
@@ -244,7 +270,7 @@ void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const dou
     }
     {
         KTimer t(c, K_SMALL);
-        k_reduce_blocks<<<blocks_for((int64_t)ni * R, 128), 128, 0, c.stream>>>(partial, nblk, ni, R, out, accumulate);
+        k_reduce_blocks<<<blocks_for((int64_t)ni * R, 8), 256, 0, c.stream>>>(partial, nblk, ni, R, out, accumulate);
         GPX_LAUNCH_CHECK();
     }
     c.launches += 2;
