@@ -339,10 +339,11 @@ __global__ void __launch_bounds__(256) k_m2m_tree(DevPlan p, int pb0, const int3
             dst[(int64_t)r * NS + ap * NN + bc] = s;
         }
     }
-    for (int e = threadIdx.x; e < rc * (NS - N3); e += blockDim.x) {
-        const int r = e / (NS - N3), m = N3 + e % (NS - N3);
-        dst[(int64_t)r * NS + m] = (T)0;
-    }
+    if constexpr (NS > N3)
+        for (int e = threadIdx.x; e < rc * (NS - N3); e += blockDim.x) {
+            const int r = e / (NS - N3), m = N3 + e % (NS - N3);
+            dst[(int64_t)r * NS + m] = (T)0;
+        }
 }
 
 // L2L, one CTA per (parent box, chunk of RC rows r): the transposed tree.
@@ -597,7 +598,6 @@ template <class T, int MW>
 __global__ void __launch_bounds__(MW) k_m2l_fac_u(FacM2L<T> f, int b0, T* __restrict__ L, int R, double scale) {
     constexpr int V = 16 / sizeof(T);
     constexpr int KC = 128 / sizeof(T);
-    constexpr int PP = KC + V;
     constexpr int XP = MW + V;
     constexpr int AP = 64 + V;
     constexpr int TXN = MW / 8;
