@@ -11,8 +11,9 @@
 //  L2L  L[child][r][.] += (Mx (x) My (x) Mz)^T L[par][r][.]
 //  L2P  Y[j][r]       += coef sum_m S(c_j)[m] L[leaf][r][m]  (collocation point)
 //
-// P2M and L2P are register-tiled GEMMs per leaf.  M2M and L2L run one CTA per
-// parent box over all eight octants at once: the 1-D operator of an axis
+// P2M and L2P are register-tiled GEMMs per work item of at most 64 panels of
+// one leaf (so large leaves spread over several CTAs).  M2M and L2L run one
+// CTA per parent box over all eight octants at once: the 1-D operator of an axis
 // depends only on the child's bit along that axis, so the eight children's
 // contractions share partial sums along a binary tree (z, then y, then x for
 // M2M; the reverse for L2L): 14 n^4 multiply-adds per parent and right-hand
