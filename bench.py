@@ -265,8 +265,8 @@ def roofline_of(ks, ms_total, m2l_engine):
 
 
 def run_workload(args):
-    """The survey's other workloads, one JSON line each (not the headline
-    line): two wires on a 0.05 um mesh, a batch of uneven windows through
+    """The other workloads, one JSON line each (not the headline line): two
+    wires on a 0.05 um mesh, a batch of uneven windows through
     gpx_cap_solve_batched, and the met2-bus sensitivities."""
     import numpy as np
     import torch
