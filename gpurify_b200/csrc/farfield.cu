@@ -38,6 +38,14 @@ struct Ord {
     static constexpr int ns = (n3 + 31) & ~31;
 };
 
+// CTAs per SM the FP32 P2M and L2P are compiled for at orders <= 5: four
+// (64 registers, no spills) instead of the two that 90 registers allowed, so
+// more warps hide the latency of each staged slice's global loads.
+template <class T, int N>
+constexpr int kMinCtas() {
+    return sizeof(T) == 4 && N <= 5 ? 4 : 1;
+}
+
 // P2M as a GEMM per (work item = leaf and <= 64 of its panels, 64-wide chunk
 // of rows r):  E[leaf][r][m] = sum_j W[j][m] * (a_j X[j][r]).
 // The work items are the near-field items (64 panels each), so a leaf of a few
@@ -49,9 +57,9 @@ struct Ord {
 // 8 tr .. 8 tr + 7.  Panels are staged KP at a time.  Every row r < Rb and node
 // m < ns of the chunk is written (zeros outside r < R, m < n3).
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_p2m(DevPlan p, const int32_t* __restrict__ slot, const T* __restrict__ X,
-                                             const T* __restrict__ W, bool mul_area, T* __restrict__ E, int R,
-                                             int Rb) {
+__global__ void __launch_bounds__(256, kMinCtas<T, N>())
+    k_p2m(DevPlan p, const int32_t* __restrict__ slot, const T* __restrict__ X, const T* __restrict__ W,
+          bool mul_area, T* __restrict__ E, int R, int Rb) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, MI = NS / 32;
     constexpr int KP = sizeof(T) == 8 ? 16 : 32;  // panels per staged chunk (static shared memory <= 48 KB)
     constexpr int QW = 64 + 16 / (int)sizeof(T);  // Qs row stride: 16-byte aligned rows
@@ -143,8 +151,9 @@ __global__ void __launch_bounds__(256) k_p2m_fix(int nbox, int leaf_box0, const 
 // 256 threads; thread (tj, tr) holds panels 4 tj .. 4 tj + 3 and rows
 // 4 tr .. 4 tr + 3; nodes are staged 32 at a time.
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_l2p(DevPlan p, const T* __restrict__ L, const T* __restrict__ Wt,
-                                             bool mul_area, double* __restrict__ Y, int R, int Rb, double coef) {
+__global__ void __launch_bounds__(256, kMinCtas<T, N>())
+    k_l2p(DevPlan p, const T* __restrict__ L, const T* __restrict__ Wt, bool mul_area, double* __restrict__ Y, int R,
+          int Rb, double coef) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns;
     constexpr int JP = kItemPanels, MK = 32, SW = 64 + 16 / (int)sizeof(T);
     const int it = blockIdx.x;
