@@ -67,9 +67,10 @@ def parse():
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 QR-compressed M2L operators (reference), 1 exact")
     ap.add_argument("--mixed-m2l", type=int, default=2,
                     help="mixed M2L: 0 auto, 1 factored on CUDA cores, 2 tensor cores also with Gauss sources")
-    ap.add_argument("--workload", default="window64", choices=["window64", "twowires", "batch", "bus"],
+    ap.add_argument("--workload", default="window64", choices=["window64", "twowires", "batch", "bus", "block"],
                     help="window64: the headline 64-net window; twowires: two met1 wires on a 0.05 um mesh; "
-                         "batch: many uneven windows in one batched call; bus: met2 bus sensitivities")
+                         "batch: many uneven windows in one batched call; bus: met2 bus sensitivities; "
+                         "block: 200 um, 6-layer, 512-net block with layer-parameter gradients (mixed)")
     ap.add_argument("--windows", type=int, default=256, help="batch workload: number of windows")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
@@ -268,7 +269,9 @@ def roofline_of(ks, ms_total, m2l_engine):
 def run_workload(args):
     """The other workloads, one JSON line each (not the headline line): two
     wires on a 0.05 um mesh, a batch of uneven windows through
-    gpx_cap_solve_batched, and the met2-bus sensitivities."""
+    gpx_cap_solve_batched, the met2-bus sensitivities, and the large block
+    (mixed precision; gradients along the 6 layers' thickness and height and
+    k, reported for 16 seeded nets)."""
     import numpy as np
     import torch
 
@@ -321,6 +324,23 @@ def run_workload(args):
         out["mixed"] = {"windows_per_s": len(probs) / dt, "s": dt, "panel_rhs_per_s": NR / dt,
                         "max_iterations": max(r["iterations"] for _, r in res),
                         "timing": "wall clock around the synchronous batched call (8 streams)"}
+    elif args.workload == "block":
+        lay = layouts.large_block()
+        p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                 mesh_max_edge_m=0.8e-6, max_panels=-1)
+        nc = len(p["nets"]) + 1
+        spans = [sensitivity.layer_span(lay.deck, name) for name, *_ in layouts.BLOCK_LAYERS]
+        params = [("thickness", z0, z1) for z0, z1 in spans] + [("height", z0, z1) for z0, z1 in spans] + [("k",)]
+        V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params)
+        rows = sorted(int(r) for r in np.random.default_rng(16).choice(nc - 1, 16, replace=False))
+        out.update(panels=len(p["verts"]), rhs=nc - 1, params=len(params), gradient_nets=rows)
+        kw = dict(base, precision=_lib.PREC_MIXED, precond=1)
+        dt0, (C, rep) = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), 1)
+        dt, (_, dC, rep2) = timed(lambda: ctx.cap_sensitivity(p["verts"], p["cond"], nc, V, **kw), 1)
+        out["mixed"] = {"ms_capacitance_only": dt0 * 1e3, "ms_capacitance_plus_gradients": dt * 1e3,
+                        "iterations": rep["iterations"], "iterations_forward_plus_adjoint": rep2["iterations"],
+                        "panel_rhs_per_s": len(p["verts"]) * (nc - 1) / dt0,
+                        "max_abs_dC_of_gradient_nets": float(np.abs(dC[:, rows, :nc - 1]).max())}
     else:  # bus
         lay = layouts.bus_crossing()
         z0, z1 = sensitivity.layer_span(lay.deck, "met2")

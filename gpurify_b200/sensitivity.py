@@ -12,9 +12,10 @@ derivative is that of the discretised Maxwell matrix.  Supported parameters
 * ``("spacing", net)``   the gap between ``net`` and the next wire of the same
   layer (higher coordinate across the wires) grows: every same-layer wire past
   ``net`` translates by +1;
-* ``("thickness", z0, z1)`` the conductors of the layer spanning [z0, z1]
-  thicken upward: vertices stretch linearly, the top faces move by +1;
-* ``("height", z0, z1)``  the conductors of that layer move up by +1;
+* ``("thickness", z0, z1)`` the metal of the layer spanning [z0, z1] (the
+  panels with every vertex in that span) thickens upward: vertices stretch
+  linearly, the top faces move by +1;
+* ``("height", z0, z1)``  the metal of that layer moves up by +1;
 * ``("k",)``             the dielectric constant: no vertex moves; with a
   homogeneous dielectric dC/dk = C / k exactly (the reference scales the
   vacuum Maxwell matrix by k, bridge.rs:405-407).
@@ -75,15 +76,17 @@ def velocity_fields(verts: np.ndarray, cond: np.ndarray, nets: Sequence[int], pa
                 if 0.5 * (box[o, ax] + box[o, 3 + ax]) > centre:
                     out[q, cond == o, :, ax] = 1.0
         elif kind in ("thickness", "height"):
+            # the panels of the layer's metal: every vertex within [z0, z1]
+            # (a net routed over several layers moves only its part on this
+            # layer; the substrate plate never moves)
             z0, z1 = float(prm[1]), float(prm[2])
             tol = 1e-12 + 1e-9 * abs(z1 - z0)
-            for o in range(ncond - 1):
-                if abs(box[o, 2] - z0) <= tol and abs(box[o, 5] - z1) <= tol:
-                    sel = cond == o
-                    if kind == "height":
-                        out[q, sel, :, 2] = 1.0
-                    else:
-                        out[q, sel, :, 2] = (pts[sel, :, 2] - z0) / (z1 - z0)
+            zv = pts[:, :, 2]
+            sel = (cond != ncond - 1) & np.all((zv >= z0 - tol) & (zv <= z1 + tol), axis=1)
+            if kind == "height":
+                out[q, sel, :, 2] = 1.0
+            else:
+                out[q, sel, :, 2] = (pts[sel, :, 2] - z0) / (z1 - z0)
         elif kind == "k":
             pass
         else:

@@ -4,7 +4,9 @@ A routing window must never let two different nets touch on one metal layer:
 the bridge groups polygons by (net, layer) and does not detect shorts, so an
 overlap would silently merge two conductors.  The batch generator must follow
 its stated distributions (conductor counts in 2..48, sides 5..60 um), and the
-generators must be reproducible from their seed."""
+generators must be reproducible from their seed.  The 6-layer large block
+keeps 0.15 um between nets, reaches its stated density and panel count, and
+its layer parameters (height, thickness) move exactly that layer's metal."""
 import math
 
 import numpy as np
@@ -99,3 +101,79 @@ def test_two_wires_geometry():
     r = rects(lay)
     assert r == [(lay.deck.layers["met1"], 0, 0, 20000, 140), (lay.deck.layers["met1"], 0, 280, 20000, 420)]
     assert math.isclose(lay.deck.pex[lay.deck.layers["met1"]].thickness_nm, 360.0)
+
+
+def min_gap_between_nets(lay, layer_ids):
+    """Smallest Chebyshev gap (nm) between metal of different nets on one layer."""
+    r = rects(lay)
+    worst = None
+    for lid in layer_ids:
+        arr = np.array([(x0, y0, x1, y1, net) for (l, x0, y0, x1, y1), net in zip(r, lay.net_of_poly) if l == lid],
+                       dtype=np.int64)
+        for i in range(len(arr)):
+            o = arr[i + 1:]
+            o = o[o[:, 4] != arr[i, 4]]
+            if len(o) == 0:
+                continue
+            gap = np.maximum(np.maximum(o[:, 0] - arr[i, 2], arr[i, 0] - o[:, 2]),
+                             np.maximum(o[:, 1] - arr[i, 3], arr[i, 1] - o[:, 3])).min()
+            worst = gap if worst is None else min(worst, gap)
+    return worst
+
+
+def layer_density(lay, lid, side_nm, cell=50):
+    m = np.zeros((side_nm // cell, side_nm // cell), bool)
+    for l, x0, y0, x1, y1 in rects(lay):
+        if l == lid:
+            m[x0 // cell:x1 // cell, y0 // cell:y1 // cell] = True
+    return m.mean()
+
+
+def test_large_block_clearance_density_and_size():
+    from gpurify_b200 import _lib
+
+    lay = layouts.large_block()
+    metals = [lid for _, lid, _, _ in layouts.BLOCK_LAYERS]
+    assert len(set(lay.net_of_poly)) == 512
+    assert min_gap_between_nets(lay, metals) >= 150
+    dens = [layer_density(lay, lid, 200000) for lid in metals]
+    assert all(0.2 <= d <= 0.5 for d in dens), dens
+    # thickness 0.36 to 1.2 um, layers stacked with dielectric between them
+    t = [lay.deck.pex[lid].thickness_nm for lid in metals]
+    h = [lay.deck.pex[lid].height_nm for lid in metals]
+    assert min(t) == 360.0 and max(t) == 1200.0
+    assert all(h[i] + t[i] < h[i + 1] for i in range(5))
+    p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                             mesh_max_edge_m=0.8e-6, max_panels=-1)
+    assert 1.2e6 <= len(p["verts"]) <= 2.0e6
+    assert len(p["nets"]) == 512
+
+
+def test_layer_parameters_move_only_their_layer():
+    """Height and thickness fields of a multi-layer block: each layer's
+    parameter moves the panels of that layer's metal only, never the plate."""
+    from gpurify_b200 import _lib, sensitivity
+
+    lay = layouts.large_block(n_nets=48, side_um=30.0, seed=9)
+    p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                             mesh_max_edge_m=0.8e-6, max_panels=-1)
+    names = [name for name, *_ in layouts.BLOCK_LAYERS]
+    spans = [sensitivity.layer_span(lay.deck, n) for n in names]
+    V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], [("height", a, b) for a, b in spans] +
+                                    [("thickness", a, b) for a, b in spans])
+    n = len(p["verts"])
+    z = p["verts"].reshape(n, 4, 3)[:, :, 2]
+    plate = p["cond"] == len(p["nets"])
+    covered = np.zeros(n, int)
+    for q, (z0, z1) in enumerate(spans):
+        Vh = V[q].reshape(n, 4, 3)
+        moved = np.abs(Vh).max(axis=(1, 2)) > 0
+        assert moved.any()
+        assert np.all((z[moved] >= z0 - 1e-12) & (z[moved] <= z1 + 1e-12))
+        assert np.all(Vh[moved][:, :, 2] == 1.0) and np.all(Vh[:, :, :2] == 0.0)
+        Vt = V[6 + q].reshape(n, 4, 3)[:, :, 2]
+        np.testing.assert_allclose(Vt[moved], (z[moved] - z0) / (z1 - z0))
+        covered += moved
+    assert covered.max() == 1
+    assert not np.any(covered[plate])
+    assert np.all(covered[~plate] == 1)
