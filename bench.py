@@ -72,6 +72,8 @@ def parse():
                          "batch: many uneven windows in one batched call; bus: met2 bus sensitivities; "
                          "block: 200 um, 6-layer, 512-net block with layer-parameter gradients (mixed)")
     ap.add_argument("--windows", type=int, default=256, help="batch workload: number of windows")
+    ap.add_argument("--block-nets", type=int, default=512, help="block workload: nets")
+    ap.add_argument("--block-side", type=float, default=200.0, help="block workload: side in um")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     return ap.parse_args()
@@ -325,14 +327,14 @@ def run_workload(args):
                         "max_iterations": max(r["iterations"] for _, r in res),
                         "timing": "wall clock around the synchronous batched call (8 streams)"}
     elif args.workload == "block":
-        lay = layouts.large_block()
+        lay = layouts.large_block(n_nets=args.block_nets, side_um=args.block_side)
         p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
                                  mesh_max_edge_m=0.8e-6, max_panels=-1)
         nc = len(p["nets"]) + 1
         spans = [sensitivity.layer_span(lay.deck, name) for name, *_ in layouts.BLOCK_LAYERS]
         params = [("thickness", z0, z1) for z0, z1 in spans] + [("height", z0, z1) for z0, z1 in spans] + [("k",)]
         V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params)
-        rows = sorted(int(r) for r in np.random.default_rng(16).choice(nc - 1, 16, replace=False))
+        rows = sorted(int(r) for r in np.random.default_rng(16).choice(nc - 1, min(16, nc - 1), replace=False))
         out.update(panels=len(p["verts"]), rhs=nc - 1, params=len(params), gradient_nets=rows)
         kw = dict(base, precision=_lib.PREC_MIXED, precond=1)
         dt0, (C, rep) = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), 1)
