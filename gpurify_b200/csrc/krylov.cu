@@ -202,17 +202,6 @@ __global__ void k_trisolve(GmresDev g) {
     }
 }
 
-// X[n][r] += inv_diag[n] * sum_i y[i][r] V_i[n][r]  (krylov.rs:154-168)
-__global__ void k_combine(const double* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ y,
-                          const double* __restrict__ d, double* __restrict__ X, int64_t N, int R) {
-    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= N * R) return;
-    const int r = (int)(o % R);
-    double s = 0.0;
-    for (int i = 0; i < ni; ++i) s += y[i * R + r] * V[i * strideV + o];
-    X[o] += d[o / R] * s;
-}
-
 // Start of a cycle: beta = ||res||, converged-at-start test, V_0 = res/beta,
 // g = (beta, 0, ...), activity flags.
 __global__ void k_cycle_start(GmresDev g, const double* __restrict__ beta) {
@@ -352,14 +341,6 @@ void launch_givens(Ctx& c, const GmresDev& g, int k) {
 void launch_trisolve(Ctx& c, const GmresDev& g) {
     KTimer t(c, K_SMALL);
     k_trisolve<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g);
-    GPX_LAUNCH_CHECK();
-    c.launches += 1;
-}
-
-void launch_combine(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, const double* d, double* X,
-                    int64_t N, int R) {
-    KTimer t(c, K_VEC, 8.0 * (ni + 2) * (double)N * R, 2.0 * ni * (double)N * R);
-    k_combine<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, y, d, X, N, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }

@@ -45,8 +45,6 @@ void launch_add(Ctx& c, double* X, const double* D, int64_t n);
 void launch_zero_cols(Ctx& c, double* V, const int32_t* mask, int64_t N, int R);
 void launch_givens(Ctx& c, const GmresDev& g, int k);
 void launch_trisolve(Ctx& c, const GmresDev& g);
-void launch_combine(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, const double* d, double* X,
-                    int64_t N, int R);
 void launch_cycle_start(Ctx& c, const GmresDev& g, const double* beta);
 void launch_cycle_end(Ctx& c, const GmresDev& g, const double* rnorm);
 void launch_count_active(Ctx& c, const int32_t* act, int R, int32_t* out);
