@@ -62,6 +62,7 @@ class FmmOpts(C.Structure):
         ("tol", C.c_double),
         ("threads", C.c_int32),
         ("rhs_limit", C.c_int32),
+        ("rhs_stride", C.c_int32),
     ]
 
 
@@ -102,6 +103,13 @@ def lib():
         L.orc_cap_dense_gmres.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
         L.orc_cap_fmm.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(FmmOpts), C.c_void_p,
                                   C.POINTER(FmmReport)]
+        L.orc_fmm_new.restype = C.c_void_p
+        L.orc_fmm_new.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                  C.POINTER(C.c_double)]
+        L.orc_fmm_solve_column.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_void_p,
+                                           C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+        L.orc_fmm_free.argtypes = [C.c_void_p]
+        L.orc_fmm_free.restype = None
         L.orc_dense_P.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
         L.orc_fmm_point_matvec.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                            C.c_void_p]
@@ -234,18 +242,57 @@ def cap_dense_gmres(verts, cond, ncond) -> np.ndarray:
 
 
 def cap_fmm(verts, cond, ncond, order=4, max_level=4, tol=1e-8, restart=200, max_restarts=50, threads=0,
-            rhs_limit=0):
+            rhs_limit=0, rhs_stride=1):
     """cap::fmm_solver::solve (cap/fmm_solver.rs:147-172). Returns (C, report dict).
-    ``rhs_limit`` > 0 solves only the first conductors (bounded CPU samples)."""
+    ``rhs_limit`` > 0 solves only that many conductors (bounded CPU samples):
+    conductors 0, rhs_stride, 2 rhs_stride, ...; the other columns stay zero."""
     v, c = _prep(verts, cond)
     C_ = np.zeros((ncond, ncond))
-    o = FmmOpts(order, max_level, restart, max_restarts, tol, threads, rhs_limit)
+    o = FmmOpts(order, max_level, restart, max_restarts, tol, threads, rhs_limit, rhs_stride)
     r = FmmReport()
     rc = lib().orc_cap_fmm(len(v), v.ctypes.data, c.ctypes.data, ncond, C.byref(o), C_.ctypes.data, C.byref(r))
     if rc != 0:
         raise RuntimeError(f"orc_cap_fmm rc={rc}")
     rep = {k: getattr(r, k) for k, _ in FmmReport._fields_}
     return C_, rep
+
+
+class FmmSolver:
+    """cap::fmm_solver::solve in steps (cap/fmm_solver.rs:147-172): the
+    operator and Jacobi preconditioner are built once (``t_setup_s``), then
+    ``solve_column(j)`` runs one conductor's GMRES and returns column j of the
+    Maxwell matrix with its iteration count."""
+
+    def __init__(self, verts, cond, ncond, order=4, max_level=4, threads=0):
+        v, c = _prep(verts, cond)
+        self._keep = (v, c)
+        self.ncond = ncond
+        t = C.c_double()
+        self.h = lib().orc_fmm_new(len(v), v.ctypes.data, c.ctypes.data, ncond, order, max_level, threads,
+                                   C.byref(t))
+        if not self.h:
+            raise RuntimeError("orc_fmm_new failed")
+        self.t_setup_s = t.value
+
+    def solve_column(self, j, tol=1e-8, restart=200, max_restarts=50):
+        col = np.zeros(self.ncond)
+        its, res = C.c_int64(), C.c_double()
+        rc = lib().orc_fmm_solve_column(self.h, j, tol, restart, max_restarts, col.ctypes.data, C.byref(its),
+                                        C.byref(res))
+        if rc < 0:
+            raise RuntimeError(f"orc_fmm_solve_column rc={rc}")
+        return col, {"iterations": its.value, "residual": res.value, "converged": rc == 0}
+
+    def close(self):
+        if self.h:
+            lib().orc_fmm_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def dense_P(verts) -> np.ndarray:

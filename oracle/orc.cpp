@@ -1537,8 +1537,11 @@ int orc_cap_fmm(int64_t n, const double* verts, const int32_t* cond, int32_t nco
     std::fill(C, C + (size_t)ncond * ncond, 0.0);
     orc_fmm_report r{};
     r.all_converged = 1;
-    const int nrhs = o->rhs_limit > 0 ? std::min(o->rhs_limit, ncond) : ncond;
-    for (int j = 0; j < nrhs; ++j) {
+    const int stride = o->rhs_stride > 1 ? o->rhs_stride : 1;
+    const int avail = (ncond + stride - 1) / stride;
+    const int nrhs = o->rhs_limit > 0 ? std::min(o->rhs_limit, avail) : avail;
+    for (int q = 0; q < nrhs; ++q) {
+        const int j = q * stride;
         std::vector<double> b = rhs_unit(s, j);
         GmresResult g = gmres(op, b.data(), &pc, {o->tol, (size_t)o->restart, (size_t)o->max_restarts});
         accumulate_c(s, g.x, j, ncond, C);
@@ -1558,6 +1561,66 @@ int orc_cap_fmm(int64_t n, const double* verts, const int32_t* cond, int32_t nco
 #endif
     return 0;
 }
+
+// The same solve split into its set-up and its per-conductor solves, so a
+// caller can time one conductor's GMRES at a time (cap/fmm_solver.rs:147-172:
+// the operator and the Jacobi preconditioner are built once, then each
+// conductor is solved in turn).
+struct OrcFmmHandle {
+    PanelSet s;
+    FmmCapOp op;
+    DiagJacobi pc;
+    int ncond;
+    int threads;
+    OrcFmmHandle(PanelSet&& set, int order, int level, int nc, int th)
+        : s(std::move(set)), op(s, order, level), ncond(nc), threads(th) {}
+};
+
+void* orc_fmm_new(int64_t n, const double* verts, const int32_t* cond, int32_t ncond, int32_t order,
+                  int32_t max_level, int32_t threads, double* t_setup_s) {
+    if (n <= 0) return nullptr;
+#ifdef _OPENMP
+    int saved = omp_get_max_threads();
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+    double t0 = now_s();
+    OrcFmmHandle* h = new OrcFmmHandle(build_set(n, verts, cond), order, max_level, ncond, threads);
+    h->pc.inv.resize((size_t)n);
+    for (size_t i = 0; i < (size_t)n; ++i) {
+        double d = 1.0;
+        h->op.diagonal(i, d);
+        h->pc.inv[i] = std::fabs(d) > 1e-30 ? 1.0 / d : 1.0;
+    }
+    if (t_setup_s) *t_setup_s = now_s() - t0;
+#ifdef _OPENMP
+    omp_set_num_threads(saved);
+#endif
+    return h;
+}
+
+// Column j of the Maxwell matrix: C_out[i] = C[i][j] for i < ncond.
+int orc_fmm_solve_column(void* handle, int32_t j, double tol, int32_t restart, int32_t max_restarts,
+                         double* C_col, int64_t* iterations, double* residual) {
+    OrcFmmHandle* h = static_cast<OrcFmmHandle*>(handle);
+    if (!h || j < 0 || j >= h->ncond) return -1;
+#ifdef _OPENMP
+    int saved = omp_get_max_threads();
+    if (h->threads > 0) omp_set_num_threads(h->threads);
+#endif
+    std::vector<double> b = rhs_unit(h->s, j);
+    GmresResult g = gmres(h->op, b.data(), &h->pc, {tol, (size_t)restart, (size_t)max_restarts});
+    std::vector<double> C((size_t)h->ncond * h->ncond, 0.0);
+    accumulate_c(h->s, g.x, j, h->ncond, C.data());
+    for (int i = 0; i < h->ncond; ++i) C_col[i] = C[(size_t)i * h->ncond + j];
+    if (iterations) *iterations = (int64_t)g.iterations;
+    if (residual) *residual = g.residual;
+#ifdef _OPENMP
+    omp_set_num_threads(saved);
+#endif
+    return g.converged ? 0 : 1;
+}
+
+void orc_fmm_free(void* handle) { delete static_cast<OrcFmmHandle*>(handle); }
 
 int orc_fmm_point_matvec(int64_t n, const double* pts3, const double* q, int32_t order, int32_t max_level,
                          int32_t with_p2p, double* y) {

@@ -78,7 +78,8 @@ typedef struct {
     int32_t order, max_level, restart, max_restarts;
     double tol;
     int32_t threads;          /* 0 = OpenMP default */
-    int32_t rhs_limit;        /* > 0: solve only the first rhs_limit conductors */
+    int32_t rhs_limit;        /* > 0: solve only rhs_limit conductors (a bounded CPU sample) */
+    int32_t rhs_stride;       /* > 1: the sampled conductors are 0, stride, 2 stride, ... */
 } orc_fmm_opts;
 typedef struct {
     int64_t total_iterations;
@@ -91,6 +92,14 @@ typedef struct {
 } orc_fmm_report;
 int orc_cap_fmm(int64_t n, const double* verts, const int32_t* cond, int32_t ncond,
                 const orc_fmm_opts* opts, double* C_out, orc_fmm_report* rep);
+/* The same solve in steps: build the operator and preconditioner once
+ * (t_setup_s receives the seconds), then solve one conductor's column at a
+ * time (0 converged, 1 not converged, -1 bad argument). */
+void* orc_fmm_new(int64_t n, const double* verts, const int32_t* cond, int32_t ncond, int32_t order,
+                  int32_t max_level, int32_t threads, double* t_setup_s);
+int orc_fmm_solve_column(void* handle, int32_t j, double tol, int32_t restart, int32_t max_restarts,
+                         double* C_col, int64_t* iterations, double* residual);
+void orc_fmm_free(void* handle);
 /* Dense GMRES path (cap/solver.rs:118-125, tol 1e-8 restart 100). */
 int orc_cap_dense_gmres(int64_t n, const double* verts, const int32_t* cond, int32_t ncond,
                         double* C_out);

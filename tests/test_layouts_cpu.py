@@ -177,3 +177,24 @@ def test_layer_parameters_move_only_their_layer():
     assert covered.max() == 1
     assert not np.any(covered[plate])
     assert np.all(covered[~plate] == 1)
+
+
+def test_config_parity_fixture_meshes_are_the_product_meshes():
+    """The product library's host panelisation reproduces, bit for bit, the
+    meshes the oracle fixtures of tests/golden/config_parity.json were made
+    on (the config-2-style window, the 64-net benchmark window, the bus)."""
+    import json
+    import os
+
+    from gpurify_b200 import _lib
+    from tests.golden import make_config_golden as mk
+
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "config_parity.json")))
+
+    def panelize(lay, edge):
+        return _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                    mesh_max_edge_m=edge, max_panels=-1)
+
+    assert mk.verts_sha256(mk.window16_panels(panelize)["verts"]) == gold["window16"]["verts_sha256"]
+    assert mk.verts_sha256(mk.window64_panels(panelize)["verts"]) == gold["window64"]["verts_sha256"]
+    assert mk.verts_sha256(mk.bus_panels(panelize)[1]["verts"]) == gold["bus"]["verts_sha256"]
