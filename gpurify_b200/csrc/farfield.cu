@@ -698,7 +698,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     const unsigned rchunks64 = cdiv(Rb, 64), rchunks_tree = cdiv(Rb, RC);
     GPX_CUDA(cudaMemsetAsync(L, 0, (size_t)p.nbox * NS * Rb * sizeof(T), s));
     {
-        KTimer t(c, K_P2M, (double)p.N * (wb * R + wb * N3 + 8.0) + (p.nleaf + 2.0 * f.npart) * box_bytes,
+        KTimer t(c, prec_tag<T>(K_P2M), (double)p.N * (wb * R + wb * N3 + 8.0) + (p.nleaf + 2.0 * f.npart) * box_bytes,
                  2.0 * (double)p.N * N3 * R);
         k_p2m<T, N><<<dim3(p.nitems, rchunks64), 256, 0, s>>>(p, f.p2m_slot, X, w.src, w.src_area, E, R, Rb);
         GPX_LAUNCH_CHECK();
@@ -718,7 +718,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     for (int l = Lv; l >= 3; --l) {
         const int pb0 = f.lvl_off[l - 1], npb = f.lvl_off[l] - pb0, nch = f.lvl_off[l + 1] - f.lvl_off[l];
         if (npb == 0) continue;
-        KTimer t(c, K_M2M, (double)(npb + nch) * box_bytes, 2.0 * 14.0 * N * N3 * R * (double)npb);
+        KTimer t(c, prec_tag<T>(K_M2M), (double)(npb + nch) * box_bytes, 2.0 * 14.0 * N * N3 * R * (double)npb);
         k_m2m_tree<T, N><<<dim3(npb, rchunks_tree), 256, smem, s>>>(p, pb0, f.child_first, f.child_count, E, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
@@ -727,7 +727,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
         const int b0 = f.lvl_off[2], nb = f.lvl_off[Lv + 1] - b0;
         const double pairs = (double)(f.m2l_off[b0 + nb] - f.m2l_off[b0]);
         if (pairs > 0) {
-            KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
+            KTimer t(c, prec_tag<T>(K_M2L), 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
             m2l(-1, b0, nb, 0.0);
             c.launches += 1;
         }
@@ -737,7 +737,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
             if (nb == 0) continue;
             const double pairs = (double)(f.m2l_off[b0 + nb] - f.m2l_off[b0]);
             if (pairs == 0) continue;
-            KTimer t(c, K_M2L, 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
+            KTimer t(c, prec_tag<T>(K_M2L), 2.0 * nb * box_bytes, 2.0 * (double)N3 * N3 * R * pairs);
             m2l(l, b0, nb, 1.0 / f.lvl_half[l]);
             c.launches += 1;
         }
@@ -745,13 +745,13 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     for (int l = 2; l < Lv; ++l) {
         const int pb0 = f.lvl_off[l], npb = f.lvl_off[l + 1] - pb0, ncb = f.lvl_off[l + 2] - f.lvl_off[l + 1];
         if (ncb == 0) continue;
-        KTimer t(c, K_L2L, (double)(npb + 2 * ncb) * box_bytes, 2.0 * 14.0 * N * N3 * R * (double)npb);
+        KTimer t(c, prec_tag<T>(K_L2L), (double)(npb + 2 * ncb) * box_bytes, 2.0 * 14.0 * N * N3 * R * (double)npb);
         k_l2l_tree<T, N><<<dim3(npb, rchunks_tree), 256, smem, s>>>(p, pb0, f.child_first, f.child_count, L, Rb);
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
     {
-        KTimer t(c, K_L2P, (double)p.N * (16.0 * R + 24.0 * N) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
+        KTimer t(c, prec_tag<T>(K_L2P), (double)p.N * (16.0 * R + 24.0 * N) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
         k_l2p<T, N><<<dim3(p.nitems, cdiv(R, 64)), 256, 0, s>>>(p, L, w.tgt, w.tgt_area, Y, R, Rb, coef);
         GPX_LAUNCH_CHECK();
         c.launches += 1;

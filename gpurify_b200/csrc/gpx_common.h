@@ -103,10 +103,18 @@ struct DBuf {
 struct DevM2L;  // device M2L operator table, cached per (order, mode)
 
 // Kernel classes timed by the optional per-kernel event timer.
+// The operator's kernel classes are split by precision: the plain names hold
+// the FP32 / TF32 launches of the mixed path's inner operator, the *64 names
+// the FP64 launches (the plain path, and the mixed path's refinement
+// residuals).
 enum KTag {
     K_NEAR_ASSEMBLE = 0, K_NEAR_APPLY, K_P2M, K_M2M, K_M2L, K_L2L, K_L2P, K_GS_DOT, K_GS_AXPY, K_VEC, K_SMALL,
-    K_NTAGS
+    K_NEAR_APPLY64, K_P2M64, K_M2M64, K_M2L64, K_L2L64, K_L2P64, K_NTAGS
 };
+// The FP64 class of an operator kernel class.
+constexpr int f64_tag(int tag) { return tag >= K_NEAR_APPLY && tag <= K_L2P ? tag + (K_NEAR_APPLY64 - K_NEAR_APPLY) : tag; }
+template <class T>
+constexpr int prec_tag(int tag) { return sizeof(T) == 8 ? f64_tag(tag) : tag; }
 
 struct KStats {
     int64_t launches = 0;

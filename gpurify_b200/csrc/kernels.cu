@@ -291,7 +291,7 @@ void launch_diag_inv(Ctx& c, const DevPlan& p, const double* P, double* inv) {
 
 void launch_near_apply(Ctx& c, const DevPlan& p, int64_t nnz, const double* P, const double* X, double* Y, int R) {
     if (p.nleaf == 0) return;
-    KTimer t(c, K_NEAR_APPLY, 8.0 * nnz + 16.0 * (double)p.N * R, 2.0 * (double)nnz * R);
+    KTimer t(c, K_NEAR_APPLY64, 8.0 * nnz + 16.0 * (double)p.N * R, 2.0 * (double)nnz * R);
     k_near_apply<double><<<dim3(p.nitems, (R + 63) / 64), 64, 0, c.stream>>>(p, P, X, Y, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;

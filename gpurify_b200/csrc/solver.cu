@@ -912,6 +912,8 @@ Opts normalize(const gpx_solve_opts* o) {
     r.mixed_m2l = o->mixed_m2l;
     r.graphs = o->no_graphs ? 0 : 1;
     r.batch_streams = o->batch_streams;
+    r.col_begin = o->col_begin;
+    r.col_count = o->col_count;
     return r;
 }
 
@@ -1141,7 +1143,13 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     check_problem(n, verts, cond, ncond, o);
     const int depth = choose_depth(o, n, verts);
     const bool dense = depth == 1;
-    const int Rn = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;  // conductors solved
+    const int Rall = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;  // conductors of a full solve
+    if (o.col_count < 0 || (o.col_count > 0 && (o.col_begin < 0 || o.col_begin + o.col_count > ncond)))
+        throw Error(GPX_ERR_INVALID_ARG, "column subset [col_begin, col_begin + col_count) outside the conductors");
+    // conductor columns solved: [cb, cb + Rn)
+    const int cb = o.col_count > 0 ? o.col_begin : 0;
+    const int Rn = o.col_count > 0 ? o.col_count : Rall;
+    const bool full = o.col_count == 0;
     // Conductors are solved in chunks of at most kMaxChunk columns sharing one
     // operator (its expansion and Krylov buffers are sized for one chunk).
     // Columns are padded to a multiple of 4 (16-byte rows); padding columns
@@ -1161,7 +1169,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     for (int c0 = 0; c0 < Rn; c0 += Rc) {
         const int nc = std::min(Rc, Rn - c0);
         std::vector<int32_t> rhs_cond(R);
-        for (int r = 0; r < R; ++r) rhs_cond[r] = r < nc ? c0 + r : -1;
+        for (int r = 0; r < R; ++r) rhs_cond[r] = r < nc ? cb + c0 + r : -1;
         DBuf<int32_t> d_rhs;
         d_rhs.upload(rhs_cond, ctx.stream);
         DBuf<double> X;
@@ -1190,9 +1198,9 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     for (int i = 0; i < ncond; ++i)
         for (int j = 0; j < ncond; ++j) {
             double v;
-            if (j < Rn)
-                v = hc[(size_t)i * Rn + j];
-            else if (i < Rn)
+            if (j >= cb && j < cb + Rn)
+                v = hc[(size_t)i * Rn + (j - cb)];
+            else if (full && i < Rn)
                 v = hc[(size_t)j * Rn + i];  // substrate column by symmetry
             else
                 v = std::nan("");

@@ -22,6 +22,7 @@ struct Opts {
     int mixed_m2l = 0;
     int graphs = 1;         // capture operator applies into CUDA graphs
     int batch_streams = 0;  // batched solves: concurrent streams (0 -> default)
+    int col_begin = 0, col_count = 0;  // column subset (col_count 0: every column)
 };
 Opts normalize(const gpx_solve_opts* o);
 

@@ -294,12 +294,25 @@ std::mutex g_small_mu[kMaxDevices];
 double* g_small_ptr[kMaxDevices] = {};
 
 // Device address of this device's scratch array.  The first call on a device
-// (made with that device current and its lock held) looks the address up and
-// raises the panel kernel's dynamic shared-memory limit.
+// (made with that device current and its lock held) looks the address up,
+// loads every kernel this entry point launches and raises the panel kernel's
+// dynamic shared-memory limit.  With CUDA's lazy module loading a kernel is
+// otherwise loaded, and its device memory taken, on its first launch: a later
+// call that reaches a kernel the earlier calls did not (k_small_gemm runs
+// only above 32 panels) would then allocate.  Querying each kernel's
+// attributes here loads them all up front.
 double* small_scratch(int dev) {
     if (!g_small_ptr[dev]) {
         void* p = nullptr;
         GPX_CUDA(cudaGetSymbolAddress(&p, g_small_scratch));
+        const void* kernels[] = {(const void*)k_small_setup,     (const void*)k_small_assemble,
+                                 (const void*)k_small_panel,     (const void*)k_small_swap_trsm,
+                                 (const void*)k_small_gemm,      (const void*)k_small_diag_back,
+                                 (const void*)k_small_maxwell};
+        for (const void* k : kernels) {
+            cudaFuncAttributes fa{};
+            GPX_CUDA(cudaFuncGetAttributes(&fa, k));
+        }
         GPX_CUDA(cudaFuncSetAttribute(k_small_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem));
         g_small_ptr[dev] = static_cast<double*>(p);
     }

@@ -110,7 +110,12 @@ typedef struct {
                                 captured CUDA graph (results are identical) */
     int32_t batch_streams;   /* gpx_cap_solve_batched: windows solved concurrently, one stream each;
                                 0 -> 8 */
-    int32_t reserved[3];
+    int32_t col_begin;       /* gpx_cap_solve: with col_count > 0, solve only the conductor columns
+                                [col_begin, col_begin + col_count) (one rank's share of a window whose
+                                right-hand sides are spread over several GPUs); the other columns of
+                                maxwell_out are NaN */
+    int32_t col_count;       /* 0 -> every column (all but the substrate with skip_ground_rhs) */
+    int32_t reserved[1];
 } gpx_solve_opts;
 
 typedef struct {
@@ -232,9 +237,12 @@ gpx_status gpx_potential_matrix(gpx_ctx* ctx, int64_t n_src, const double* src_v
  * The caller zeroes nothing: the call clears its own status word before its
  * first launch, and writes every other scratch element before reading it.
  * The call runs on the context's stream and waits for that stream before it
- * returns.  The first call on each device also does a one-time set-up (looks
- * up the scratch array's device address and raises one kernel's shared-memory
- * limit); make that first call before any stream capture on that device.
+ * returns.  The first call on each device also does a one-time set-up: it looks
+ * up the scratch array's device address, loads every kernel the entry point
+ * launches (CUDA loads kernels lazily by default, and loading one takes device
+ * memory) and raises one kernel's shared-memory limit.  Make that first call
+ * before any stream capture on that device, and before the caller's own pool
+ * reserves the device memory it means to keep; later calls take none.
  * Every call on one device uses the same scratch array, so two calls that
  * overlapped would race on it; the library therefore serialises the calls of
  * one process per device with a lock held until the call's stream work has
@@ -302,10 +310,15 @@ gpx_status gpx_bridge_panelize(gpx_ctx* ctx, const gpx_geometry_store* store, co
                                int64_t nets_cap, int64_t* n_nets, uint32_t* err_polygon);
 
 /* ---- instrumentation ---- */
-/* Kernel classes of gpx_ctx_kernel_stats. */
+/* Kernel classes of gpx_ctx_kernel_stats.  The operator's classes are split
+ * by precision: GPX_K_NEAR_APPLY .. GPX_K_L2P count the FP32 / TF32 launches
+ * (the mixed path's inner operator), GPX_K_NEAR_APPLY_F64 .. GPX_K_L2P_F64 the
+ * FP64 ones (the plain path, and the mixed path's refinement residuals). */
 typedef enum {
     GPX_K_NEAR_ASSEMBLE = 0, GPX_K_NEAR_APPLY = 1, GPX_K_P2M = 2, GPX_K_M2M = 3, GPX_K_M2L = 4, GPX_K_L2L = 5,
-    GPX_K_L2P = 6, GPX_K_GS_DOT = 7, GPX_K_GS_AXPY = 8, GPX_K_VEC = 9, GPX_K_SMALL = 10, GPX_K_COUNT = 11
+    GPX_K_L2P = 6, GPX_K_GS_DOT = 7, GPX_K_GS_AXPY = 8, GPX_K_VEC = 9, GPX_K_SMALL = 10,
+    GPX_K_NEAR_APPLY_F64 = 11, GPX_K_P2M_F64 = 12, GPX_K_M2M_F64 = 13, GPX_K_M2L_F64 = 14, GPX_K_L2L_F64 = 15,
+    GPX_K_L2P_F64 = 16, GPX_K_COUNT = 17
 } gpx_kernel_class;
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
 void* gpx_ctx_stream(gpx_ctx* ctx);
