@@ -103,9 +103,14 @@ void launch_to_f32(Ctx& c, const double* a, float* b, int64_t n);
 void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n);
 // Y = P_near X on the tensor cores (TF32 inputs, FP32 accumulation, FP64 Y),
 // work items of <= 128 rows (it_leaf, it_row0); P holds TF32-rounded values;
-// R a multiple of 4.  *err becomes nonzero if a bounded pipeline wait expired.
+// X is given as its TF32 split Xhi + Xlo (launch_split_tf32); R a multiple
+// of 4.  *err becomes nonzero if a bounded pipeline wait expired.
 void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, const int32_t* it_leaf,
-                          const int32_t* it_row0, const float* P, const float* X, double* Y, int R, int* err);
+                          const int32_t* it_row0, const float* P, const float* Xhi, const float* Xlo, double* Y, int R,
+                          int* err);
+// X32 = (float) X, and its TF32 split Xhi = tf32(X), Xlo = tf32(X - Xhi)
+// (n values each).
+void launch_split_tf32(Ctx& c, const double* X, float* X32, float* Xhi, float* Xlo, int64_t n);
 // Far-field source weights W[j][m]: the Chebyshev interpolation weights of
 // panel j's charge in its leaf; quad 0: at the centroid (the reference's
 // point lumping), quad 1: averaged over 2x2 Gauss points of the panel.

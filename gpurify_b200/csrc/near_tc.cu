@@ -7,47 +7,58 @@
 // the near blocks from HBM.
 //
 // One CTA per (work item = target leaf and <= 128 of its rows, 64-wide chunk
-// of right-hand sides), 128 threads, D = 128 x 64 FP32 in TMEM.  The
-// contraction runs over the leaf's S near-source panels in slices of 32:
-//   A slice (128 x 32) = P rows, K-major, streamed from HBM with cp.async into
-//     a 4-stage ring of 128-byte-swizzled tiles, issued two slices ahead;
-//   B slice (64 x 32) = the 32 gathered source rows of X (L2-resident),
-//     loaded two slices ahead into registers and written transposed (K-major)
-//     into a double buffer as two TF32 tiles, x_hi = tf32(x) and
-//     x_lo = tf32(x - x_hi).
+// of right-hand sides), D = 128 x 64 FP32 in TMEM.  The contraction runs over
+// the leaf's S near-source panels in slices of 32; each slice is one stage of
+// a kStages ring in shared memory:
+//   A (128 x 32, K-major, 128-byte swizzle) = the item's P rows, streamed from
+//     HBM;
+//   B_hi, B_lo (32 x 64 each, MN-major, 128-byte swizzle) = the 32 source
+//     panels' rows of X_hi = tf32(x) and X_lo = tf32(x - x_hi), gathered from
+//     the L2-resident split copies written by k_split_tf32.  A source row of
+//     X is 64 contiguous FP32 values, which is exactly one K row of an
+//     MN-major tile, so the gather is a plain copy: no transpose and no
+//     per-slice register work.
 // D += A B_hi + A B_lo represents X to about 2^-21, so the operator stays
 // linear in X (the GMRES inner solves converge as for any fixed matrix); the
 // one approximation left is P rounded once to TF32 (round to nearest, stored
 // that way), a fixed perturbation the FP64 refinement removes.
-// One thread issues the eight K=8 MMAs of a slice and commits them to the
-// stage's mbarrier; a stage or B buffer is refilled only after the MMAs that
-// read it completed.  Every mbarrier wait is bounded: on expiry the kernel
-// records an error code, drains (bounded) its own MMAs, frees its TMEM and
-// returns.
+// Warp-specialised: four producer warps copy each stage with cp.async
+// straight into the swizzled layouts and signal the stage's `full` mbarrier
+// (cp.async.mbarrier.arrive, 128 arrivals); one thread of the fifth warp
+// waits on `full`, issues the eight K=8 MMAs of the slice and commits them to
+// the stage's `empty` mbarrier, which the producers wait on before refilling
+// the stage.  No block-wide barrier runs in the main loop.  Rows past the
+// item's last row are not loaded (their D rows are never stored); source
+// columns past S are zero-filled in both A and B.  Every mbarrier wait is
+// bounded: on expiry the kernel records an error code, drains (bounded) its
+// own MMAs and copies, frees its TMEM and returns.
 #include "kernels.cuh"
 
 namespace gpx {
 
 namespace {
 
-constexpr int kThreads = 128;
-constexpr int kStages = 4;              // A ring; A is issued kStages - 2 slices ahead
-constexpr uint32_t kATile = 128 * 128;  // 128 rows x 128 B
-constexpr uint32_t kBTile = 64 * 128;   // 64 rows x 128 B
-constexpr uint32_t kBBuf = 2 * kBTile;  // hi + lo
-constexpr uint32_t kBOff = kStages * kATile;
-constexpr uint32_t kSmemBytes = kBOff + 2 * kBBuf + 128 + 1024;  // + barriers, TMEM slot, alignment slack
+constexpr int kProducers = 128;            // four producer warps, also the epilogue
+constexpr int kThreads = kProducers + 32;  // + the MMA warp
+constexpr int kStages = 3;
+constexpr uint32_t kATile = 128 * 128;      // 128 rows x 128 B
+constexpr uint32_t kBTile = 32 * 256;       // 32 K rows x 64 FP32
+constexpr uint32_t kStage = kATile + 2 * kBTile;  // 32 KB, a multiple of 1024
+// + alignment slack, barriers and TMEM slot, and 4 KB past the last stage so
+// that no MMA operand read can leave the allocation
+constexpr uint32_t kSmemBytes = kStages * kStage + 1024 + 256 + 4096;
 constexpr uint32_t kTmemCols = 64;
 constexpr int kWaitLimit = 1 << 22;
-// Instruction descriptor: D F32, A/B TF32, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// Instruction descriptor: D F32, A/B TF32, A K-major, B MN-major, N = 64, M = 128.
+constexpr uint32_t kIdesc =
+    (1u << 4) | (2u << 7) | (2u << 10) | (1u << 16) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor: 128 B swizzle, K-major, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
+// K-major operand, 128 B swizzle: 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t desc_k_sw128(uint32_t addr) {
     uint64_t d = 0;
     d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
     d |= (uint64_t)1 << 16;
@@ -57,9 +68,30 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
     return d;
 }
 
-// Byte offset of 16-byte chunk `chunk` of row `row` in a 128-byte-swizzled tile.
+// MN-major operand, 128 B swizzle: an atom is 8 K rows x 128 B (32 FP32 along
+// MN); `lbo` = bytes between the atoms of consecutive 32-wide MN blocks,
+// `sbo` = bytes between consecutive 8-row K groups.
+__device__ __forceinline__ uint64_t desc_mn_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)(lbo >> 4) << 16;
+    d |= (uint64_t)(sbo >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Byte offset of 16-byte chunk `chunk` of row `row` in a 128-byte-swizzled
+// K-major tile.
 __device__ __forceinline__ uint32_t swz(uint32_t row, uint32_t chunk) {
     return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk ^ (row & 7u)) << 4);
+}
+
+// Byte offset of 16-byte chunk q (0..15: FP32 columns 4q..4q+3) of K row k
+// (0..31) in the MN-major B tile: atom (K group k/8, MN block q/8) at
+// (2 (k/8) + q/8) x 1024 B, row k%8 of the atom, chunk q%8 swizzled.
+__device__ __forceinline__ uint32_t swz_mn(uint32_t k, uint32_t q) {
+    return ((k >> 3) * 2u + (q >> 3)) * 1024u + (k & 7u) * 128u + (((q & 7u) ^ (k & 7u)) << 4);
 }
 
 __device__ __forceinline__ float to_tf32(float x) {
@@ -95,16 +127,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int32_t* __restrict__ it_leaf,
                                                             const int32_t* __restrict__ it_row0,
-                                                            const float* __restrict__ P, const float* __restrict__ X,
-                                                            double* __restrict__ Y, int R, int* __restrict__ err) {
+                                                            const float* __restrict__ P,
+                                                            const float* __restrict__ Xhi,
+                                                            const float* __restrict__ Xlo, double* __restrict__ Y,
+                                                            int R, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* sbase = smem_raw + (base - raw);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + kBOff + 2 * kBBuf);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kStages);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sbase + kStages * kStage);
+    uint64_t* empty = full + kStages;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + kStages);
     __shared__ int64_t s_beg[28];
     __shared__ int32_t s_pre[29];
+    __shared__ int s_bad;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int t = it_leaf[blockIdx.x];
     const int r0 = it_row0[blockIdx.x];
@@ -118,11 +154,14 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
 
     if (warp == 1) near_ranges_warp(p, t, lane, s_beg, s_pre);
     if (tid == 0) {
-        for (int st = 0; st < kStages; ++st)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[st])));
+        for (int st = 0; st < kStages; ++st) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[st])), "r"(kProducers));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[st])));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_bad = 0;
     }
-    if (warp == 0) {
+    if (warp == 4) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -132,120 +171,91 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tslot;
 
-    // A: 1024 16-byte chunks per slice, 8 per thread.
-    auto issue_a = [&](int j) {
-        if (j < nsl) {
-            const uint32_t a = base + (uint32_t)(j % kStages) * kATile;
+    if (tid < kProducers) {
+        // B: this thread copies K row kb = tid / 4 of every slice, chunks
+        // 4 (tid % 4) .. 4 (tid % 4) + 3 of X_hi and X_lo.
+        const int kb = tid >> 2, q0 = (tid & 3) * 4;
+        int e = 0;
+        for (int j = 0; j < nsl; ++j) {
+            const int st = j % kStages;
+            if (j >= kStages && !mbar_wait(smem_u32(&empty[st]), (uint32_t)(((j / kStages) - 1) & 1))) {
+                atomicExch(&s_bad, 1);
+                break;
+            }
+            if (*(volatile int*)&s_bad) break;
+            const uint32_t a = base + (uint32_t)st * kStage;
+            const uint32_t bh = a + kATile, bl = bh + kBTile;
             const int k0 = j * 32;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int id = tid + kThreads * q, row = id >> 3, c16 = id & 7;
-                const bool ok = row < m && k0 + 4 * c16 < Sp;
-                cp16(a + swz(row, c16), ok ? (const void*)(Pi + (int64_t)row * Sp + k0 + 4 * c16) : (const void*)P, ok);
-            }
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-    // B: 32 panels x 16 quads of right-hand sides per slice; this thread's
-    // panels are kk = (lane >> 1) + 16 h, its quads c4 = 2 (2 warp + g) + (lane & 1).
-    int ep[2] = {0, 0};
-    auto load_b = [&](int j, float4 (&v)[4]) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int k = j * 32 + (lane >> 1) + 16 * h;
-            int64_t gid = -1;
-            if (j < nsl && k < S) {
-                while (s_pre[ep[h] + 1] <= k) ++ep[h];
-                gid = s_beg[ep[h]] + (k - s_pre[ep[h]]);
-            }
-#pragma unroll
-            for (int g = 0; g < 2; ++g) {
-                const int c4 = 2 * (2 * warp + g) + (lane & 1);
-                const int col = rc + 4 * c4;
-                float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (gid >= 0 && col < R) x = *reinterpret_cast<const float4*>(X + gid * R + col);
-                v[2 * h + g] = x;
-            }
-        }
-    };
-    auto store_b = [&](int j, const float4 (&v)[4]) {
-        uint8_t* b = sbase + kBOff + (size_t)(j & 1) * kBBuf;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int kk = (lane >> 1) + 16 * h;
-#pragma unroll
-            for (int g = 0; g < 2; ++g) {
-                const int c4 = 2 * (2 * warp + g) + (lane & 1);
-                const float4 x = v[2 * h + g];
-                const float e[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const uint32_t off = swz(4 * c4 + i, kk >> 2) + (kk & 3) * 4;
-                    const float hi = to_tf32(e[i]);
-                    *reinterpret_cast<float*>(b + off) = hi;
-                    *reinterpret_cast<float*>(b + kBTile + off) = to_tf32(e[i] - hi);
+                const int id = tid + kProducers * q, row = id >> 3, c16 = id & 7;
+                if (row < m) {
+                    const bool ok = k0 + 4 * c16 < Sp;
+                    cp16(a + swz(row, c16), ok ? (const void*)(Pi + (int64_t)row * Sp + k0 + 4 * c16) : (const void*)P,
+                         ok);
                 }
             }
+            const int k = k0 + kb;
+            int64_t gid = -1;
+            if (k < S) {
+                while (s_pre[e + 1] <= k) ++e;
+                gid = s_beg[e] + (k - s_pre[e]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int q = q0 + i, col = rc + 4 * q;
+                const bool ok = gid >= 0 && col < R;
+                const int64_t off = ok ? gid * R + col : 0;
+                const uint32_t d = swz_mn((uint32_t)kb, (uint32_t)q);
+                cp16(bh + d, Xhi + off, ok);
+                cp16(bl + d, Xlo + off, ok);
+            }
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st])) : "memory");
         }
-    };
-
-    bool bad = false;
-    int issued = 0;  // slices whose MMAs were committed
-    float4 breg[2][4];
-    for (int j = 0; j < kStages - 2; ++j) issue_a(j);
-    load_b(0, breg[0]);
-    load_b(1, breg[1]);
-    for (int j = 0; j < nsl; ++j) {
-        if (j >= 2) {
-            const bool ok = mbar_wait(smem_u32(&bars[(j - 2) % kStages]), (uint32_t)(((j - 2) / kStages) & 1));
-            if (__syncthreads_or(!ok)) {
-                bad = true;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (tid == kProducers) {
+        int issued = 0;
+        for (int j = 0; j < nsl; ++j) {
+            const int st = j % kStages;
+            if (!mbar_wait(smem_u32(&full[st]), (uint32_t)((j / kStages) & 1))) {
+                atomicExch(&s_bad, 1);
                 break;
             }
-        }
-        issue_a(j + kStages - 2);
-        if (j & 1) {
-            store_b(j, breg[1]);
-            load_b(j + 2, breg[1]);
-        } else {
-            store_b(j, breg[0]);
-            load_b(j + 2, breg[0]);
-        }
-        asm volatile("cp.async.wait_group %0;" ::"n"(kStages - 2) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t abase = base + (uint32_t)(j % kStages) * kATile;
-            const uint32_t bbase = base + kBOff + (uint32_t)(j & 1) * kBBuf;
+            const uint32_t a = base + (uint32_t)st * kStage;
+            const uint32_t bh = a + kATile, bl = bh + kBTile;
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                const uint64_t ad = desc_sw128(abase + (uint32_t)(s >> 1) * 32u);
-                const uint64_t bd = desc_sw128(bbase + (uint32_t)(s & 1) * kBTile + (uint32_t)(s >> 1) * 32u);
-                const uint32_t accf = (j > 0 || s > 0) ? 1u : 0u;
+            for (int kk = 0; kk < 4; ++kk) {
+                const uint64_t ad = desc_k_sw128(a + (uint32_t)kk * 32u);
+                const uint64_t bdh = desc_mn_sw128(bh + (uint32_t)kk * 2048u, 1024u, 2048u);
+                const uint64_t bdl = desc_mn_sw128(bl + (uint32_t)kk * 2048u, 1024u, 2048u);
+                const uint32_t accf = (j > 0 || kk > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(kIdesc), "r"(accf));
+                    "l"(ad), "l"(bdh), "r"(kIdesc), "r"(accf));
+                asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(ad), "l"(bdl),
+                             "r"(kIdesc));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&bars[j % kStages]))
+                             smem_u32(&empty[st]))
                          : "memory");
+            issued = j + 1;
         }
-        issued = j + 1;
+        // Drain: the last commit covers every MMA issued before it (after an
+        // expired wait too, so the TMEM is idle before it is freed).
+        if (issued > 0) {
+            const int last = issued - 1;
+            if (!mbar_wait(smem_u32(&empty[last % kStages]), (uint32_t)((last / kStages) & 1))) atomicExch(&s_bad, 1);
+        }
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // Drain: the last commit covers every MMA issued before it (after an
-    // expired wait too, so the TMEM is idle before it is freed).
-    if (issued > 0) {
-        const int last = issued - 1;
-        const bool ok = mbar_wait(smem_u32(&bars[last % kStages]), (uint32_t)((last / kStages) & 1));
-        if (__syncthreads_or(!ok)) bad = true;
-    }
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (bad) {
+    if (s_bad) {
         if (tid == 0) atomicExch(err, 1);
-    } else {
+    } else if (tid < kProducers) {
+        // Epilogue: warp w (0..3) reads TMEM lanes 32w..32w+31 = rows of D.
         const int row = warp * 32 + lane;
         double* dst = row < m ? Y + (tb + row) * R + rc : nullptr;
 #pragma unroll
@@ -266,7 +276,20 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    if (warp == 4) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+// X32 = (float) x for the FP32 far field, and the split X_hi = tf32(x),
+// X_lo = tf32(x - X_hi) (round to nearest) for the tensor-core near apply.
+__global__ void k_split_tf32(const double* __restrict__ X, float* __restrict__ X32, float* __restrict__ Xhi,
+                             float* __restrict__ Xlo, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = X[i];
+        const float hi = to_tf32((float)x);
+        X32[i] = (float)x;
+        Xhi[i] = hi;
+        Xlo[i] = to_tf32((float)(x - (double)hi));
+    }
 }
 
 __global__ void k_to_tf32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
@@ -285,13 +308,22 @@ void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n) {
 }
 
 void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, const int32_t* it_leaf,
-                          const int32_t* it_row0, const float* P, const float* X, double* Y, int R, int* err) {
+                          const int32_t* it_row0, const float* P, const float* Xhi, const float* Xlo, double* Y, int R,
+                          int* err) {
     if (nitems == 0) return;
     if (R % 4 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core near apply needs R a multiple of 4");
-    KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 12.0 * (double)p.N * R, 2.0 * (double)nnz * R);
+    KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 16.0 * (double)p.N * R, 4.0 * (double)nnz * R);
     set_smem_once(k_near_apply_tc, (int)kSmemBytes);
-    k_near_apply_tc<<<dim3(nitems, (R + 63) / 64), kThreads, kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, X, Y, R,
-                                                                                     err);
+    k_near_apply_tc<<<dim3(nitems, (R + 63) / 64), kThreads, kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xhi, Xlo,
+                                                                                     Y, R, err);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_split_tf32(Ctx& c, const double* X, float* X32, float* Xhi, float* Xlo, int64_t n) {
+    if (n == 0) return;
+    KTimer t(c, K_VEC, 20.0 * n, 0.0);
+    k_split_tf32<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c.stream>>>(X, X32, Xhi, Xlo, n);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }

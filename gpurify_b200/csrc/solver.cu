@@ -356,6 +356,7 @@ struct Operator {
     const DevM2L* m2l;
     DBuf<double> P, inv_diag, E64, L64;
     DBuf<float> P32, E32, L32, X32, W32, Sc32;
+    DBuf<float> Xhi32, Xlo32;  // TF32 split of the FP32 apply's input (tensor-core near apply)
     DBuf<double> Sc;  // transposed operator: collocation weights as P2M weights
     FarWeights<double> w64;
     FarWeights<float> w32;
@@ -513,6 +514,10 @@ struct Operator {
             else
                 launch_to_f32(ctx, P.p, P32.p, pl.nnz());
             X32.alloc((size_t)pl.N * R, s);
+            if (mixed_near == 0) {
+                Xhi32.alloc((size_t)pl.N * R, s);
+                Xlo32.alloc((size_t)pl.N * R, s);
+            }
             tc_err.alloc(1, s);
             tc_err.zero();
             if (has_far()) {
@@ -687,12 +692,14 @@ struct Operator {
         applies32 += 1;
     }
     void apply32_direct(const double* X, double* Y) {
-        launch_to_f32(ctx, X, X32.p, pl.N * R);
-        if (mixed_near == 0)
-            launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, X32.p, Y,
-                                 R, tc_err.p);
-        else
+        if (mixed_near == 0) {
+            launch_split_tf32(ctx, X, X32.p, Xhi32.p, Xlo32.p, pl.N * R);
+            launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, Xhi32.p,
+                                 Xlo32.p, Y, R, tc_err.p);
+        } else {
+            launch_to_f32(ctx, X, X32.p, pl.N * R);
             launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
+        }
         if (has_far()) {
             M2LLevelFn<float> m2l_fn = [&](int level, int b0, int nb, double scale) {
                 if (tc32)
