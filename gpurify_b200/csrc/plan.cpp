@@ -225,6 +225,129 @@ void build_m2l_table(M2LTable& t, int n, int mode) {
     for (auto& x : th) x.join();
 }
 
+namespace {
+
+// Eigen-decomposition of a symmetric n x n matrix A (row-major, destroyed) by
+// cyclic Jacobi rotations: eigenvalues in w, eigenvectors in the columns of Q.
+void jacobi_eigen(std::vector<double>& A, int n, std::vector<double>& w, std::vector<double>& Q) {
+    Q.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) Q[(size_t)i * n + i] = 1.0;
+    double total = 0.0;
+    for (double x : A) total += x * x;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0;
+        for (int p = 0; p < n; ++p)
+            for (int q = p + 1; q < n; ++q) off += A[(size_t)p * n + q] * A[(size_t)p * n + q];
+        if (off <= 1e-30 * total) break;
+        for (int p = 0; p < n; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[(size_t)p * n + q];
+                if (std::fabs(apq) <= 1e-300) continue;
+                const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; ++k) {  // columns p, q
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - sn * akq;
+                    A[(size_t)k * n + q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {  // rows p, q
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - sn * aqk;
+                    A[(size_t)q * n + k] = sn * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double qkp = Q[(size_t)k * n + p], qkq = Q[(size_t)k * n + q];
+                    Q[(size_t)k * n + p] = c * qkp - sn * qkq;
+                    Q[(size_t)k * n + q] = sn * qkp + c * qkq;
+                }
+            }
+    }
+    w.resize(n);
+    for (int i = 0; i < n; ++i) w[i] = A[(size_t)i * n + i];
+}
+
+// The r leading eigenvectors (largest eigenvalues first) of the symmetric
+// n x n matrix S, as the columns of an n x r row-major matrix.
+std::vector<double> leading_eigenvectors(std::vector<double> S, int n, int r) {
+    std::vector<double> w, Q;
+    jacobi_eigen(S, n, w, Q);
+    std::vector<int> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return w[a] > w[b]; });
+    std::vector<double> B((size_t)n * r);
+    for (int j = 0; j < r; ++j)
+        for (int i = 0; i < n; ++i) B[(size_t)i * r + j] = Q[(size_t)i * n + idx[j]];
+    return B;
+}
+
+}  // namespace
+
+void build_shared_basis(const M2LTable& t, int r, SharedBasis& out) {
+    const int n3 = t.n * t.n * t.n;
+    out.n = t.n;
+    out.mode = t.mode;
+    out.r = r;
+    std::vector<int> slots;
+    for (int s = 0; s < 343; ++s)
+        if (t.rank[s] >= 0) slots.push_back(s);
+    // Gram sums of all offsets' operators
+    std::vector<double> SU((size_t)n3 * n3, 0.0), SV((size_t)n3 * n3, 0.0);
+    for (int s : slots) {
+        const double* K = &t.K[(size_t)s * n3 * n3];
+        for (int a = 0; a < n3; ++a)
+            for (int b = 0; b < n3; ++b) {
+                double u = 0.0, v = 0.0;
+                for (int k = 0; k < n3; ++k) {
+                    u += K[(size_t)a * n3 + k] * K[(size_t)b * n3 + k];
+                    v += K[(size_t)k * n3 + a] * K[(size_t)k * n3 + b];
+                }
+                SU[(size_t)a * n3 + b] += u;
+                SV[(size_t)a * n3 + b] += v;
+            }
+    }
+    out.U = leading_eigenvectors(SU, n3, r);
+    out.V = leading_eigenvectors(SV, n3, r);
+    out.C.assign((size_t)343 * r * r, 0.0);
+    double worst = 0.0;
+    std::vector<double> KV((size_t)n3 * r), UC((size_t)n3 * r);
+    for (int s : slots) {
+        const double* K = &t.K[(size_t)s * n3 * n3];
+        for (int a = 0; a < n3; ++a)
+            for (int j = 0; j < r; ++j) {
+                double acc = 0.0;
+                for (int k = 0; k < n3; ++k) acc += K[(size_t)a * n3 + k] * out.V[(size_t)k * r + j];
+                KV[(size_t)a * r + j] = acc;
+            }
+        double* C = &out.C[(size_t)s * r * r];
+        for (int i = 0; i < r; ++i)
+            for (int j = 0; j < r; ++j) {
+                double acc = 0.0;
+                for (int a = 0; a < n3; ++a) acc += out.U[(size_t)a * r + i] * KV[(size_t)a * r + j];
+                C[(size_t)i * r + j] = acc;
+            }
+        // relative Frobenius error of (U C) V^T against K
+        std::fill(UC.begin(), UC.end(), 0.0);
+        for (int a = 0; a < n3; ++a)
+            for (int i = 0; i < r; ++i) {
+                const double u = out.U[(size_t)a * r + i];
+                for (int j = 0; j < r; ++j) UC[(size_t)a * r + j] += u * C[(size_t)i * r + j];
+            }
+        double num = 0.0, den = 0.0;
+        for (int a = 0; a < n3; ++a)
+            for (int b = 0; b < n3; ++b) {
+                double acc = 0.0;
+                for (int j = 0; j < r; ++j) acc += UC[(size_t)a * r + j] * out.V[(size_t)b * r + j];
+                const double k = K[(size_t)a * n3 + b];
+                num += (k - acc) * (k - acc);
+                den += k * k;
+            }
+        worst = std::max(worst, std::sqrt(num / std::max(den, 1e-300)));
+    }
+    out.rel_err = worst;
+}
+
 void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, int ncond, int order, int depth) {
     p.n = order;
     p.n3 = order * order * order;

@@ -96,4 +96,19 @@ struct M2LTable {
 };
 void build_m2l_table(M2LTable& t, int n, int mode);
 
+// Shared-basis compression of a table's M2L operators (the mixed path's
+// far field): one target basis U and one source basis V (n3 x r each,
+// orthonormal columns) for every offset, K_o ~ U C_o V^T with the r x r
+// core C_o = U^T K_o V.  U spans the dominant r-dimensional range of all K_o
+// together (the leading eigenvectors of sum_o K_o K_o^T), V their dominant
+// row space (of sum_o K_o^T K_o).  Then M2L runs on compressed expansions:
+// E^ = V^T E per source box, L^ += C_o E^ per pair, L = U L^ per target box.
+struct SharedBasis {
+    int n = 0, mode = 0, r = 0;
+    std::vector<double> U, V;  // n3 x r, row-major
+    std::vector<double> C;     // 343 x r x r (zero for slots that are not M2L offsets)
+    double rel_err = 0.0;      // max over slots of ||K_o - U C_o V^T||_F / ||K_o||_F
+};
+void build_shared_basis(const M2LTable& t, int r, SharedBasis& out);
+
 }  // namespace gpx

@@ -37,6 +37,12 @@ struct DevM2L {
     int max_rank = 0;
     DBuf<float> K32;  // the same, rounded to TF32 (round to nearest, ties away), 343 x ns x ns, orders 4-5
     std::vector<int32_t> rank;
+    // Shared-basis compression (orders 5-6, built on first use): V padded to
+    // ns x kShared, U^T padded to kShared x round_up(ns, 64), and the cores
+    // C_o rounded to TF32, 343 x kShared x kShared.
+    bool shared_ok = false;
+    double shared_err = 0.0;
+    DBuf<float> Vpad32, Utpad32, C32;
 };
 
 namespace {
@@ -57,6 +63,55 @@ std::shared_ptr<const M2LTable> host_m2l(int n, int mode) {
     build_m2l_table(*t, n, mode);
     cache.push_back(t);
     return t;
+}
+
+// Host shared bases, built once per (order, mode) in the process.
+std::shared_ptr<const SharedBasis> host_shared(int n, int mode) {
+    static std::mutex mu;
+    static std::vector<std::shared_ptr<const SharedBasis>> cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& t : cache)
+            if (t->n == n && t->mode == mode) return t;
+    }
+    auto table = host_m2l(n, mode);
+    auto b = std::make_shared<SharedBasis>();
+    build_shared_basis(*table, kShared, *b);
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& t : cache)
+        if (t->n == n && t->mode == mode) return t;
+    cache.push_back(b);
+    return b;
+}
+
+float tf32_rna(double x) {
+    float f = (float)x;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// Device tables of the shared-basis M2L for a cached operator table.
+void ensure_shared(Ctx& ctx, DevM2L& d) {
+    if (d.shared_ok) return;
+    if (d.n < 5 || d.n > 6) throw Error(GPX_ERR_INVALID_ARG, "the shared-basis M2L runs orders 5 and 6");
+    auto b = host_shared(d.n, d.mode);
+    const int n3 = d.n * d.n * d.n, ns = node_stride(d.n), r = kShared, ldb = (ns + 63) / 64 * 64;
+    std::vector<float> vp((size_t)ns * r, 0.f), up((size_t)r * ldb, 0.f), c((size_t)343 * r * r, 0.f);
+    for (int l = 0; l < n3; ++l)
+        for (int k = 0; k < r; ++k) {
+            vp[(size_t)l * r + k] = (float)b->V[(size_t)l * r + k];
+            up[(size_t)k * ldb + l] = (float)b->U[(size_t)l * r + k];
+        }
+    for (size_t i = 0; i < c.size(); ++i) c[i] = tf32_rna(b->C[i]);
+    d.Vpad32.upload(vp, ctx.stream);
+    d.Utpad32.upload(up, ctx.stream);
+    d.C32.upload(c, ctx.stream);
+    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+    d.shared_err = b->rel_err;
+    d.shared_ok = true;
 }
 
 std::shared_ptr<DevM2L> get_m2l(Ctx& ctx, int n, int mode) {
@@ -382,6 +437,8 @@ struct Operator {
     BlockJacobi bj;
     bool factored = false;  // M2L through the low-rank factors (compressed operators)
     bool tc32 = false;      // mixed: FP32 M2L on the tensor cores (orders 4 and 5)
+    bool shared = false;    // mixed: M2L in the shared compressed basis on the tensor cores (orders 5, 6)
+    DBuf<float> Eh32, Lh32; // compressed expansions, nbox x Rb32 x kShared
     FacM2L<double> fac64;
     FacM2L<float> fac32;
     DBuf<int64_t> src_col_off, col_vt, tgt_col_off, tgt_ut, tgt_base;
@@ -534,7 +591,12 @@ struct Operator {
                     launch_to_f32(ctx, Sc.p, Sc32.p, pl.N * pl.n3);
                     w32 = FarWeights<float>{Sc32.p, false, W32.p, true};
                 }
-                if (tc32) build_tc_lists(ctx, pl, tc);
+                if (tc32 || shared) build_tc_lists(ctx, pl, tc);
+                if (shared) {
+                    ensure_shared(ctx, *const_cast<DevM2L*>(m2l));
+                    Eh32.alloc((size_t)pl.nbox() * Rb32 * kShared, s);
+                    Lh32.alloc((size_t)pl.nbox() * Rb32 * kShared, s);
+                }
             }
         }
     }
@@ -702,7 +764,17 @@ struct Operator {
         }
         if (has_far()) {
             M2LLevelFn<float> m2l_fn = [&](int level, int b0, int nb, double scale) {
-                if (tc32)
+                if (shared) {
+                    // E^ = V^T E, L^ = sum_o C_o E^ (tensor cores), L = U L^ for the boxes [b0, b0 + nb)
+                    const int ns = node_stride(pl.n);
+                    const int64_t row0 = (int64_t)b0 * Rb32, nrows = (int64_t)nb * Rb32;
+                    launch_m2l_compress(ctx, E32.p, ns, m2l->Vpad32.p, Eh32.p, row0, nrows);
+                    GPX_CUDA(cudaMemsetAsync(Lh32.p + row0 * kShared, 0, (size_t)nrows * kShared * sizeof(float),
+                                             ctx.stream));
+                    launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], kShared, Eh32.p, Lh32.p, m2l->C32.p,
+                                  Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
+                    launch_m2l_decompress(ctx, Lh32.p, m2l->Utpad32.p, ns, L32.p, row0, nrows);
+                } else if (tc32)
                     launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], node_stride(pl.n), E32.p, L32.p,
                                   m2l->K32.p, Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
                 else
@@ -725,8 +797,9 @@ struct Operator {
     // ready whenever the operators are compressed); drops captured graphs of
     // the FP32 apply.  Returns false when no factored form exists.
     bool drop_tc_m2l() {
-        if (!tc32 || !factored) return false;
+        if ((!tc32 && !shared) || !factored) return false;
         tc32 = false;
+        shared = false;
         for (auto& g : graphs)
             if (g.kind == 1) {
                 if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -960,7 +1033,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.order < 2 || o.order > 6) throw Error(GPX_ERR_INVALID_ARG, "Chebyshev order must be in [2, 6]");
     if (o.precision == GPX_PREC_MIXED && o.order < 4)
         throw Error(GPX_ERR_INVALID_ARG, "the mixed-precision path runs expansion orders 4 to 6");
-    if (o.precision == GPX_PREC_MIXED && o.m2l_mode == GPX_M2L_EXACT &&
+    if (o.precision == GPX_PREC_MIXED && o.m2l_mode == GPX_M2L_EXACT && o.mixed_m2l != 3 &&
         (o.mixed_m2l == 1 || o.order > 5 || (o.far_quad != 0 && o.mixed_m2l != 2)))
         throw Error(GPX_ERR_INVALID_ARG,
                     "the mixed-precision path runs exact M2L operators on the tensor cores, at orders 4 and 5 "
@@ -968,7 +1041,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
     if (o.precond < 0 || o.precond > 2) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0, 1 or 2");
     if (o.mixed_near != 0 && o.mixed_near != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0 or 1");
-    if (o.mixed_m2l < 0 || o.mixed_m2l > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1 or 2");
+    if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -999,8 +1072,10 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     // TF32 M2L only with centroid sources: with 2x2 Gauss sources the leaf
     // expansions carry large alternating node values (sources slightly outside
     // their leaf box) and the TF32 inputs lose 1e-2 of the far field.
-    pr.op->tc32 = o.precision == GPX_PREC_MIXED && o.mixed_m2l != 1 && (o.order == 4 || o.order == 5) &&
-                  (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT || o.mixed_m2l == 2);
+    pr.op->shared = o.precision == GPX_PREC_MIXED && o.mixed_m2l == 3 && (o.order == 5 || o.order == 6);
+    pr.op->tc32 = !pr.op->shared && o.precision == GPX_PREC_MIXED && o.mixed_m2l != 1 &&
+                  (o.order == 4 || o.order == 5) &&
+                  (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT || o.mixed_m2l >= 2);
     pr.op->assemble();
 }
 
@@ -1328,6 +1403,7 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
     opT.mixed_near = o.mixed_near;
     opT.use_graphs = o.graphs != 0;
     opT.tc32 = op.tc32;
+    opT.shared = op.shared;
     opT.assemble(&op);
     DBuf<double> Q, Lam;
     Q.alloc((size_t)n * R, s);

@@ -105,7 +105,10 @@ typedef struct {
     int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5 with centroid
                                 far-field sources, else the factored low-rank form on FP32 CUDA cores;
                                 1 -> always the factored form (compressed operators); 2 -> tensor cores
-                                at orders 4 and 5 also with Gauss-point sources */
+                                at orders 4 and 5 also with Gauss-point sources; 3 -> at orders 5 and 6
+                                the operators in one shared rank-64 basis (K_o ~ U C_o V^T): expansions
+                                compressed and decompressed in FP32, the 64 x 64 cores C_o on the tensor
+                                cores (order 4 as 2) */
     int32_t no_graphs;       /* 1: launch every operator apply directly instead of replaying it as a
                                 captured CUDA graph (results are identical) */
     int32_t batch_streams;   /* gpx_cap_solve_batched: windows solved concurrently, one stream each;

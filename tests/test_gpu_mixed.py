@@ -3,7 +3,8 @@ FP32 CUDA cores, mixed_near=1) and FP32 far field with the tcgen05 TF32 M2L,
 inside an FP64 iterative-refinement loop.
 
 Bars: the FP32/TF32 operator apply is within 1e-3 (norm-wise, per column) of the FP64
-operator (TF32 keeps 10 mantissa bits, rounded to nearest);
+operator (TF32 keeps 10 mantissa bits, rounded to nearest), also with the
+M2L in the shared rank-64 basis (mixed_m2l 3, orders 5 and 6);
 the refined Maxwell matrix is within 1e-6 of the plain FP64 solve, because
 the refinement residual is the FP64 operator's."""
 import numpy as np
@@ -44,7 +45,9 @@ def test_mixed_operator_close_to_fp64(ctx, nrhs, mixed_near):
 
 
 @pytest.mark.parametrize("order,m2l_mode,mixed_m2l,far_quad", [(4, 0, 0, 0), (4, 0, 0, 1), (4, 0, 1, 1), (5, 0, 0, 0),
-                                                               (5, 0, 0, 1), (5, 1, 0, 0), (6, 0, 0, 1)])
+                                                               (5, 0, 0, 1), (5, 1, 0, 0), (6, 0, 0, 1),
+                                                               (5, 0, 3, 0), (5, 0, 3, 1), (5, 1, 3, 1),
+                                                               (6, 0, 3, 1)])
 def test_mixed_operator_close_to_fp64_high_order(ctx, order, m2l_mode, mixed_m2l, far_quad):
     """FP32 far field with the M2L on the tensor cores (orders 4-5, centroid
     sources) or in the factored low-rank form on the CUDA cores, against the
@@ -68,13 +71,15 @@ def test_mixed_exact_m2l_needs_centroid_sources(ctx):
     assert ei.value.status == 1 and "far_quad 0" in ei.value.message
 
 
-@pytest.mark.parametrize("order,far_quad,mixed_near", [(4, 0, 0), (4, 1, 0), (4, 1, 1), (5, 1, 0)])
-def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near):
+@pytest.mark.parametrize("order,far_quad,mixed_near,mixed_m2l", [(4, 0, 0, 0), (4, 1, 0, 0), (4, 1, 1, 0),
+                                                                 (5, 1, 0, 0), (5, 1, 0, 3), (6, 1, 0, 3)])
+def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near, mixed_m2l):
     p = window()
     nc = len(p["nets"]) + 1
     kw = dict(order=order, max_level=5, dense_below=-1, far_quad=far_quad, skip_ground_rhs=1)
     C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=0, **kw)
-    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, mixed_near=mixed_near, **kw)
+    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, precision=1, mixed_near=mixed_near, mixed_m2l=mixed_m2l,
+                             **kw)
     assert r32["converged"] == 1 and r32["outer_iterations"] >= 1
     assert r32["max_rel_residual"] <= 1e-8
     R = nc - 1
