@@ -19,6 +19,7 @@
 // M2M; the reverse for L2L): 14 n^4 multiply-adds per parent and right-hand
 // side instead of 24 n^4.
 #include "farfield.cuh"
+#include "krylov.cuh"
 
 namespace gpx {
 
@@ -696,7 +697,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     const double wb = (double)sizeof(T);
     const double box_bytes = wb * N3 * R;
     const unsigned rchunks64 = cdiv(Rb, 64), rchunks_tree = cdiv(Rb, RC);
-    GPX_CUDA(cudaMemsetAsync(L, 0, (size_t)p.nbox * NS * Rb * sizeof(T), s));
+    launch_zero(c, L, (size_t)p.nbox * NS * Rb * sizeof(T));  // a kernel: also valid inside a device-side loop
     {
         KTimer t(c, prec_tag<T>(K_P2M), (double)p.N * (wb * R + wb * N3 + 8.0) + (p.nleaf + 2.0 * f.npart) * box_bytes,
                  2.0 * (double)p.N * N3 * R);

@@ -102,6 +102,21 @@ struct DBuf {
 
 struct DevM2L;  // device M2L operator table, cached per (order, mode)
 
+// An iteration index held in device memory, for kernels replayed by a
+// device-side loop: the kernel reads k = *k at run time and offsets a vector
+// pointer by (k + add) * stride.  k == nullptr: no offset (host-known index).
+struct DevIndex {
+    const int32_t* k = nullptr;
+    int64_t stride = 0;
+    int add = 0;
+};
+#ifdef __CUDACC__
+template <class T>
+__device__ __forceinline__ T* dev_offset(T* p, const DevIndex& di) {
+    return di.k ? p + (int64_t)(*di.k + di.add) * di.stride : p;
+}
+#endif
+
 // Kernel classes timed by the optional per-kernel event timer.
 // The operator's kernel classes are split by precision: the plain names hold
 // the FP32 / TF32 launches of the mixed path's inner operator, the *64 names
@@ -132,6 +147,9 @@ struct Ctx {
     std::vector<std::shared_ptr<DevM2L>> m2l_cache;
     // per-kernel timing (enabled by gpx_ctx_set_profiling)
     bool profile = false;
+    // true while a device-side GMRES loop is being captured: operator applies
+    // launch their kernels into the capture instead of replaying their own graphs
+    bool capturing = false;
     KStats kstats[K_NTAGS];
     struct Pending {
         int tag;

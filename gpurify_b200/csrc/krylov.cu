@@ -18,9 +18,11 @@ constexpr int kRedThreads = 256;
 // and each thread keeps four independent loads in flight per row.  Each
 // partial sums the same rows in the same order as a one-vector pass.
 __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restrict__ A, int64_t strideA, int ni,
+                                                          const int32_t* __restrict__ kdev,
                                                           const double* __restrict__ B, int64_t N, int R,
                                                           double* __restrict__ partial) {
     constexpr int kV = 4;
+    if (kdev) ni = *kdev + 1;
     const int nsub = kRedThreads / R;
     const int r = threadIdx.x % R, sub = threadIdx.x / R;
     const int64_t per = (N + gridDim.x - 1) / gridDim.x;
@@ -62,8 +64,9 @@ __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restri
 
 // out[i][r] (+)= sum_b partial[b][i][r]; one warp per (i, r): lane l sums
 // blocks l, l + 32, ... and the lanes combine in a fixed shuffle tree.
-__global__ void k_reduce_blocks(const double* __restrict__ partial, int nblk, int ni, int R, double* __restrict__ out,
-                                int accumulate) {
+__global__ void k_reduce_blocks(const double* __restrict__ partial, int nblk, int ni, const int32_t* __restrict__ kdev,
+                                int R, double* __restrict__ out, int accumulate) {
+    if (kdev) ni = *kdev + 1;
     const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (o >= ni * R) return;
     const int64_t stride = (int64_t)ni * R;
@@ -75,8 +78,9 @@ __global__ void k_reduce_blocks(const double* __restrict__ partial, int nblk, in
 }
 
 // W[n][r] -= sum_{i<ni} h[i][r] * V_i[n][r]
-__global__ void k_multi_axpy(const double* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ h,
-                             double* __restrict__ W, int64_t N, int R) {
+__global__ void k_multi_axpy(const double* __restrict__ V, int64_t strideV, int ni, const int32_t* __restrict__ kdev,
+                             const double* __restrict__ h, double* __restrict__ W, int64_t N, int R) {
+    if (kdev) ni = *kdev + 1;
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
     const int r = (int)(o % R);
@@ -88,9 +92,10 @@ __global__ void k_multi_axpy(const double* __restrict__ V, int64_t strideV, int 
 // dst[n][r] = src[n][r] / s[r] when s[r] > thresh, else src (Arnoldi
 // normalisation with the reference's happy-breakdown rule, krylov.rs:111-115).
 __global__ void k_scale_cols(const double* __restrict__ src, const double* __restrict__ s, double thresh,
-                             double* __restrict__ dst, int64_t N, int R) {
+                             double* __restrict__ dst, DevIndex di, int64_t N, int R) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
+    dst = dev_offset(dst, di);
     const double d = s[o % R];
     dst[o] = d > thresh ? src[o] / d : src[o];
 }
@@ -101,10 +106,11 @@ __global__ void k_sqrt(double* v, int n) {
 }
 
 // Z[n][r] (+)= inv_diag[n] * V[n][r]
-__global__ void k_diag_scale(const double* __restrict__ V, const double* __restrict__ d, double* __restrict__ Z,
-                             int64_t N, int R, int add) {
+__global__ void k_diag_scale(const double* __restrict__ V, DevIndex di, const double* __restrict__ d,
+                             double* __restrict__ Z, int64_t N, int R, int add) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
+    V = dev_offset(V, di);
     const double z = V[o] * d[o / R];
     Z[o] = add ? Z[o] + z : z;
 }
@@ -147,9 +153,10 @@ __global__ void k_zero_cols(double* __restrict__ V, const int32_t* __restrict__ 
 
 // Per-column Hessenberg column k update, Givens rotation (krylov.rs:118-142,
 // :195-207), residual estimate and freeze of converged columns.
-__global__ void k_givens(GmresDev g, int k) {
+__global__ void k_givens(GmresDev g, int k, const int32_t* __restrict__ kdev) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= g.R) return;
+    if (kdev) k = *kdev;
     const int m = g.m, R = g.R;
     if (!g.act[r]) return;
     double* H = g.H;  // H[(i*m + k)*R + r]
@@ -244,6 +251,32 @@ __global__ void k_count_active(const int32_t* act, int R, int32_t* out) {
     if (threadIdx.x == 0) *out = red[0];
 }
 
+// Control of the device-side Arnoldi loop (one CTA of 256 threads): with
+// `advance`, one more iteration has completed (*kdev += 1); the loop goes on
+// while a column is still active and fewer than m iterations ran.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int32_t* __restrict__ act, int R,
+                           int32_t* __restrict__ kdev, int m, int advance) {
+    int c = 0;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) c += act[r] != 0;
+    __shared__ int red[256];
+    red[threadIdx.x] = c;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int k = *kdev + (advance ? 1 : 0);
+        *kdev = k;
+        cudaGraphSetConditional(h, (red[0] > 0 && k < m) ? 1u : 0u);
+    }
+}
+
+__global__ void k_zero_words(float4* __restrict__ p, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -251,15 +284,17 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 int reduce_blocks_for(int64_t N) { return (int)std::min<int64_t>(296, std::max<int64_t>(1, N / 64)); }
 
 void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
-                     double* partial, int nblk, double* out, int accumulate, int tag) {
+                     double* partial, int nblk, double* out, int accumulate, int tag, const int32_t* kdev) {
+    // with kdev the vector count is *kdev + 1 <= ni, read on the device
     {
         KTimer t(c, tag, 8.0 * (ni + 1) * (double)N * R, 2.0 * ni * (double)N * R);
-        k_multidot<<<nblk, kRedThreads, 0, c.stream>>>(A, strideA, ni, B, N, R, partial);
+        k_multidot<<<nblk, kRedThreads, 0, c.stream>>>(A, strideA, ni, kdev, B, N, R, partial);
         GPX_LAUNCH_CHECK();
     }
     {
         KTimer t(c, K_SMALL);
-        k_reduce_blocks<<<blocks_for((int64_t)ni * R, 8), 256, 0, c.stream>>>(partial, nblk, ni, R, out, accumulate);
+        k_reduce_blocks<<<blocks_for((int64_t)ni * R, 8), 256, 0, c.stream>>>(partial, nblk, ni, kdev, R, out,
+                                                                              accumulate);
         GPX_LAUNCH_CHECK();
     }
     c.launches += 2;
@@ -273,16 +308,18 @@ void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, 
     c.launches += 1;
 }
 
-void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R) {
+void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
+                      const int32_t* kdev) {
     KTimer t(c, K_GS_AXPY, 8.0 * (ni + 2) * (double)N * R, 2.0 * ni * (double)N * R);
-    k_multi_axpy<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, h, W, N, R);
+    k_multi_axpy<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, kdev, h, W, N, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
 
-void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R) {
+void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R,
+                       const DevIndex& di) {
     KTimer t(c, K_VEC, 16.0 * (double)N * R, (double)N * R);
-    k_scale_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(src, sc, thresh, dst, N, R);
+    k_scale_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(src, sc, thresh, dst, di, N, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
@@ -295,9 +332,10 @@ void launch_lincomb(Ctx& c, const double* V, int64_t strideV, int ni, const doub
     c.launches += 1;
 }
 
-void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add) {
+void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add,
+                       const DevIndex& di) {
     KTimer t(c, K_VEC, 16.0 * (double)N * R + 8.0 * N, (double)N * R);
-    k_diag_scale<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, d, Z, N, R, add ? 1 : 0);
+    k_diag_scale<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, di, d, Z, N, R, add ? 1 : 0);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
@@ -331,9 +369,9 @@ void launch_zero_cols(Ctx& c, double* V, const int32_t* mask, int64_t N, int R) 
     c.launches += 1;
 }
 
-void launch_givens(Ctx& c, const GmresDev& g, int k) {
+void launch_givens(Ctx& c, const GmresDev& g, int k, const int32_t* kdev) {
     KTimer t(c, K_SMALL);
-    k_givens<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g, k);
+    k_givens<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g, k, kdev);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
@@ -355,6 +393,26 @@ void launch_cycle_start(Ctx& c, const GmresDev& g, const double* beta) {
 void launch_cycle_end(Ctx& c, const GmresDev& g, const double* rnorm) {
     KTimer t(c, K_SMALL);
     k_cycle_end<<<blocks_for(g.R, 64), 64, 0, c.stream>>>(g, rnorm);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_loop_ctl(Ctx& c, cudaGraphConditionalHandle h, const int32_t* act, int R, int32_t* kdev, int m,
+                     bool advance) {
+    KTimer t(c, K_SMALL);
+    k_loop_ctl<<<1, 256, 0, c.stream>>>(h, act, R, kdev, m, advance ? 1 : 0);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_zero(Ctx& c, void* p, size_t bytes) {
+    if (bytes == 0) return;
+    if (bytes % 16 != 0 || reinterpret_cast<uintptr_t>(p) % 16 != 0)
+        throw Error(GPX_ERR_INTERNAL, "launch_zero needs 16-byte aligned, 16-byte multiple buffers");
+    const int64_t n = (int64_t)(bytes / 16);
+    KTimer t(c, K_VEC, (double)bytes, 0.0);
+    k_zero_words<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c.stream>>>(
+        reinterpret_cast<float4*>(p), n);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }

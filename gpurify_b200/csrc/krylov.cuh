@@ -30,12 +30,19 @@ struct GmresDev {
 };
 
 int reduce_blocks_for(int64_t N);
+// Kernels of one Arnoldi step take the step index k either from the host or,
+// for the device-side loop, from device memory (kdev / DevIndex; host
+// arguments then give the launch sizes for the largest k).
 void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
-                     double* partial, int nblk, double* out, int accumulate, int tag = K_GS_DOT);
+                     double* partial, int nblk, double* out, int accumulate, int tag = K_GS_DOT,
+                     const int32_t* kdev = nullptr);
 void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, int nblk, double* out);
-void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R);
-void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R);
-void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add = false);
+void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
+                       const int32_t* kdev = nullptr);
+void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R,
+                       const DevIndex& di = DevIndex());
+void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add = false,
+                       const DevIndex& di = DevIndex());
 void launch_lincomb(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, double* out, int64_t N,
                     int R);
 void launch_residual(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const double* AX, double* Res, int64_t N,
@@ -43,7 +50,13 @@ void launch_residual(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const
 void launch_sub(Ctx& c, const double* B, const double* AX, double* Res, int64_t n);
 void launch_add(Ctx& c, double* X, const double* D, int64_t n);
 void launch_zero_cols(Ctx& c, double* V, const int32_t* mask, int64_t N, int R);
-void launch_givens(Ctx& c, const GmresDev& g, int k);
+void launch_givens(Ctx& c, const GmresDev& g, int k, const int32_t* kdev = nullptr);
+// Device-side loop control: counts the active columns, advances *kdev when
+// `advance`, and sets the loop's condition (active columns left and *kdev < m).
+void launch_loop_ctl(Ctx& c, cudaGraphConditionalHandle h, const int32_t* act, int R, int32_t* kdev, int m,
+                     bool advance);
+// Zero `bytes` (a multiple of 16, 16-byte aligned) with a kernel.
+void launch_zero(Ctx& c, void* p, size_t bytes);
 void launch_trisolve(Ctx& c, const GmresDev& g);
 void launch_cycle_start(Ctx& c, const GmresDev& g, const double* beta);
 void launch_cycle_end(Ctx& c, const GmresDev& g, const double* rnorm);

@@ -92,8 +92,9 @@ template <int kB>
 __global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ Minv,
                                                      const int64_t* __restrict__ blk_start,
                                                      const int32_t* __restrict__ blk_size, const double* __restrict__ V,
-                                                     double* __restrict__ Z, int R, int add) {
+                                                     DevIndex di, double* __restrict__ Z, int R, int add) {
     constexpr int RA = kB / 16;
+    V = dev_offset(V, di);
     const int bi = blockIdx.x;
     const int rc = blockIdx.y * 64;
     const int64_t s0 = blk_start[bi];
@@ -181,17 +182,17 @@ void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double*
     if (sing) throw Error(GPX_ERR_CAPACITANCE, "singular near-field block in the block-Jacobi preconditioner");
 }
 
-void BlockJacobi::apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add) const {
+void BlockJacobi::apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add, const DevIndex& di) const {
     const int kB = block;
     KTimer t(c, K_VEC, 8.0 * (2.0 * N * R + (double)nblk * kB * kB), 2.0 * (double)N * kB * R);
     const int smem = (int)(sizeof(double) * (kB * (kB + 1) + kB * 65));
     const dim3 g(nblk, (R + 63) / 64);
     if (kB == 96) {
         set_smem_once(k_block_apply<96>, smem);
-        k_block_apply<96><<<g, 256, smem, c.stream>>>(Minv.p, d_start.p, d_size.p, V, Z, R, add ? 1 : 0);
+        k_block_apply<96><<<g, 256, smem, c.stream>>>(Minv.p, d_start.p, d_size.p, V, di, Z, R, add ? 1 : 0);
     } else {
         set_smem_once(k_block_apply<48>, smem);
-        k_block_apply<48><<<g, 256, smem, c.stream>>>(Minv.p, d_start.p, d_size.p, V, Z, R, add ? 1 : 0);
+        k_block_apply<48><<<g, 256, smem, c.stream>>>(Minv.p, d_start.p, d_size.p, V, di, Z, R, add ? 1 : 0);
     }
     GPX_LAUNCH_CHECK();
     c.launches += 1;

@@ -15,7 +15,8 @@ struct BlockJacobi {
     DBuf<double> Minv;
     void build(Ctx& c, const Plan& pl, const DevPlan& dp, const double* P);
     // Z = M^-1 V (or Z += M^-1 V), V and Z N x R row-major.
-    void apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add) const;
+    void apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add,
+               const DevIndex& di = DevIndex()) const;
 };
 
 }  // namespace gpx

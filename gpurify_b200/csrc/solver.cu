@@ -465,7 +465,7 @@ struct Operator {
 
     template <class F>
     void run_captured(int kind, const void* x, void* y, F&& body) {
-        if (!use_graphs || ctx.profile) {
+        if (!use_graphs || ctx.profile || ctx.capturing) {
             body();
             return;
         }
@@ -769,8 +769,7 @@ struct Operator {
                     const int ns = node_stride(pl.n);
                     const int64_t row0 = (int64_t)b0 * Rb32, nrows = (int64_t)nb * Rb32;
                     launch_m2l_compress(ctx, E32.p, ns, m2l->Vpad32.p, Eh32.p, row0, nrows);
-                    GPX_CUDA(cudaMemsetAsync(Lh32.p + row0 * kShared, 0, (size_t)nrows * kShared * sizeof(float),
-                                             ctx.stream));
+                    launch_zero(ctx, Lh32.p + row0 * kShared, (size_t)nrows * kShared * sizeof(float));
                     launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], kShared, Eh32.p, Lh32.p, m2l->C32.p,
                                   Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
                     launch_m2l_decompress(ctx, Lh32.p, m2l->Utpad32.p, ns, L32.p, row0, nrows);
@@ -785,12 +784,13 @@ struct Operator {
         }
     }
 
-    // Z (+)= M^-1 V with the chosen right preconditioner.
-    void precondition(const double* V, double* Z, bool add) {
+    // Z (+)= M^-1 V with the chosen right preconditioner (V offset on the
+    // device by di when given).
+    void precondition(const double* V, double* Z, bool add, const DevIndex& di = DevIndex()) {
         if (precond >= 1)
-            bj.apply(ctx, V, Z, pl.N, R, add);
+            bj.apply(ctx, V, Z, pl.N, R, add, di);
         else
-            launch_diag_scale(ctx, V, inv_diag.p, Z, pl.N, R, add);
+            launch_diag_scale(ctx, V, inv_diag.p, Z, pl.N, R, add, di);
     }
 
     // Switch the FP32 M2L from the tensor cores to the factored form (kept
@@ -852,22 +852,41 @@ struct SolveStats {
 };
 
 using ApplyFn = std::function<void(const double*, double*)>;
-using PrecondFn = std::function<void(const double*, double*, bool)>;
+using PrecondFn = std::function<void(const double*, double*, bool, const DevIndex&)>;
+
+// The device-side Arnoldi loop of one gmres_multi call: a CUDA graph whose
+// first node evaluates the loop condition and whose conditional WHILE node
+// runs one Arnoldi step per pass (operator apply, Gram-Schmidt, Givens) and
+// then advances the step counter on the device.  The loop ends when every
+// column has converged or the restart length is reached, so a cycle needs no
+// host round trip per step.
+struct ArnoldiGraph {
+    cudaGraphExec_t exec = nullptr;
+    ArnoldiGraph() = default;
+    ArnoldiGraph(const ArnoldiGraph&) = delete;
+    ArnoldiGraph& operator=(const ArnoldiGraph&) = delete;
+    ~ArnoldiGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
 
 // Restarted right-preconditioned GMRES(m) on all R columns at once
 // (krylov.rs:50-191 per column); X (N x R) receives the solution.  The
 // right-hand sides are B (N x R) when given, else the unit-conductor vectors
-// of rhs_cond (cap/solver.rs:55-63).
+// of rhs_cond (cap/solver.rs:55-63).  With device_loop the Arnoldi steps of a
+// cycle run as one graph launch (ArnoldiGraph; the first step of the call
+// runs directly, which also does the kernels' one-time set-up); otherwise
+// the host launches each step and reads the active-column count after it.
 void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_t* d_cond,
                  const int32_t* d_rhs_cond, const double* B, int R, int64_t N, double tol, int m, int max_restarts,
-                 DBuf<double>& X, SolveStats& st, bool reorth = true) {
+                 DBuf<double>& X, SolveStats& st, bool reorth = true, bool device_loop = false) {
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
     // Krylov basis within a memory budget (16 GB per solve), restart >= 20
     constexpr double kBasisBudget = 16.0 * (1ull << 30);
     m = (int)std::max<int64_t>(std::min<int64_t>(20, m), std::min<int64_t>(m, (int64_t)(kBasisBudget / (8.0 * NR)) - 1));
     DBuf<double> V, W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
-    DBuf<int32_t> act, done, kused, cnt;
+    DBuf<int32_t> act, done, kused, cnt, kdev;
     V.alloc((size_t)(m + 1) * NR, s);
     W.alloc(NR, s);
     Z.alloc(NR, s);
@@ -879,11 +898,13 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
     y.alloc((size_t)m * R, s);
     h1.alloc((size_t)(m + 1) * R, s);
     h2.alloc((size_t)(m + 1) * R, s);
+    h2.zero();  // stays zero without the re-orthogonalisation pass
     for (auto* b : {&hnorm, &bnorm, &bcur, &est, &resid, &beta}) b->alloc(R, s);
     act.alloc(R, s);
     done.alloc(R, s);
     kused.alloc(R, s);
     cnt.alloc(1, s);
+    kdev.alloc(1, s);
     const int nblk = reduce_blocks_for(N);
     partial.alloc((size_t)nblk * (m + 1) * R, s);
     X.alloc(NR, s);
@@ -892,8 +913,10 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
     kused.zero();
     GmresDev gd{m, R, tol, H.p, cs.p, sn.p, g.p, y.p, h1.p, h2.p, hnorm.p, bnorm.p, bcur.p, est.p, resid.p,
                 act.p, done.p, kused.p};
+    // pinned host words: [0] active-column count, [1] loop step counter read
+    // back, [2] loop step counter to start from
     int32_t* hcount = nullptr;
-    GPX_CUDA(cudaMallocHost((void**)&hcount, sizeof(int32_t)));
+    GPX_CUDA(cudaMallocHost((void**)&hcount, 4 * sizeof(int32_t)));
     struct HostFree {
         int32_t* p;
         ~HostFree() { cudaFreeHost(p); }
@@ -903,6 +926,76 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
         GPX_CUDA(cudaMemcpyAsync(hcount, cnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         GPX_CUDA(cudaStreamSynchronize(s));
         return count_zero ? R - *hcount : *hcount;
+    };
+    // One Arnoldi step: k from the host, or (kd) from device memory.
+    auto step = [&](int k, const int32_t* kd) {
+        const DevIndex dk{kd, NR, 0}, dk1{kd, NR, 1};
+        Minv(kd ? V.p : V.p + (int64_t)k * NR, Z.p, false, dk);
+        A(Z.p, W.p);
+        const int ni = kd ? m : k + 1;  // launch sizes cover the largest k
+        launch_multidot(ctx, V.p, NR, ni, W.p, N, R, partial.p, nblk, h1.p, 0, K_GS_DOT, kd);
+        launch_multi_axpy(ctx, V.p, NR, ni, h1.p, W.p, N, R, kd);
+        if (reorth) {
+            launch_multidot(ctx, V.p, NR, ni, W.p, N, R, partial.p, nblk, h2.p, 0, K_GS_DOT, kd);
+            launch_multi_axpy(ctx, V.p, NR, ni, h2.p, W.p, N, R, kd);
+        }
+        launch_colnorm(ctx, W.p, N, R, partial.p, nblk, hnorm.p);
+        launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, kd ? V.p : V.p + (int64_t)(k + 1) * NR, N, R, dk1);
+        launch_givens(ctx, gd, k, kd);
+    };
+    ArnoldiGraph loop;
+    int64_t step_launches = 0;  // kernels of one pass of the loop body
+    auto build_loop = [&] {
+        cudaGraph_t gr = nullptr;
+        GPX_CUDA(cudaGraphCreate(&gr, 0));
+        struct GraphFree {
+            cudaGraph_t g;
+            ~GraphFree() {
+                if (g) cudaGraphDestroy(g);
+            }
+        } gf{gr};
+        cudaGraphConditionalHandle h;
+        GPX_CUDA(cudaGraphConditionalHandleCreate(&h, gr, 0, cudaGraphCondAssignDefault));
+        GPX_CUDA(cudaStreamBeginCaptureToGraph(s, gr, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        try {
+            launch_loop_ctl(ctx, h, act.p, R, kdev.p, m, false);
+        } catch (...) {
+            cudaGraph_t dummy;
+            cudaStreamEndCapture(s, &dummy);
+            throw;
+        }
+        GPX_CUDA(cudaStreamEndCapture(s, &gr));
+        size_t nn = 0;
+        GPX_CUDA(cudaGraphGetNodes(gr, nullptr, &nn));
+        std::vector<cudaGraphNode_t> deps(nn);
+        GPX_CUDA(cudaGraphGetNodes(gr, deps.data(), &nn));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t wn;
+        GPX_CUDA(cudaGraphAddNode(&wn, gr, deps.data(), nn, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        const int64_t l0 = ctx.launches;
+        ctx.capturing = true;
+        GPX_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        try {
+            step(0, kdev.p);
+            launch_loop_ctl(ctx, h, act.p, R, kdev.p, m, true);
+        } catch (...) {
+            ctx.capturing = false;
+            cudaGraph_t dummy;
+            cudaStreamEndCapture(s, &dummy);
+            throw;
+        }
+        ctx.capturing = false;
+        GPX_CUDA(cudaStreamEndCapture(s, &body));
+        ctx.launches = l0;  // captured, not launched
+        GPX_CUDA(cudaGraphInstantiate(&loop.exec, gr, 0));
+        size_t bn = 0;
+        GPX_CUDA(cudaGraphGetNodes(body, nullptr, &bn));
+        step_launches = (int64_t)bn;
     };
     // ||b|| (krylov.rs:58, clamped to the smallest positive normal)
     if (B)
@@ -924,28 +1017,34 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
         launch_scale_cols(ctx, Res.p, beta.p, 0.0, V.p, N, R);
         if (read_count(act.p, false) == 0) break;
         int kmax = 0;
-        for (int k = 0; k < m; ++k) {
-            const double* Vk = V.p + (int64_t)k * NR;
-            Minv(Vk, Z.p, false);
-            A(Z.p, W.p);
-            launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h1.p, 0);
-            launch_multi_axpy(ctx, V.p, NR, k + 1, h1.p, W.p, N, R);
-            if (reorth) {
-                launch_multidot(ctx, V.p, NR, k + 1, W.p, N, R, partial.p, nblk, h2.p, 0);
-                launch_multi_axpy(ctx, V.p, NR, k + 1, h2.p, W.p, N, R);
-            } else if (k == 0) {
-                GPX_CUDA(cudaMemsetAsync(h2.p, 0, (size_t)(m + 1) * R * sizeof(double), s));
-            }
-            launch_colnorm(ctx, W.p, N, R, partial.p, nblk, hnorm.p);
-            launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, V.p + (int64_t)(k + 1) * NR, N, R);
-            launch_givens(ctx, gd, k);
+        if (device_loop && !loop.exec) {
+            // first step of the call directly, then the loop graph
+            step(0, nullptr);
             st.iterations += 1;
-            kmax = k + 1;
-            if (read_count(act.p, false) == 0) break;
+            kmax = 1;
+            if (m > 1 && read_count(act.p, false) > 0) build_loop();
+        }
+        if (device_loop && loop.exec && kmax < m) {
+            hcount[2] = kmax;
+            GPX_CUDA(cudaMemcpyAsync(kdev.p, hcount + 2, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+            GPX_CUDA(cudaGraphLaunch(loop.exec, s));
+            GPX_CUDA(cudaMemcpyAsync(hcount + 1, kdev.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            GPX_CUDA(cudaStreamSynchronize(s));
+            const int k1 = hcount[1];
+            ctx.launches += (int64_t)(k1 - kmax) * step_launches + 1;
+            st.iterations += k1 - kmax;
+            kmax = k1;
+        } else if (!device_loop) {
+            for (int k = 0; k < m; ++k) {
+                step(k, nullptr);
+                st.iterations += 1;
+                kmax = k + 1;
+                if (read_count(act.p, false) == 0) break;
+            }
         }
         launch_trisolve(ctx, gd);
         launch_lincomb(ctx, V.p, NR, kmax, y.p, Z.p, N, R);
-        Minv(Z.p, X.p, true);  // x += M^-1 (V y)  (krylov.rs:154-168)
+        Minv(Z.p, X.p, true, DevIndex());  // x += M^-1 (V y)  (krylov.rs:154-168)
         A(X.p, W.p);
         if (B)
             launch_sub(ctx, B, W.p, Res.p, NR);
@@ -1144,9 +1243,11 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         SolveStats in;
         // Inner solves stop at 1e-3..1e-5: one classical Gram-Schmidt pass (FP64) keeps the
         // basis orthogonal far below that, so the re-orthogonalisation pass is skipped.
-        const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
+        const PrecondFn pc = [&](const double* v, double* z, bool add, const DevIndex& di) {
+            op.precondition(v, z, add, di);
+        };
         gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, std::min(o.max_restarts, 3), D, in,
-                    false);
+                    false, o.graphs != 0 && !ctx.profile);
         st.iterations += in.iterations;
         launch_add(ctx, X.p, D.p, NR);
         op.apply(X.p, W.p);
@@ -1173,8 +1274,11 @@ void solve_columns(Ctx& ctx, Operator& op, const Opts& o, bool dense, const int3
         mixed_solve(ctx, op, d_cond, d_rhs, B, R, n, oi, X, st, outer);
     } else {
         const ApplyFn a64 = [&](const double* x, double* y) { op.apply(x, y); };
-        const PrecondFn pc = [&](const double* v, double* z, bool add) { op.precondition(v, z, add); };
-        gmres_multi(ctx, a64, pc, d_cond, d_rhs, B, R, n, tol, o.restart, o.max_restarts, X, st);
+        const PrecondFn pc = [&](const double* v, double* z, bool add, const DevIndex& di) {
+            op.precondition(v, z, add, di);
+        };
+        gmres_multi(ctx, a64, pc, d_cond, d_rhs, B, R, n, tol, o.restart, o.max_restarts, X, st, true,
+                    o.graphs != 0 && !ctx.profile);
     }
 }
 
