@@ -176,6 +176,9 @@ void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double*
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
+}
+
+void BlockJacobi::check(Ctx& c) const {
     int sing = 0;
     d_sing.download(&sing, 1);
     GPX_CUDA(cudaStreamSynchronize(c.stream));

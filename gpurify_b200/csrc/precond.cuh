@@ -13,7 +13,10 @@ struct BlockJacobi {
     DBuf<int32_t> d_leaf, d_row0, d_size, d_sing;
     DBuf<int64_t> d_start;
     DBuf<double> Minv;
+    // Inverts the blocks on the device (no host wait); check() then waits for
+    // the stream and fails if a block was singular.
     void build(Ctx& c, const Plan& pl, const DevPlan& dp, const double* P);
+    void check(Ctx& c) const;
     // Z = M^-1 V (or Z += M^-1 V), V and Z N x R row-major.
     void apply(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add,
                const DevIndex& di = DevIndex()) const;

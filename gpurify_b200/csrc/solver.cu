@@ -535,12 +535,27 @@ struct Operator {
             bj.block = precond == 2 ? 96 : 48;
             bj.build(ctx, pl, d.v, P.p);
         }
-        GPX_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        GPX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        t_assembly_s = ms * 1e-3;
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        // The host-side set-up below (far-field lists) runs while the device
+        // assembles; the assembly time and the preconditioner check are read
+        // at the end.
+        struct Finish {
+            Operator& op;
+            cudaEvent_t a, b;
+            bool done = false;
+            void operator()() {
+                GPX_CUDA(cudaEventSynchronize(b));
+                float ms = 0.f;
+                GPX_CUDA(cudaEventElapsedTime(&ms, a, b));
+                op.t_assembly_s = ms * 1e-3;
+                if (op.precond >= 1) op.bj.check(op.ctx);
+                done = true;
+            }
+            ~Finish() {
+                if (!done) cudaEventSynchronize(b);
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } finish{*this, e0, e1};
         if (has_far()) {
             const int ns = node_stride(pl.n);
             if (!transposed) {
@@ -599,6 +614,7 @@ struct Operator {
                 }
             }
         }
+        finish();
     }
 
     // Column lists of the factored M2L: phase 1 per source box, phase 2 per
@@ -606,9 +622,7 @@ struct Operator {
     void setup_factored() {
         const int64_t np = pl.m2l_pairs(), nb = pl.nbox();
         const int ns = node_stride(pl.n);
-        std::vector<int32_t> rank(343);
-        m2l->d_rank.download(rank.data(), 343);
-        GPX_CUDA(cudaStreamSynchronize(ctx.stream));
+        const std::vector<int32_t>& rank = m2l->rank;  // host copy: no device round trip
         std::vector<int64_t> tcol(nb + 1, 0), base(nb, 0), pos_of_pair(np);
         std::vector<int32_t> tgt_of_pair(np);
         int64_t acc = 0;
