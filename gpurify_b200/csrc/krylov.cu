@@ -14,14 +14,14 @@ namespace {
 constexpr int kRedThreads = 256;
 
 // partial[b][i][r] = sum over rows of block b of A_i[n][r] * B[n][r].
-// Four vectors A_i per pass over the block's rows: B is read once per four,
-// and each thread keeps four independent loads in flight per row.  Each
+// Eight vectors A_i per pass over the block's rows: B is read once per eight,
+// and each thread keeps eight independent loads in flight per row.  Each
 // partial sums the same rows in the same order as a one-vector pass.
 __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restrict__ A, int64_t strideA, int ni,
                                                           const int32_t* __restrict__ kdev,
                                                           const double* __restrict__ B, int64_t N, int R,
                                                           double* __restrict__ partial) {
-    constexpr int kV = 4;
+    constexpr int kV = 8;
     if (kdev) ni = *kdev + 1;
     const int nsub = kRedThreads / R;
     const int r = threadIdx.x % R, sub = threadIdx.x / R;
@@ -31,7 +31,9 @@ __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restri
     for (int i0 = 0; i0 < ni; i0 += kV) {
         const int nv = min(kV, ni - i0);
         const double* A0 = A + i0 * strideA;
-        double acc[kV] = {0.0, 0.0, 0.0, 0.0};
+        double acc[kV];
+#pragma unroll
+        for (int q = 0; q < kV; ++q) acc[q] = 0.0;
         if (sub < nsub) {
             if (nv == kV) {
 #pragma unroll 2
@@ -281,7 +283,7 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 
 }  // namespace
 
-int reduce_blocks_for(int64_t N) { return (int)std::min<int64_t>(296, std::max<int64_t>(1, N / 64)); }
+int reduce_blocks_for(int64_t N) { return (int)std::min<int64_t>(592, std::max<int64_t>(1, N / 64)); }
 
 void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
                      double* partial, int nblk, double* out, int accumulate, int tag, const int32_t* kdev) {
