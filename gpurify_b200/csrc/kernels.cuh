@@ -105,9 +105,11 @@ void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n);
 // work items of <= 128 rows (it_leaf, it_row0); P holds TF32-rounded values;
 // X is given as its TF32 split Xhi + Xlo (launch_split_tf32); R a multiple
 // of 4.  *err becomes nonzero if a bounded pipeline wait expired.
+// split_p: P holds full FP32 values and is split into TF32 hi and lo parts on
+// chip (three products instead of two; accurate to about 2^-21 in P too).
 void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, const int32_t* it_leaf,
                           const int32_t* it_row0, const float* P, const float* Xhi, const float* Xlo, double* Y, int R,
-                          int* err);
+                          int* err, bool split_p = false);
 // X32 = (float) X, and its TF32 split Xhi = tf32(X), Xlo = tf32(X - Xhi)
 // (n values each).
 void launch_split_tf32(Ctx& c, const double* X, float* X32, float* Xhi, float* Xlo, int64_t n);

@@ -40,13 +40,20 @@ namespace {
 
 constexpr int kProducers = 128;            // four producer warps, also the epilogue
 constexpr int kThreads = kProducers + 32;  // + the MMA warp
-constexpr int kStages = 3;
 constexpr uint32_t kATile = 128 * 128;      // 128 rows x 128 B
 constexpr uint32_t kBTile = 32 * 256;       // 32 K rows x 64 FP32
-constexpr uint32_t kStage = kATile + 2 * kBTile;  // 32 KB, a multiple of 1024
-// + alignment slack, barriers and TMEM slot, and 4 KB past the last stage so
-// that no MMA operand read can leave the allocation
-constexpr uint32_t kSmemBytes = kStages * kStage + 1024 + 256 + 4096;
+// Stage layout: A, [A_lo when P is split], B_hi, B_lo.  Without the split a
+// stage is 32 KB and three stages fit twice per SM; with it 48 KB and two.
+template <bool SP>
+struct NearCfg {
+    static constexpr int kStages = SP ? 2 : 3;
+    static constexpr uint32_t kALo = kATile;                          // offset of A_lo (SP)
+    static constexpr uint32_t kBOff = SP ? 2 * kATile : kATile;       // offset of B_hi
+    static constexpr uint32_t kStage = kBOff + 2 * kBTile;            // multiple of 1024
+    // + alignment slack, barriers and TMEM slot, and 4 KB past the last
+    // stage so that no MMA operand read can leave the allocation
+    static constexpr uint32_t kSmemBytes = kStages * kStage + 1024 + 256 + 4096;
+};
 constexpr uint32_t kTmemCols = 64;
 constexpr int kWaitLimit = 1 << 22;
 // Instruction descriptor: D F32, A/B TF32, A K-major, B MN-major, N = 64, M = 128.
@@ -125,12 +132,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
+// SP (split P): P holds full FP32 values; the producers split each staged A
+// tile into TF32 hi (in place) and lo (A_lo) parts once its copies landed,
+// and the MMA thread adds the third product A_lo B_hi, so the near apply is
+// accurate to about 2^-21 in both P and X.
+template <bool SP>
 __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int32_t* __restrict__ it_leaf,
                                                             const int32_t* __restrict__ it_row0,
                                                             const float* __restrict__ P,
                                                             const float* __restrict__ Xhi,
                                                             const float* __restrict__ Xlo, double* __restrict__ Y,
                                                             int R, int* __restrict__ err) {
+    using Cfg = NearCfg<SP>;
+    constexpr int kStages = Cfg::kStages;
+    constexpr uint32_t kStage = Cfg::kStage;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -176,6 +191,27 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
         // 4 (tid % 4) .. 4 (tid % 4) + 3 of X_hi and X_lo.
         const int kb = tid >> 2, q0 = (tid & 3) * 4;
         int e = 0;
+        // SP: split the A chunks this thread copied into stage `jj` (after
+        // its copies landed), then signal the stage.
+        auto split_and_signal = [&](int jj) {
+            const int sst = jj % kStages;
+            uint8_t* at = sbase + (size_t)sst * kStage;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int id = tid + kProducers * q, row = id >> 3, c16 = id & 7;
+                if (row < m) {
+                    float4* hp = reinterpret_cast<float4*>(at + swz(row, c16));
+                    float4* lp = reinterpret_cast<float4*>(at + Cfg::kALo + swz(row, c16));
+                    const float4 v = *hp;
+                    const float4 h = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
+                    *lp = make_float4(to_tf32(v.x - h.x), to_tf32(v.y - h.y), to_tf32(v.z - h.z), to_tf32(v.w - h.w));
+                    *hp = h;
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[sst])) : "memory");
+        };
+        int signalled = 0;  // SP: stages split and signalled
         for (int j = 0; j < nsl; ++j) {
             const int st = j % kStages;
             if (j >= kStages && !mbar_wait(smem_u32(&empty[st]), (uint32_t)(((j / kStages) - 1) & 1))) {
@@ -184,7 +220,7 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
             }
             if (*(volatile int*)&s_bad) break;
             const uint32_t a = base + (uint32_t)st * kStage;
-            const uint32_t bh = a + kATile, bl = bh + kBTile;
+            const uint32_t bh = a + Cfg::kBOff, bl = bh + kBTile;
             const int k0 = j * 32;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -210,9 +246,26 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
                 cp16(bh + d, Xhi + off, ok);
                 cp16(bl + d, Xlo + off, ok);
             }
-            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st])) : "memory");
+            if constexpr (SP) {
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                if (j >= 1) {
+                    asm volatile("cp.async.wait_group 1;" ::: "memory");
+                    split_and_signal(j - 1);
+                    signalled = j;
+                }
+            } else {
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st]))
+                             : "memory");
+            }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
+        if constexpr (SP) {
+            // the last issued stage (also after an expired wait: every
+            // issued stage is signalled, so the MMA thread never waits on a
+            // stage whose copies went out)
+            const int issued_p = *(volatile int*)&s_bad ? signalled + 1 : nsl;
+            for (int jj = signalled; jj < issued_p && jj < nsl; ++jj) split_and_signal(jj);
+        }
     } else if (tid == kProducers) {
         int issued = 0;
         for (int j = 0; j < nsl; ++j) {
@@ -224,7 +277,7 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t a = base + (uint32_t)st * kStage;
-            const uint32_t bh = a + kATile, bl = bh + kBTile;
+            const uint32_t bh = a + Cfg::kBOff, bl = bh + kBTile;
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
                 const uint64_t ad = desc_k_sw128(a + (uint32_t)kk * 32u);
@@ -237,6 +290,11 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
                     "l"(ad), "l"(bdh), "r"(kIdesc), "r"(accf));
                 asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(ad), "l"(bdl),
                              "r"(kIdesc));
+                if constexpr (SP) {
+                    const uint64_t adl = desc_k_sw128(a + Cfg::kALo + (uint32_t)kk * 32u);
+                    asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(adl),
+                                 "l"(bdh), "r"(kIdesc));
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&empty[st]))
@@ -309,13 +367,20 @@ void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n) {
 
 void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, const int32_t* it_leaf,
                           const int32_t* it_row0, const float* P, const float* Xhi, const float* Xlo, double* Y, int R,
-                          int* err) {
+                          int* err, bool split_p) {
     if (nitems == 0) return;
     if (R % 4 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core near apply needs R a multiple of 4");
-    KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 16.0 * (double)p.N * R, 4.0 * (double)nnz * R);
-    set_smem_once(k_near_apply_tc, (int)kSmemBytes);
-    k_near_apply_tc<<<dim3(nitems, (R + 63) / 64), kThreads, kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xhi, Xlo,
-                                                                                     Y, R, err);
+    KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 16.0 * (double)p.N * R, (split_p ? 6.0 : 4.0) * (double)nnz * R);
+    const dim3 grid(nitems, (R + 63) / 64);
+    if (split_p) {
+        set_smem_once(k_near_apply_tc<true>, (int)NearCfg<true>::kSmemBytes);
+        k_near_apply_tc<true><<<grid, kThreads, NearCfg<true>::kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xhi,
+                                                                                      Xlo, Y, R, err);
+    } else {
+        set_smem_once(k_near_apply_tc<false>, (int)NearCfg<false>::kSmemBytes);
+        k_near_apply_tc<false><<<grid, kThreads, NearCfg<false>::kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xhi,
+                                                                                        Xlo, Y, R, err);
+    }
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }

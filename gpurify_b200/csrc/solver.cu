@@ -433,7 +433,7 @@ struct Operator {
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
-    int mixed_near = 0;  // 0: TF32 tensor-core near apply, 1: FP32 CUDA cores
+    int mixed_near = 0;  // 0: TF32 tensor-core near apply, 1: FP32 CUDA cores, 2: tensor cores with P split hi/lo
     BlockJacobi bj;
     bool factored = false;  // M2L through the low-rank factors (compressed operators)
     bool tc32 = false;      // mixed: FP32 M2L on the tensor cores (orders 4 and 5)
@@ -583,10 +583,10 @@ struct Operator {
             P32.alloc((size_t)pl.nnz(), s);
             if (mixed_near == 0)
                 launch_to_tf32(ctx, P.p, P32.p, pl.nnz());
-            else
+            else  // FP32 CUDA-core apply, or the tensor-core apply that splits P on chip
                 launch_to_f32(ctx, P.p, P32.p, pl.nnz());
             X32.alloc((size_t)pl.N * R, s);
-            if (mixed_near == 0) {
+            if (mixed_near != 1) {
                 Xhi32.alloc((size_t)pl.N * R, s);
                 Xlo32.alloc((size_t)pl.N * R, s);
             }
@@ -768,10 +768,10 @@ struct Operator {
         applies32 += 1;
     }
     void apply32_direct(const double* X, double* Y) {
-        if (mixed_near == 0) {
+        if (mixed_near != 1) {
             launch_split_tf32(ctx, X, X32.p, Xhi32.p, Xlo32.p, pl.N * R);
             launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, Xhi32.p,
-                                 Xlo32.p, Y, R, tc_err.p);
+                                 Xlo32.p, Y, R, tc_err.p, mixed_near == 2);
         } else {
             launch_to_f32(ctx, X, X32.p, pl.N * R);
             launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
@@ -1096,7 +1096,8 @@ Opts normalize(const gpx_solve_opts* o) {
     r.precond = o->precond;
     r.skip_ground_rhs = o->skip_ground_rhs;
     // The TF32 near apply perturbs the inner operator by ~2^-11 per entry, so
-    // inner solves past 1e-3 buy little; the FP32 near apply supports 1e-5.
+    // inner solves past 1e-3 buy little; the FP32-accurate near applies
+    // (CUDA cores, or tensor cores with P split) support 1e-5.
     r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : (o->mixed_near == 0 ? 3 : 5);
     r.mesh_max_edge = o->mesh_max_edge_m;
     r.max_panels = o->max_panels;
@@ -1153,7 +1154,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
                     "with centroid far-field sources (far_quad 0)");
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
     if (o.precond < 0 || o.precond > 2) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0, 1 or 2");
-    if (o.mixed_near != 0 && o.mixed_near != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0 or 1");
+    if (o.mixed_near < 0 || o.mixed_near > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1 or 2");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))

@@ -96,12 +96,14 @@ typedef struct {
     int32_t skip_ground_rhs; /* 1: do not solve the substrate column (the reference solves it);
                                 the per-net result needs only the nets' columns */
     int32_t inner_tol_exp;   /* mixed: floor of the adaptive inner tolerance, 10^-x; 0 -> 3 with the
-                                tensor-core near apply, 5 with the FP32 one */
+                                TF32 near apply (mixed_near 0), 5 with the FP32-accurate ones */
     double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
                                 (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
-    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05), 1 -> FP32 CUDA cores */
+    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05), 1 -> FP32 CUDA cores,
+                                2 -> TF32 tensor cores with the near blocks kept in FP32 and split into TF32
+                                hi and lo parts on chip (three products; FP32-accurate) */
     int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5 with centroid
                                 far-field sources, else the factored low-rank form on FP32 CUDA cores;
                                 1 -> always the factored form (compressed operators); 2 -> tensor cores

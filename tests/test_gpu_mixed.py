@@ -29,7 +29,7 @@ def window(nets=12, side=15.0, edge=0.3e-6):
                                 mesh_max_edge_m=edge, max_panels=-1)
 
 
-@pytest.mark.parametrize("mixed_near", [0, 1])
+@pytest.mark.parametrize("mixed_near", [0, 1, 2])
 @pytest.mark.parametrize("nrhs", [3, 64, 100])
 def test_mixed_operator_close_to_fp64(ctx, nrhs, mixed_near):
     p = window()
@@ -72,7 +72,8 @@ def test_mixed_exact_m2l_needs_centroid_sources(ctx):
 
 
 @pytest.mark.parametrize("order,far_quad,mixed_near,mixed_m2l", [(4, 0, 0, 0), (4, 1, 0, 0), (4, 1, 1, 0),
-                                                                 (5, 1, 0, 0), (5, 1, 0, 3), (6, 1, 0, 3)])
+                                                                 (5, 1, 0, 0), (5, 1, 0, 3), (6, 1, 0, 3),
+                                                                 (5, 1, 2, 3)])
 def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near, mixed_m2l):
     p = window()
     nc = len(p["nets"]) + 1
