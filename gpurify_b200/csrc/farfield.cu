@@ -689,7 +689,7 @@ inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b);
 
 template <class T, int N>
 void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y, int R,
-                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all) {
+                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all, const P2MSplit* p2m_tc) {
     cudaStream_t s = c.stream;
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>();
     constexpr size_t smem = tree_smem<T, N>();
@@ -701,9 +701,20 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     {
         KTimer t(c, prec_tag<T>(K_P2M), (double)p.N * (wb * R + wb * N3 + 8.0) + (p.nleaf + 2.0 * f.npart) * box_bytes,
                  2.0 * (double)p.N * N3 * R);
-        k_p2m<T, N><<<dim3(p.nitems, rchunks64), 256, 0, s>>>(p, f.p2m_slot, X, w.src, w.src_area, E, R, Rb);
-        GPX_LAUNCH_CHECK();
-        c.launches += 1;
+        if constexpr (sizeof(T) == 4 && (N == 4 || N == 5)) {
+            if (p2m_tc) {
+                launch_p2m_tc(c, p, f.p2m_slot, p2m_tc->whi, p2m_tc->wlo, p2m_tc->xhi, p2m_tc->xlo,
+                              reinterpret_cast<float*>(E), R, Rb, p2m_tc->err);
+            } else {
+                k_p2m<T, N><<<dim3(p.nitems, rchunks64), 256, 0, s>>>(p, f.p2m_slot, X, w.src, w.src_area, E, R, Rb);
+                GPX_LAUNCH_CHECK();
+                c.launches += 1;
+            }
+        } else {
+            k_p2m<T, N><<<dim3(p.nitems, rchunks64), 256, 0, s>>>(p, f.p2m_slot, X, w.src, w.src_area, E, R, Rb);
+            GPX_LAUNCH_CHECK();
+            c.launches += 1;
+        }
         if (f.nfix > 0) {
             const int64_t block = (int64_t)Rb * NS;
             k_p2m_fix<T><<<dim3(f.nfix, cdiv(block, 1024)), 256, 0, s>>>(p.nbox, p.leaf_box0, f.fix_leaf, f.fix_first,
@@ -763,13 +774,14 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
 
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
-                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all) {
+                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all,
+                      const P2MSplit* p2m_tc) {
     switch (p.n) {
-        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
-        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
-        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
-        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
-        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all); break;
+        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
+        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
+        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
+        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
+        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
         default: throw Error(GPX_ERR_INVALID_ARG, "far field runs Chebyshev orders 2 to 6");
     }
 }
@@ -812,8 +824,9 @@ void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const dou
 
 template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*,
                                        const FarWeights<double>&, double*, int, int, double*, double*, double,
-                                       const M2LLevelFn<double>&, bool);
+                                       const M2LLevelFn<double>&, bool, const P2MSplit*);
 template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, const FarWeights<float>&,
-                                      double*, int, int, float*, float*, double, const M2LLevelFn<float>&, bool);
+                                      double*, int, int, float*, float*, double, const M2LLevelFn<float>&, bool,
+                                      const P2MSplit*);
 
 }  // namespace gpx

@@ -30,9 +30,26 @@ struct FarWeights {
 // supplied per level.
 // m2l_all_levels: the M2L callback runs once for every level (level -1,
 // first box of level 2, box count of levels 2..L) instead of once per level.
+// Inputs of the tensor-core P2M (p2m_tc.cu): the source weights (area
+// folded in) and the charges, each split into TF32 hi and lo parts; weight
+// rows have a stride of 128 nodes.
+struct P2MSplit {
+    const float* whi = nullptr;
+    const float* wlo = nullptr;
+    const float* xhi = nullptr;
+    const float* xlo = nullptr;
+    int* err = nullptr;
+};
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
-                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all_levels = false);
+                      int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all_levels = false,
+                      const P2MSplit* p2m_tc = nullptr);
+// Whi / Wlo [N][128] = TF32 split of (area if mul_area) x W[N][n3] (n3 <= 128).
+void launch_split_weights(Ctx& c, const double* W, int n3, const double* area, bool mul_area, float* Whi, float* Wlo,
+                          int64_t N);
+// E[leaf or partial slot] = P2M of the split weights and charges (orders 4 and 5).
+void launch_p2m_tc(Ctx& c, const DevPlan& p, const int32_t* slot, const float* Whi, const float* Wlo, const float* Xhi,
+                   const float* Xlo, float* E, int R, int Rb, int* err);
 
 // FP64 M2L of one level with CUDA-core FMAs (dense operators).
 void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const double* E, int R, double scale);

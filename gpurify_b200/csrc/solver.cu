@@ -412,6 +412,8 @@ struct Operator {
     DBuf<double> P, inv_diag, E64, L64;
     DBuf<float> P32, E32, L32, X32, W32, Sc32;
     DBuf<float> Xhi32, Xlo32;  // TF32 split of the FP32 apply's input (tensor-core near apply)
+    bool p2m_tc = false;       // mixed: P2M on the tensor cores from the split weights below
+    DBuf<float> Whi32, Wlo32;  // TF32 split of the P2M weights (area folded in), N x 128
     DBuf<double> Sc;  // transposed operator: collocation weights as P2M weights
     FarWeights<double> w64;
     FarWeights<float> w32;
@@ -606,6 +608,14 @@ struct Operator {
                     launch_to_f32(ctx, Sc.p, Sc32.p, pl.N * pl.n3);
                     w32 = FarWeights<float>{Sc32.p, false, W32.p, true};
                 }
+                if (p2m_tc) {
+                    Whi32.alloc((size_t)pl.N * 128, s);
+                    Wlo32.alloc((size_t)pl.N * 128, s);
+                    if (!transposed)
+                        launch_split_weights(ctx, d.wsrc.p, pl.n3, d.area.p, true, Whi32.p, Wlo32.p, pl.N);
+                    else
+                        launch_split_weights(ctx, Sc.p, pl.n3, d.area.p, false, Whi32.p, Wlo32.p, pl.N);
+                }
                 if (tc32 || shared) build_tc_lists(ctx, pl, tc);
                 if (shared) {
                     ensure_shared(ctx, *const_cast<DevM2L*>(m2l));
@@ -794,7 +804,9 @@ struct Operator {
                     launch_m2l_fac<float>(ctx, fac32, level < 0 ? fac_all : fac_level[level], b0, nb, L32.p, E32.p,
                                           Rb32, scale);
             };
-            launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true);
+            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p};
+            launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true,
+                                    p2m_tc ? &sp : nullptr);
         }
     }
 
@@ -1108,6 +1120,7 @@ Opts normalize(const gpx_solve_opts* o) {
     r.batch_streams = o->batch_streams;
     r.col_begin = o->col_begin;
     r.col_count = o->col_count;
+    r.mixed_far_tc = o->mixed_far_tc;
     return r;
 }
 
@@ -1156,6 +1169,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.precond < 0 || o.precond > 2) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0, 1 or 2");
     if (o.mixed_near < 0 || o.mixed_near > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1 or 2");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
+    if (o.mixed_far_tc != 0 && o.mixed_far_tc != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_far_tc must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -1187,6 +1201,8 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     // expansions carry large alternating node values (sources slightly outside
     // their leaf box) and the TF32 inputs lose 1e-2 of the far field.
     pr.op->shared = o.precision == GPX_PREC_MIXED && o.mixed_m2l == 3 && (o.order == 5 || o.order == 6);
+    pr.op->p2m_tc = o.precision == GPX_PREC_MIXED && o.mixed_far_tc == 1 && o.mixed_near != 1 &&
+                    (o.order == 4 || o.order == 5);
     pr.op->tc32 = !pr.op->shared && o.precision == GPX_PREC_MIXED && o.mixed_m2l != 1 &&
                   (o.order == 4 || o.order == 5) &&
                   (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT || o.mixed_m2l >= 2);
@@ -1523,6 +1539,7 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
     opT.use_graphs = o.graphs != 0;
     opT.tc32 = op.tc32;
     opT.shared = op.shared;
+    opT.p2m_tc = op.p2m_tc;
     opT.assemble(&op);
     DBuf<double> Q, Lam;
     Q.alloc((size_t)n * R, s);

@@ -23,6 +23,7 @@ struct Opts {
     int graphs = 1;         // capture operator applies into CUDA graphs
     int batch_streams = 0;  // batched solves: concurrent streams (0 -> default)
     int col_begin = 0, col_count = 0;  // column subset (col_count 0: every column)
+    int mixed_far_tc = 0;              // mixed: P2M on the tensor cores
 };
 Opts normalize(const gpx_solve_opts* o);
 

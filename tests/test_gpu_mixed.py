@@ -63,6 +63,24 @@ def test_mixed_operator_close_to_fp64_high_order(ctx, order, m2l_mode, mixed_m2l
     assert e.max() < 1e-3, e.max()
 
 
+@pytest.mark.parametrize("order,far_quad,mixed_m2l", [(4, 1, 0), (5, 0, 3), (5, 1, 3), (5, 1, 2)])
+def test_tensor_core_p2m_matches_cuda_core_p2m(ctx, order, far_quad, mixed_m2l):
+    """The tensor-core P2M (weights and charges split into TF32 hi and lo
+    parts) gives the same inner operator as the FP32 CUDA-core P2M to well
+    below the TF32 M2L's own error."""
+    p = window()
+    rng = np.random.default_rng(6)
+    sig = rng.standard_normal((len(p["verts"]), 64))
+    kw = dict(order=order, max_level=5, dense_below=-1, far_quad=far_quad, precision=1, mixed_m2l=mixed_m2l)
+    y0, _ = ctx.operator_apply(p["verts"], sig, **kw)
+    y1, _ = ctx.operator_apply(p["verts"], sig, mixed_far_tc=1, **kw)
+    y64, _ = ctx.operator_apply(p["verts"], sig, **dict(kw, precision=0, mixed_m2l=0))
+    d01 = np.linalg.norm(y1 - y0, axis=0) / np.linalg.norm(y0, axis=0)
+    e1 = np.linalg.norm(y1 - y64, axis=0) / np.linalg.norm(y64, axis=0)
+    assert d01.max() < 1e-5, d01.max()
+    assert e1.max() < 1e-3, e1.max()
+
+
 def test_mixed_exact_m2l_needs_centroid_sources(ctx):
     p = window()
     with pytest.raises(_lib.GpxError) as ei:
