@@ -39,6 +39,10 @@ struct P2MSplit {
     const float* xhi = nullptr;
     const float* xlo = nullptr;
     int* err = nullptr;
+    // L2P on the tensor cores too when given: the target weights split into
+    // TF32 hi and lo parts (rows of 128 nodes)
+    const float* shi = nullptr;
+    const float* slo = nullptr;
 };
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
@@ -47,6 +51,9 @@ void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, 
 // Whi / Wlo [N][128] = TF32 split of (area if mul_area) x W[N][n3] (n3 <= 128).
 void launch_split_weights(Ctx& c, const double* W, int n3, const double* area, bool mul_area, float* Whi, float* Wlo,
                           int64_t N);
+// Y += coef L2P of the far-field locals L with split target weights (orders 4 and 5).
+void launch_l2p_tc(Ctx& c, const DevPlan& p, const float* L, const float* Shi, const float* Slo, double* Y, int R,
+                   int Rb, double coef, int* err);
 // E[leaf or partial slot] = P2M of the split weights and charges (orders 4 and 5).
 void launch_p2m_tc(Ctx& c, const DevPlan& p, const int32_t* slot, const float* Whi, const float* Wlo, const float* Xhi,
                    const float* Xlo, float* E, int R, int Rb, int* err);

@@ -414,6 +414,7 @@ struct Operator {
     DBuf<float> Xhi32, Xlo32;  // TF32 split of the FP32 apply's input (tensor-core near apply)
     bool p2m_tc = false;       // mixed: P2M on the tensor cores from the split weights below
     DBuf<float> Whi32, Wlo32;  // TF32 split of the P2M weights (area folded in), N x 128
+    DBuf<float> Shi32, Slo32;  // TF32 split of the L2P weights, N x 128
     DBuf<double> Sc;  // transposed operator: collocation weights as P2M weights
     FarWeights<double> w64;
     FarWeights<float> w32;
@@ -611,10 +612,19 @@ struct Operator {
                 if (p2m_tc) {
                     Whi32.alloc((size_t)pl.N * 128, s);
                     Wlo32.alloc((size_t)pl.N * 128, s);
-                    if (!transposed)
+                    Shi32.alloc((size_t)pl.N * 128, s);
+                    Slo32.alloc((size_t)pl.N * 128, s);
+                    if (!transposed) {
+                        // P2M: source weights with the area; L2P: collocation weights at the centroids
                         launch_split_weights(ctx, d.wsrc.p, pl.n3, d.area.p, true, Whi32.p, Wlo32.p, pl.N);
-                    else
+                        DBuf<double> S64;
+                        S64.alloc((size_t)pl.N * pl.n3, s);
+                        launch_centroid_weights(ctx, d.v, nullptr, S64.p);
+                        launch_split_weights(ctx, S64.p, pl.n3, d.area.p, false, Shi32.p, Slo32.p, pl.N);
+                    } else {
                         launch_split_weights(ctx, Sc.p, pl.n3, d.area.p, false, Whi32.p, Wlo32.p, pl.N);
+                        launch_split_weights(ctx, d.wsrc.p, pl.n3, d.area.p, true, Shi32.p, Slo32.p, pl.N);
+                    }
                 }
                 if (tc32 || shared) build_tc_lists(ctx, pl, tc);
                 if (shared) {
@@ -804,7 +814,7 @@ struct Operator {
                     launch_m2l_fac<float>(ctx, fac32, level < 0 ? fac_all : fac_level[level], b0, nb, L32.p, E32.p,
                                           Rb32, scale);
             };
-            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p};
+            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p, Shi32.p, Slo32.p};
             launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true,
                                     p2m_tc ? &sp : nullptr);
         }

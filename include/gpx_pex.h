@@ -120,8 +120,9 @@ typedef struct {
                                 right-hand sides are spread over several GPUs); the other columns of
                                 maxwell_out are NaN */
     int32_t col_count;       /* 0 -> every column (all but the substrate with skip_ground_rhs) */
-    int32_t mixed_far_tc;    /* mixed, orders 4 and 5, tensor-core near apply: 1 -> P2M on the tensor cores
-                                too (weights and charges split into TF32 hi and lo parts, FP32-accurate) */
+    int32_t mixed_far_tc;    /* mixed, orders 4 and 5, tensor-core near apply: 1 -> P2M and L2P on the tensor
+                                cores too (weights, charges and local expansions split into TF32 hi and lo
+                                parts, FP32-accurate) */
 } gpx_solve_opts;
 
 typedef struct {

@@ -64,10 +64,10 @@ def test_mixed_operator_close_to_fp64_high_order(ctx, order, m2l_mode, mixed_m2l
 
 
 @pytest.mark.parametrize("order,far_quad,mixed_m2l", [(4, 1, 0), (5, 0, 3), (5, 1, 3), (5, 1, 2)])
-def test_tensor_core_p2m_matches_cuda_core_p2m(ctx, order, far_quad, mixed_m2l):
-    """The tensor-core P2M (weights and charges split into TF32 hi and lo
-    parts) gives the same inner operator as the FP32 CUDA-core P2M to well
-    below the TF32 M2L's own error."""
+def test_tensor_core_p2m_l2p_match_cuda_cores(ctx, order, far_quad, mixed_m2l):
+    """The tensor-core P2M and L2P (weights, charges and local expansions split
+    into TF32 hi and lo parts) give the same inner operator as the FP32
+    CUDA-core P2M and L2P to well below the TF32 M2L's own error."""
     p = window()
     rng = np.random.default_rng(6)
     sig = rng.standard_normal((len(p["verts"]), 64))
