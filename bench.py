@@ -482,6 +482,7 @@ def run_workload(args):
         dt, res = timed(lambda: ctx.cap_solve_batched(probs, **kw), 1)
         out["mixed"] = {"windows_per_s": len(probs) / dt, "s": dt, "panel_rhs_per_s": NR / dt,
                         "max_iterations": max(r["iterations"] for _, r in res),
+                        "kernel_launches": int(sum(r["kernel_launches"] for _, r in res)),
                         "timing": "wall clock around the synchronous batched call (8 streams)"}
     elif args.workload == "block":
         lay = layouts.large_block(n_nets=args.block_nets, side_um=args.block_side)
