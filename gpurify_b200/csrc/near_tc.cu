@@ -12,7 +12,7 @@
 // a kStages ring in shared memory:
 //   A (128 x 32, K-major, 128-byte swizzle) = the item's P rows, streamed from
 //     HBM;
-//   B_hi, B_lo (32 x 64 each, MN-major, 128-byte swizzle) = the 32 source
+//   B_hi, B_lo (32 x 64 each, MN-major, 128-byte swizzle on a 32-byte base) = the 32 source
 //     panels' rows of X_hi = tf32(x) and X_lo = tf32(x - x_hi), gathered from
 //     the L2-resident split copies written by k_split_tf32.  A source row of
 //     X is 64 contiguous FP32 values, which is exactly one K row of an
@@ -75,16 +75,19 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t addr) {
     return d;
 }
 
-// MN-major operand, 128 B swizzle: an atom is 8 K rows x 128 B (32 FP32 along
-// MN); `lbo` = bytes between the atoms of consecutive 32-wide MN blocks,
-// `sbo` = bytes between consecutive 8-row K groups.
-__device__ __forceinline__ uint64_t desc_mn_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// MN-major TF32 operand: the only shared-memory layout the tensor cores take
+// for 32-bit MN-major operands is SWIZZLE_128B_BASE32B (descriptor layout
+// type 1): atoms of 4 K rows x 128 B (32 FP32 along MN), the 32-byte granules
+// of row r stored at granule ^ r.  `lbo` = bytes between the atoms of
+// consecutive 32-wide MN blocks, `sbo` = bytes between consecutive 4-row K
+// groups.
+__device__ __forceinline__ uint64_t desc_mn_sw128b32(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     uint64_t d = 0;
     d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
     d |= (uint64_t)(lbo >> 4) << 16;
     d |= (uint64_t)(sbo >> 4) << 32;
     d |= (uint64_t)1 << 46;
-    d |= (uint64_t)2 << 61;
+    d |= (uint64_t)1 << 61;
     return d;
 }
 
@@ -95,10 +98,12 @@ __device__ __forceinline__ uint32_t swz(uint32_t row, uint32_t chunk) {
 }
 
 // Byte offset of 16-byte chunk q (0..15: FP32 columns 4q..4q+3) of K row k
-// (0..31) in the MN-major B tile: atom (K group k/8, MN block q/8) at
-// (2 (k/8) + q/8) x 1024 B, row k%8 of the atom, chunk q%8 swizzled.
+// (0..31) in the MN-major B tile: atom (4-row K group k/4, MN block q/8) at
+// (2 (k/4) + q/8) x 512 B, row k%4 of the atom, 32-byte granule (q%8)/2
+// swizzled by the row.
 __device__ __forceinline__ uint32_t swz_mn(uint32_t k, uint32_t q) {
-    return ((k >> 3) * 2u + (q >> 3)) * 1024u + (k & 7u) * 128u + (((q & 7u) ^ (k & 7u)) << 4);
+    const uint32_t r = k & 3u;
+    return ((k >> 2) * 2u + (q >> 3)) * 512u + r * 128u + ((((q & 7u) >> 1) ^ r) << 5) + ((q & 1u) << 4);
 }
 
 __device__ __forceinline__ float to_tf32(float x) {
@@ -281,8 +286,8 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
                 const uint64_t ad = desc_k_sw128(a + (uint32_t)kk * 32u);
-                const uint64_t bdh = desc_mn_sw128(bh + (uint32_t)kk * 2048u, 1024u, 2048u);
-                const uint64_t bdl = desc_mn_sw128(bl + (uint32_t)kk * 2048u, 1024u, 2048u);
+                const uint64_t bdh = desc_mn_sw128b32(bh + (uint32_t)kk * 2048u, 512u, 1024u);
+                const uint64_t bdl = desc_mn_sw128b32(bl + (uint32_t)kk * 2048u, 512u, 1024u);
                 const uint32_t accf = (j > 0 || kk > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"

@@ -36,21 +36,28 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// MN-major operand, 128 B swizzle (see near_tc.cu).
-__device__ __forceinline__ uint64_t desc_mn_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// MN-major TF32 operand: the only shared-memory layout the tensor cores take
+// for 32-bit MN-major operands is SWIZZLE_128B_BASE32B (descriptor layout
+// type 1): atoms of 4 K rows x 128 B (32 FP32 along MN), the 32-byte granules
+// of row r stored at granule ^ r.  `lbo` = bytes between the atoms of
+// consecutive 32-wide MN blocks, `sbo` = bytes between consecutive 4-row K
+// groups.
+__device__ __forceinline__ uint64_t desc_mn_sw128b32(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     uint64_t d = 0;
     d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
     d |= (uint64_t)(lbo >> 4) << 16;
     d |= (uint64_t)(sbo >> 4) << 32;
     d |= (uint64_t)1 << 46;
-    d |= (uint64_t)2 << 61;
+    d |= (uint64_t)1 << 61;
     return d;
 }
 
 // Byte offset of 16-byte chunk q of K row k in an MN-major tile with `nb`
-// 32-wide MN blocks: atom (K group k/8, MN block q/8) at (nb (k/8) + q/8) KB.
+// 32-wide MN blocks: atom (4-row K group k/4, MN block q/8) at
+// (nb (k/4) + q/8) x 512 B, row k%4, 32-byte granule (q%8)/2 swizzled by the row.
 __device__ __forceinline__ uint32_t swz_mn(uint32_t k, uint32_t q, uint32_t nb) {
-    return ((k >> 3) * nb + (q >> 3)) * 1024u + (k & 7u) * 128u + (((q & 7u) ^ (k & 7u)) << 4);
+    const uint32_t r = k & 3u;
+    return ((k >> 2) * nb + (q >> 3)) * 512u + r * 128u + ((((q & 7u) >> 1) ^ r) << 5) + ((q & 1u) << 4);
 }
 
 __device__ __forceinline__ void cp16(uint32_t dst, const void* src, bool valid) {
@@ -146,10 +153,10 @@ __global__ void __launch_bounds__(kThreads) k_p2m_tc(DevPlan p, const int32_t* _
             const uint32_t bh = ah + 2 * kATile, bl = bh + kBTile;
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
-                const uint64_t adh = desc_mn_sw128(ah + (uint32_t)kk * 4096u, 1024u, 4096u);
-                const uint64_t adl = desc_mn_sw128(al + (uint32_t)kk * 4096u, 1024u, 4096u);
-                const uint64_t bdh = desc_mn_sw128(bh + (uint32_t)kk * 2048u, 1024u, 2048u);
-                const uint64_t bdl = desc_mn_sw128(bl + (uint32_t)kk * 2048u, 1024u, 2048u);
+                const uint64_t adh = desc_mn_sw128b32(ah + (uint32_t)kk * 4096u, 512u, 2048u);
+                const uint64_t adl = desc_mn_sw128b32(al + (uint32_t)kk * 4096u, 512u, 2048u);
+                const uint64_t bdh = desc_mn_sw128b32(bh + (uint32_t)kk * 2048u, 512u, 1024u);
+                const uint64_t bdl = desc_mn_sw128b32(bl + (uint32_t)kk * 2048u, 512u, 1024u);
                 const uint32_t accf = (s > 0 || kk > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
