@@ -135,6 +135,37 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class DeviceMemoryWatch:
+    """High-water mark of device memory in use (total - free, cudaMemGetInfo on
+    device 0) sampled every 20 ms by a thread while the block runs; catches
+    the library's stream-ordered allocations, which torch's counters miss."""
+
+    def __enter__(self):
+        import torch
+
+        self.torch = torch
+        self.peak_used = 0
+        self.stop = threading.Event()
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self._sample()
+        self.t.start()
+        return self
+
+    def _sample(self):
+        free, total = self.torch.cuda.mem_get_info(0)
+        self.peak_used = max(self.peak_used, total - free)
+
+    def _run(self):
+        while not self.stop.wait(0.02):
+            self._sample()
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.t.join()
+        self._sample()
+        return False
+
+
 def load_peaks():
     """Measured peaks of this pool's B200s (driver-written MEASURED_PEAKS.json):
     HBM copy GB/s, and dense bf16 TFLOP/s as a burst and sustained under the
@@ -495,12 +526,24 @@ def run_workload(args):
         rows = sorted(int(r) for r in np.random.default_rng(16).choice(nc - 1, min(16, nc - 1), replace=False))
         out.update(panels=len(p["verts"]), rhs=nc - 1, params=len(params), gradient_nets=rows)
         kw = dict(base, precision=_lib.PREC_MIXED, precond=1)
-        dt0, (C, rep) = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), 1)
-        dt, (_, dC, rep2) = timed(lambda: ctx.cap_sensitivity(p["verts"], p["cond"], nc, V, **kw), 1)
-        out["mixed"] = {"ms_capacitance_only": dt0 * 1e3, "ms_capacitance_plus_gradients": dt * 1e3,
-                        "iterations": rep["iterations"], "iterations_forward_plus_adjoint": rep2["iterations"],
+        free0, total = torch.cuda.mem_get_info(0)
+        with DeviceMemoryWatch() as mw:
+            dt0, (C, rep) = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), 1)
+        out["mixed"] = {"ms_capacitance_only": dt0 * 1e3, "iterations": rep["iterations"],
+                        "outer_iterations": rep["outer_iterations"], "converged": bool(rep["converged"]),
                         "panel_rhs_per_s": len(p["verts"]) * (nc - 1) / dt0,
-                        "max_abs_dC_of_gradient_nets": float(np.abs(dC[:, rows, :nc - 1]).max())}
+                        "peak_device_bytes_solve": int(mw.peak_used - (total - free0)),
+                        "device_bytes_total": int(total), "near_pairs": int(rep["nnz_near"]),
+                        "depth": int(rep["max_level"]),
+                        "memory_sampling": "free device memory sampled every 20 ms during the call"}
+        print(json.dumps(dict(out, part="capacitance")), flush=True)
+        with DeviceMemoryWatch() as mw:
+            dt, (_, dC, rep2) = timed(lambda: ctx.cap_sensitivity(p["verts"], p["cond"], nc, V, grad_rows=rows,
+                                                                  **kw), 1)
+        out["mixed"].update(ms_capacitance_plus_gradients=dt * 1e3,
+                            iterations_forward_plus_adjoint=rep2["iterations"],
+                            max_abs_dC_of_gradient_nets=float(np.abs(dC[:, rows, :nc - 1]).max()),
+                            peak_device_bytes_gradients=int(mw.peak_used - (total - free0)))
     else:  # bus
         lay = layouts.bus_crossing()
         z0, z1 = sensitivity.layer_span(lay.deck, "met2")

@@ -29,7 +29,7 @@ EXPORTS = (
     "gpx_cap_solve_batched", "gpx_operator_apply", "gpx_potential_matrix", "gpx_cap_solve_groups",
     "gpx_extract_quasistatic", "gpx_bridge_panelize", "gpx_plan_check", "gpx_ctx_stream",
     "gpx_ctx_set_profiling", "gpx_ctx_kernel_stats", "gpx_ctx_reset_stats", "gpx_cap_solve_small_static",
-    "gpx_cap_sensitivity", "gpx_autotune",
+    "gpx_cap_sensitivity", "gpx_cap_sensitivity_rows", "gpx_autotune",
 )
 KERNEL_CLASSES = ("near_assemble", "near_apply", "p2m", "m2m", "m2l", "l2l", "l2p", "gs_dot", "gs_axpy", "vec",
                   "small", "near_apply_f64", "p2m_f64", "m2m_f64", "m2l_f64", "l2l_f64", "l2p_f64")
@@ -157,6 +157,8 @@ def load(build_if_missing: bool = True):
                                    C.POINTER(SolveOpts), C.POINTER(TuneReport)]
         L.gpx_cap_sensitivity.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), i32, vp, vp, vp,
                                           C.POINTER(SolveReport)]
+        L.gpx_cap_sensitivity_rows.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), i32, vp, i32, vp,
+                                               vp, vp, C.POINTER(SolveReport)]
         for name in EXPORTS:
             if name not in ("gpx_ctx_destroy", "gpx_last_error", "gpx_version", "gpx_ctx_stream"):
                 getattr(L, name).restype = C.c_int
@@ -260,10 +262,12 @@ class Context:
                                                  C.cast(ptrs, C.c_void_p), C.cast(reps, C.c_void_p)))
         return [(outs[i], reps[i].as_dict()) for i in range(len(outs))]
 
-    def cap_sensitivity(self, verts, cond, ncond, velocities, **kw):
+    def cap_sensitivity(self, verts, cond, ncond, velocities, grad_rows=None, **kw):
         """Maxwell matrix and its derivatives along vertex velocity fields
         (``velocities``: n_params x n_panels x 12).  Returns (C, dC, report)
-        with dC n_params x ncond x ncond (farads per unit parameter)."""
+        with dC n_params x ncond x ncond (farads per unit parameter).  With
+        ``grad_rows`` (conductor indices) only those rows of dC are computed
+        (gpx_cap_sensitivity_rows); the other rows are NaN."""
         v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)
         c = np.ascontiguousarray(cond, dtype=np.int32)
         V = np.ascontiguousarray(velocities, dtype=np.float64).reshape(-1, len(v), 12)
@@ -271,8 +275,14 @@ class Context:
         Cm = np.zeros((ncond, ncond))
         dC = np.zeros((len(V), ncond, ncond))
         rep = SolveReport()
-        self._check(self.L.gpx_cap_sensitivity(self.h, C.byref(pb), C.byref(opts(**kw)), len(V), V.ctypes.data,
-                                               Cm.ctypes.data, dC.ctypes.data, C.byref(rep)))
+        if grad_rows is None:
+            self._check(self.L.gpx_cap_sensitivity(self.h, C.byref(pb), C.byref(opts(**kw)), len(V), V.ctypes.data,
+                                                   Cm.ctypes.data, dC.ctypes.data, C.byref(rep)))
+        else:
+            rows = np.ascontiguousarray(grad_rows, dtype=np.int32)
+            self._check(self.L.gpx_cap_sensitivity_rows(self.h, C.byref(pb), C.byref(opts(**kw)), len(V),
+                                                        V.ctypes.data, len(rows), rows.ctypes.data, Cm.ctypes.data,
+                                                        dC.ctypes.data, C.byref(rep)))
         return Cm, dC, rep.as_dict()
 
     def operator_apply(self, verts, sigma, **kw):

@@ -240,30 +240,43 @@ __global__ void __launch_bounds__(256) k_near_transpose(DevPlan p, const int32_t
     }
 }
 
-// G[i][j] = sum_k da_k [cond_k == rhs_i] X[k][j] - sum_k Lam[k][i] D[k][j]
-// for the conductors solved (rhs_i >= 0); one block per i, threads over j.
-__global__ void k_grad_contract(const int32_t* __restrict__ cond, const int32_t* __restrict__ rhs_cond,
+// Partial sums over one range of panels of
+//   G[i][j] = sum_k da_k [cond_k == row_i] X[k][j] - sum_k Lam[k][i] D[k][j]
+// for the rows solved (row_i >= 0).  X and D are N x R, Lam is N x Ra.  Grid
+// (Ra, splits); 256 threads = 64 columns x 4 panel phases; the block writes
+// Gp[split][i][j] and k_sum_splits adds the splits in order (deterministic).
+__global__ void k_grad_contract(const int32_t* __restrict__ cond, const int32_t* __restrict__ row_cond,
                                 const double* __restrict__ darea, const double* __restrict__ X,
                                 const double* __restrict__ Lam, const double* __restrict__ D, int64_t N, int R,
-                                double* __restrict__ G) {
-    const int i = blockIdx.x;
-    const int ci = rhs_cond[i];
+                                int Ra, double* __restrict__ Gp) {
+    const int i = blockIdx.x, sp = blockIdx.y, nsp = gridDim.y;
+    const int ci = row_cond[i];
+    const int64_t k0 = N * sp / nsp, k1 = N * (sp + 1) / nsp;
     __shared__ double red[256];
     for (int j0 = 0; j0 < R; j0 += 64) {
-        const int j = j0 + (threadIdx.x & 63), part = threadIdx.x >> 6;  // 4 parts over k
+        const int j = j0 + (threadIdx.x & 63), part = threadIdx.x >> 6;  // 4 phases over k
         double acc = 0.0;
         if (j < R && ci >= 0)
-            for (int64_t k = part; k < N; k += 4) {
-                double v = -Lam[k * R + i] * D[k * R + j];
+            for (int64_t k = k0 + part; k < k1; k += 4) {
+                double v = -Lam[k * Ra + i] * D[k * R + j];
                 if (cond[k] == ci) v += darea[k] * X[k * R + j];
                 acc += v;
             }
         red[threadIdx.x] = acc;
         __syncthreads();
-        if (part == 0 && j < R) G[(int64_t)i * R + j] = red[threadIdx.x] + red[threadIdx.x + 64] +
-                                                        red[threadIdx.x + 128] + red[threadIdx.x + 192];
+        if (part == 0 && j < R)
+            Gp[((int64_t)sp * Ra + i) * R + j] =
+                red[threadIdx.x] + red[threadIdx.x + 64] + red[threadIdx.x + 128] + red[threadIdx.x + 192];
         __syncthreads();
     }
+}
+
+__global__ void k_sum_splits(const double* __restrict__ Gp, int nsp, int64_t n, double* __restrict__ G) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    double acc = 0.0;
+    for (int s = 0; s < nsp; ++s) acc += Gp[(int64_t)s * n + e];
+    G[e] = acc;
 }
 
 inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -307,12 +320,17 @@ void launch_near_transpose(Ctx& c, const DevPlan& p, const int32_t* near_rev, co
     c.launches += 1;
 }
 
-void launch_grad_contract(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const double* darea,
-                          const double* X, const double* Lam, const double* D, int64_t N, int R, double* G) {
-    KTimer t(c, K_VEC, 24.0 * N * R + 12.0 * N, 4.0 * (double)N * R * R);
-    k_grad_contract<<<R, 256, 0, c.stream>>>(cond, rhs_cond, darea, X, Lam, D, N, R, G);
+void launch_grad_contract(Ctx& c, const int32_t* cond, const int32_t* row_cond, const double* darea,
+                          const double* X, const double* Lam, const double* D, int64_t N, int R, int Ra, double* Gp,
+                          double* G) {
+    const int nsp = grad_contract_splits(Ra);
+    KTimer t(c, K_VEC, 8.0 * N * (2.0 * R + Ra) + 12.0 * N, 4.0 * (double)N * R * Ra);
+    k_grad_contract<<<dim3(Ra, nsp), 256, 0, c.stream>>>(cond, row_cond, darea, X, Lam, D, N, R, Ra, Gp);
     GPX_LAUNCH_CHECK();
-    c.launches += 1;
+    const int64_t n = (int64_t)Ra * R;
+    k_sum_splits<<<blocks(n, 256), 256, 0, c.stream>>>(Gp, nsp, n, G);
+    GPX_LAUNCH_CHECK();
+    c.launches += 2;
 }
 
 }  // namespace gpx

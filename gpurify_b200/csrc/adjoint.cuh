@@ -1,6 +1,8 @@
 // Launch wrappers of the adjoint-sensitivity and transposed-operator kernels
 // (adjoint.cu).  All arrays are in the plan's leaf-sorted panel order.
 #pragma once
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace gpx {
@@ -20,8 +22,13 @@ void launch_centroid_weights(Ctx& c, const DevPlan& p, const double* dcent, doub
 // PT = transposed near blocks of P (same block layout).
 void launch_near_transpose(Ctx& c, const DevPlan& p, const int32_t* near_rev, const int32_t* near_pre,
                            const double* P, double* PT, int64_t nnz);
-// G (R x R) = sum_k darea_k [cond_k == rhs_cond_i] X[k][j] - Lam^T D.
-void launch_grad_contract(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const double* darea,
-                          const double* X, const double* Lam, const double* D, int64_t N, int R, double* G);
+// Splits of the panel range per row in launch_grad_contract: about two
+// blocks per SM over the Ra rows.
+inline int grad_contract_splits(int Ra) { return std::max(1, std::min(64, 296 / std::max(1, Ra))); }
+// G (Ra x R) = da^T [cond == row] X - Lam^T D over the N panels; Gp is scratch
+// of grad_contract_splits(Ra) x Ra x R doubles.
+void launch_grad_contract(Ctx& c, const int32_t* cond, const int32_t* row_cond, const double* darea,
+                          const double* X, const double* Lam, const double* D, int64_t N, int R, int Ra, double* Gp,
+                          double* G);
 
 }  // namespace gpx

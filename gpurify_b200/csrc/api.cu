@@ -233,7 +233,22 @@ gpx_status gpx_cap_sensitivity(gpx_ctx* ctx, const gpx_panel_problem* pb, const 
     return guarded(ctx, [&] {
         Opts o = normalize(opts);
         cap_sensitivity(ctx->impl, pb->n_panels, pb->verts, pb->conductor, pb->n_conductors, o, n_params,
-                        vert_velocity, maxwell_out, dmaxwell_out, report);
+                        vert_velocity, 0, nullptr, maxwell_out, dmaxwell_out, report);
+    });
+}
+
+gpx_status gpx_cap_sensitivity_rows(gpx_ctx* ctx, const gpx_panel_problem* pb, const gpx_solve_opts* opts,
+                                    int32_t n_params, const double* vert_velocity, int32_t n_rows,
+                                    const int32_t* rows, double* maxwell_out, double* dmaxwell_out,
+                                    gpx_solve_report* report) {
+    if (!ctx || !pb || !maxwell_out || !rows || (n_params > 0 && (!vert_velocity || !dmaxwell_out)))
+        return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
+    if (report) std::memset(report, 0, sizeof(*report));
+    CopyMeter meter(report);
+    return guarded(ctx, [&] {
+        Opts o = normalize(opts);
+        cap_sensitivity(ctx->impl, pb->n_panels, pb->verts, pb->conductor, pb->n_conductors, o, n_params,
+                        vert_velocity, n_rows, rows, maxwell_out, dmaxwell_out, report);
     });
 }
 

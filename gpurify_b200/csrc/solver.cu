@@ -515,6 +515,18 @@ struct Operator {
 
     bool has_far() const { return pl.far && pl.m2l_pairs() > 0; }
 
+    // Frees the near blocks (FP64 and FP32), the block-Jacobi inverses and the
+    // captured applies that read them, once no solve runs with this operator
+    // any more; the far field (apply_far_with) stays usable.
+    void release_near() {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+        P.release();
+        P32.release();
+        bj.Minv.release();
+    }
+
     // Near blocks: the Wilton assembly, or (fwd given) the transpose of the
     // forward operator's blocks; then the preconditioners and the far-field
     // end weights (swapped for the transpose).
@@ -1335,31 +1347,6 @@ __global__ void k_rhs_areas(const int32_t* __restrict__ cond, const double* __re
 
 // C (ncond x ncond) from the solved columns (R x ... device X); columns not
 // solved are filled by symmetry, the unsolved diagonal entry is NaN.
-void maxwell_from_columns(Ctx& ctx, const Prepared& pr, const DBuf<double>& X, int64_t n, int ncond, int Rn, int R,
-                          double* C) {
-    DBuf<double> dC;
-    dC.alloc((size_t)ncond * R, ctx.stream);
-    {
-        KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
-        k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, pr.dp.area.p, X.p, n, R, dC.p);
-        GPX_LAUNCH_CHECK();
-        ctx.launches += 1;
-    }
-    std::vector<double> hc((size_t)ncond * R);
-    dC.download(hc.data(), hc.size());
-    GPX_CUDA(cudaStreamSynchronize(ctx.stream));
-    for (int i = 0; i < ncond; ++i)
-        for (int j = 0; j < ncond; ++j) {
-            double v;
-            if (j < Rn)
-                v = hc[(size_t)i * R + j];
-            else if (i < Rn)
-                v = hc[(size_t)j * R + i];  // substrate column by symmetry
-            else
-                v = std::nan("");
-            C[(size_t)i * ncond + j] = v;
-        }
-}
 
 }  // namespace
 
@@ -1513,7 +1500,8 @@ void potential_matrix(Ctx& ctx, int64_t ns, const double* sv, int64_t nt, const 
 
 
 void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o,
-                     int np, const double* V, double* C, double* dCdp, gpx_solve_report* rep) {
+                     int np, const double* V, int nrows, const int32_t* rows, double* C, double* dCdp,
+                     gpx_solve_report* rep) {
     const double t0 = now_s();
     const int64_t l0 = ctx.launches;
     check_problem(n, verts, cond, ncond, o);
@@ -1523,63 +1511,136 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
     const int depth = choose_depth(o, n, verts);
     const bool dense = depth == 1;
     const int Rn = (!o.skip_ground_rhs || ncond == 1) ? ncond : ncond - 1;
-    if (Rn > 256) throw Error(GPX_ERR_INVALID_ARG, "more than 256 right-hand sides per solve");
-    const int R = (Rn + 3) & ~3;
+    // rows of dC: the listed conductors, or every solved conductor
+    std::vector<int32_t> rowlist;
+    if (rows) {
+        if (nrows < 1 || nrows > Rn) throw Error(GPX_ERR_INVALID_ARG, "gradient rows must list 1 to n_rhs conductors");
+        std::vector<char> seen(Rn, 0);
+        for (int k = 0; k < nrows; ++k) {
+            if (rows[k] < 0 || rows[k] >= Rn || seen[rows[k]])
+                throw Error(GPX_ERR_INVALID_ARG, "gradient row " + std::to_string(rows[k]) +
+                                                     " is not a solved conductor or repeats");
+            seen[rows[k]] = 1;
+            rowlist.push_back(rows[k]);
+        }
+    } else {
+        for (int k = 0; k < Rn; ++k) rowlist.push_back(k);
+    }
+    const int nr = (int)rowlist.size();
+    // Columns (forward solves) and rows (transposed solves) run in chunks of at
+    // most 128 right-hand sides; the forward densities of all columns and the
+    // adjoint densities of all rows stay resident (N x (Rn + nr) doubles).
+    constexpr int kMaxChunk = 128;
+    const int R = (std::min(Rn, kMaxChunk) + 3) & ~3;
+    const int Ra = (std::min(nr, kMaxChunk) + 3) & ~3;
     cudaStream_t s = ctx.stream;
     Prepared pr;
     prepare(ctx, n, verts, cond, ncond, o, R, depth, pr);
     Operator& op = *pr.op;
-    std::vector<int32_t> rhs_cond(R);
-    for (int r = 0; r < R; ++r) rhs_cond[r] = r < Rn ? r : -1;
-    DBuf<int32_t> d_rhs;
-    d_rhs.upload(rhs_cond, s);
-    // forward: P sigma_j = b_j
-    DBuf<double> X;
-    SolveStats st, stT;
-    int outer = 0, outerT = 0;
-    solve_columns(ctx, op, o, dense, pr.dp.cond.p, d_rhs.p, nullptr, R, n, X, st, outer);
-    if (!st.converged)
-        throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge (forward): max relative residual " +
-                                             std::to_string(st.max_resid));
-    maxwell_from_columns(ctx, pr, X, n, ncond, Rn, R, C);
-    // adjoint: P^T lambda_i = q_i
-    Operator opT(ctx, pr.plan, pr.dp, R, o.far_quad, o.precision == GPX_PREC_MIXED, pr.m2l.get());
-    opT.precond = o.precond;
-    opT.mixed_near = o.mixed_near;
-    opT.use_graphs = o.graphs != 0;
-    opT.tc32 = op.tc32;
-    opT.shared = op.shared;
-    opT.p2m_tc = op.p2m_tc;
-    opT.assemble(&op);
-    DBuf<double> Q, Lam;
-    Q.alloc((size_t)n * R, s);
-    {
-        KTimer kt(ctx, K_VEC, 16.0 * (double)n * R, 0.0);
-        k_rhs_areas<<<(unsigned)((n * R + 255) / 256), 256, 0, s>>>(pr.dp.cond.p, pr.dp.area.p, d_rhs.p, n, R, Q.p);
-        GPX_LAUNCH_CHECK();
-        ctx.launches += 1;
-    }
-    solve_columns(ctx, opT, o, dense, pr.dp.cond.p, d_rhs.p, Q.p, R, n, Lam, stT, outerT);
-    op.check_tc();
-    opT.check_tc();
-    if (!stT.converged)
-        throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge (adjoint): max relative residual " +
-                                             std::to_string(stT.max_resid));
-    // per parameter: dC = dq^T sigma - lambda^T (dP sigma)
     const Plan& pl = pr.plan;
-    DBuf<double> dV, dcent, darea, dP, D, dW, dS, G;
+    const double t_assembly = op.t_assembly_s;
+    // forward: P sigma_j = b_j
+    std::vector<DBuf<double>> Xs;
+    std::vector<int32_t> col0;
+    SolveStats st, stT;
+    int outer = 0, outerT = 0, its = 0, itsT = 0;
+    int64_t applies = 0;
+    std::vector<double> hc((size_t)ncond * Rn);
+    {
+        DBuf<int32_t> d_rhs;
+        DBuf<double> dC;
+        dC.alloc((size_t)ncond * R, s);
+        std::vector<double> part((size_t)ncond * R);
+        for (int c0 = 0; c0 < Rn; c0 += R) {
+            const int nc = std::min(R, Rn - c0);
+            std::vector<int32_t> rc(R);
+            for (int r = 0; r < R; ++r) rc[r] = r < nc ? c0 + r : -1;
+            d_rhs.upload(rc, s);
+            Xs.emplace_back();
+            col0.push_back(c0);
+            int oc = 0;
+            solve_columns(ctx, op, o, dense, pr.dp.cond.p, d_rhs.p, nullptr, R, n, Xs.back(), st, oc);
+            if (!st.converged)
+                throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge (forward): max relative residual " +
+                                                     std::to_string(st.max_resid));
+            its = std::max(its, st.iterations);
+            outer = std::max(outer, oc);
+            {
+                KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
+                k_accum_c<<<ncond, 256, 0, s>>>(pr.dp.cond.p, pr.dp.area.p, Xs.back().p, n, R, dC.p);
+                GPX_LAUNCH_CHECK();
+                ctx.launches += 1;
+            }
+            dC.download(part.data(), part.size());
+            GPX_CUDA(cudaStreamSynchronize(s));
+            for (int i = 0; i < ncond; ++i)
+                for (int r = 0; r < nc; ++r) hc[(size_t)i * Rn + c0 + r] = part[(size_t)i * R + r];
+        }
+        op.check_tc();
+    }
+    for (int i = 0; i < ncond; ++i)
+        for (int j = 0; j < ncond; ++j)
+            C[(size_t)i * ncond + j] = j < Rn ? hc[(size_t)i * Rn + j]
+                                              : (i < Rn ? hc[(size_t)j * Rn + i] : std::nan(""));
+    // adjoint: P^T lambda_i = q_i for the gradient rows (its own operator of
+    // width Ra; the forward near blocks are freed once transposed)
+    std::vector<DBuf<double>> Lams;
+    std::vector<DBuf<int32_t>> row_rhs;
+    {
+        std::unique_ptr<Operator> opT(new Operator(ctx, pl, pr.dp, Ra, o.far_quad, o.precision == GPX_PREC_MIXED,
+                                                   pr.m2l.get()));
+        opT->precond = o.precond;
+        opT->mixed_near = o.mixed_near;
+        opT->use_graphs = o.graphs != 0;
+        opT->tc32 = op.tc32;
+        opT->shared = op.shared;
+        opT->p2m_tc = op.p2m_tc;
+        opT->assemble(&op);
+        applies += op.applies + op.applies32;
+        op.release_near();
+        DBuf<double> Q;
+        Q.alloc((size_t)n * Ra, s);
+        for (int k0 = 0; k0 < nr; k0 += Ra) {
+            const int nk = std::min(Ra, nr - k0);
+            std::vector<int32_t> rr(Ra);
+            for (int r = 0; r < Ra; ++r) rr[r] = r < nk ? rowlist[k0 + r] : -1;
+            row_rhs.emplace_back();
+            row_rhs.back().upload(rr, s);
+            {
+                KTimer kt(ctx, K_VEC, 16.0 * (double)n * Ra, 0.0);
+                k_rhs_areas<<<(unsigned)((n * Ra + 255) / 256), 256, 0, s>>>(pr.dp.cond.p, pr.dp.area.p,
+                                                                             row_rhs.back().p, n, Ra, Q.p);
+                GPX_LAUNCH_CHECK();
+                ctx.launches += 1;
+            }
+            Lams.emplace_back();
+            int oc = 0;
+            solve_columns(ctx, *opT, o, dense, pr.dp.cond.p, row_rhs.back().p, Q.p, Ra, n, Lams.back(), stT, oc);
+            if (!stT.converged)
+                throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge (adjoint): max relative residual " +
+                                                     std::to_string(stT.max_resid));
+            itsT = std::max(itsT, stT.iterations);
+            outerT = std::max(outerT, oc);
+        }
+        opT->check_tc();
+        applies += opT->applies + opT->applies32;
+    }
+    // per parameter: dC_ij = dq_i^T sigma_j - lambda_i^T (dP sigma_j)
+    DBuf<double> dV, dcent, darea, dP, D, dW, dS, G, Gp;
     dV.alloc((size_t)n * 12, s);
     dcent.alloc((size_t)n * 3, s);
     darea.alloc((size_t)n, s);
     dP.alloc((size_t)pl.nnz(), s);
     dP.zero();
     D.alloc((size_t)n * R, s);
-    G.alloc((size_t)R * R, s);
+    G.alloc((size_t)Ra * R, s);
+    Gp.alloc((size_t)grad_contract_splits(Ra) * Ra * R, s);
     if (op.has_far()) {
         dW.alloc((size_t)n * pl.n3, s);
         dS.alloc((size_t)n * pl.n3, s);
     }
-    std::vector<double> vs((size_t)n * 12), hg((size_t)R * R);
+    std::vector<double> vs((size_t)n * 12), hg((size_t)Ra * R);
+    for (size_t e = 0; e < (size_t)np * ncond * ncond; ++e) dCdp[e] = std::nan("");
     for (int q = 0; q < np; ++q) {
         const double* Vq = V + (size_t)q * n * 12;
         for (int64_t k = 0; k < n; ++k)
@@ -1587,20 +1648,30 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
         dV.upload(vs, s);
         launch_panel_dprops(ctx, pr.dp.v, dV.p, dcent.p, darea.p);
         launch_near_assemble_dual(ctx, pr.dp.v, pl.nnz(), dV.p, dcent.p, dP.p, kCoulomb);
-        launch_near_apply(ctx, pr.dp.v, pl.nnz(), dP.p, X.p, D.p, R);
         if (op.has_far()) {
             launch_dsrc_weights(ctx, pr.dp.v, o.far_quad, dV.p, dW.p);
-            op.apply_far_with(X.p, D.p, FarWeights<double>{dW.p, false, nullptr, false});
             launch_centroid_weights(ctx, pr.dp.v, dcent.p, dS.p);
-            op.apply_far_with(X.p, D.p, FarWeights<double>{pr.dp.wsrc.p, true, dS.p, false});
         }
-        launch_grad_contract(ctx, pr.dp.cond.p, d_rhs.p, darea.p, X.p, Lam.p, D.p, n, R, G.p);
-        G.download(hg.data(), hg.size());
-        GPX_CUDA(cudaStreamSynchronize(s));
         double* out = dCdp + (size_t)q * ncond * ncond;
-        for (int i = 0; i < ncond; ++i)
-            for (int j = 0; j < ncond; ++j)
-                out[(size_t)i * ncond + j] = (i < Rn && j < Rn) ? hg[(size_t)i * R + j] : std::nan("");
+        for (size_t cc = 0; cc < Xs.size(); ++cc) {
+            const double* X = Xs[cc].p;
+            launch_near_apply(ctx, pr.dp.v, pl.nnz(), dP.p, X, D.p, R);
+            if (op.has_far()) {
+                op.apply_far_with(X, D.p, FarWeights<double>{dW.p, false, nullptr, false});
+                op.apply_far_with(X, D.p, FarWeights<double>{pr.dp.wsrc.p, true, dS.p, false});
+            }
+            const int nc = std::min(R, Rn - col0[cc]);
+            for (size_t rc = 0; rc < Lams.size(); ++rc) {
+                launch_grad_contract(ctx, pr.dp.cond.p, row_rhs[rc].p, darea.p, X, Lams[rc].p, D.p, n, R, Ra, Gp.p,
+                                     G.p);
+                G.download(hg.data(), hg.size());
+                GPX_CUDA(cudaStreamSynchronize(s));
+                const int k0 = (int)rc * Ra, nk = std::min(Ra, nr - k0);
+                for (int a = 0; a < nk; ++a)
+                    for (int j = 0; j < nc; ++j)
+                        out[(size_t)rowlist[k0 + a] * ncond + col0[cc] + j] = hg[(size_t)a * R + j];
+            }
+        }
     }
     const double t1 = now_s();
     if (rep) {
@@ -1614,15 +1685,15 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
         r.n_leaves = pl.nleaf();
         r.nnz_near = pl.near_pairs();
         r.m2l_pairs = pl.m2l_pairs();
-        r.iterations = st.iterations + stT.iterations;
+        r.iterations = its + itsT;
         r.outer_iterations = outer + outerT;
-        r.operator_applies = op.applies + op.applies32 + opT.applies + opT.applies32;
+        r.operator_applies = applies;
         r.max_rel_residual = std::max(st.max_resid, stT.max_resid);
         r.converged = 1;
         r.dense = dense ? 1 : 0;
         r.t_solve_s = t1 - t0;
         r.t_total_s = t1 - t0;
-        r.t_near_assembly_s = op.t_assembly_s;
+        r.t_near_assembly_s = t_assembly;
         r.kernel_launches = ctx.launches - l0;
     }
 }

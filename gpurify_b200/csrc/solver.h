@@ -41,8 +41,12 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
 // (np x n x 12, caller panel order): one forward and one transposed solve
 // (all conductors at once), then one derivative apply per parameter.
 // dCdp: np x ncond x ncond; entries of conductors not solved are NaN.
+// Maxwell matrix and dC/dp along np vertex velocity fields; the rows of dC
+// are the nrows listed conductors (rows null: every solved conductor), the
+// other rows NaN.  Columns and rows are solved in chunks of 128.
 void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o,
-                     int np, const double* V, double* C, double* dCdp, gpx_solve_report* rep);
+                     int np, const double* V, int nrows, const int32_t* rows, double* C, double* dCdp,
+                     gpx_solve_report* rep);
 
 // Autotuner: the fastest far-field configuration (order, depth, far-field
 // source model, near-apply engine) whose sampled operator error against the

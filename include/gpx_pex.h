@@ -21,6 +21,8 @@
  *                            windows; each window is one gpx_cap_solve)
  *   gpx_cap_sensitivity      (no reference counterpart: adjoint dC/dp beside the
  *                            capacitance result of cap/fmm_solver.rs:147-172)
+ *   gpx_cap_sensitivity_rows (no reference counterpart: the same for a subset of
+ *                            conductor rows)
  *   gpx_autotune             (no reference counterpart: replaces the fixed order 4 /
  *                            depth 4 of bridge.rs:403 by a measured choice)
  *   gpx_operator_apply       crates/pex/src/quasistatic/cap/fmm_solver.rs:109-129
@@ -174,10 +176,23 @@ gpx_status gpx_cap_solve_batched(gpx_ctx* ctx, const gpx_panel_problem* problems
  * forward and one transposed solve for all conductors, then one derivative
  * apply per parameter (Wilton near blocks differentiated exactly on dual
  * numbers, far field with differentiated end weights).  With
- * opts.skip_ground_rhs the substrate row and column of dmaxwell_out are NaN. */
+ * opts.skip_ground_rhs the substrate row and column of dmaxwell_out are NaN.
+ * Conductors are solved in chunks of at most 128 right-hand sides (forward
+ * columns and transposed rows alike); the forward charge densities of every
+ * column stay resident for the derivative applies. */
 gpx_status gpx_cap_sensitivity(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
                                int32_t n_params, const double* vert_velocity, double* maxwell_out,
                                double* dmaxwell_out, gpx_solve_report* report);
+/* As gpx_cap_sensitivity, with dC/dp for the n_rows listed conductors only
+ * (rows: distinct solved conductor indices): the transposed solves run for
+ * those rows alone, and the other rows of dmaxwell_out (still n_params x
+ * n_conductors x n_conductors) are NaN.  The forward solve covers every
+ * column, so row i of dC/dp is complete.  Used for gradients of a few nets
+ * of a large block. */
+gpx_status gpx_cap_sensitivity_rows(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
+                                    int32_t n_params, const double* vert_velocity, int32_t n_rows,
+                                    const int32_t* rows, double* maxwell_out, double* dmaxwell_out,
+                                    gpx_solve_report* report);
 
 /* ---- autotuner (no reference counterpart: the reference hard-codes order 4,
  * depth 4, bridge.rs:403) ----

@@ -4,8 +4,9 @@
   5..60 um) solved through the work queue on several streams gives, window by
   window, exactly the Maxwell matrix of a separate gpx_cap_solve call (same
   code path, fixed-order reductions: bit-identical), in FP64 and mixed.
-* Operator applies replayed from captured CUDA graphs give results identical
-  to direct launches and the same kernel count.
+* Operator applies replayed from captured CUDA graphs, and the Arnoldi steps
+  run as a device-side graph loop, give results identical to direct launches
+  and the same iteration count.
 * A failing window names itself and fails the call."""
 import numpy as np
 import pytest
@@ -51,8 +52,12 @@ def test_graph_replay_matches_direct_launches(ctx):
         Cg, rg = ctx.cap_solve(v, c, nc, **kw)
         Cd, rd = ctx.cap_solve(v, c, nc, no_graphs=1, **kw)
         assert np.array_equal(Cg, Cd, equal_nan=True)
-        assert rg["kernel_launches"] == rd["kernel_launches"]
         assert rg["iterations"] == rd["iterations"]
+        # per Arnoldi step the device loop runs its loop-control kernel where
+        # the host-driven loop runs its active-column count; each launch of
+        # the loop graph adds one loop-entry kernel (one per restart cycle)
+        extra = rg["kernel_launches"] - rd["kernel_launches"]
+        assert 0 <= extra <= 4 * max(1, rg["outer_iterations"]), (rg["kernel_launches"], rd["kernel_launches"])
 
 
 def test_batched_error_names_window(ctx):

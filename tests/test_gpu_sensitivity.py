@@ -110,3 +110,38 @@ def test_per_net_sensitivity_api(ctx):
     # the bus wires' coupling to the substrate
     assert res.grad[("width", 1)][1, 1] > 0
     assert res.grad[("height", z0, z1)][0, -1] > 0  # C_ij < 0 off-diagonal: weaker coupling -> less negative
+
+
+def test_row_subset_and_chunked_columns(ctx, orc):
+    """145 conductors (144 plates and no substrate split): forward columns and
+    transposed rows both run in chunks of 128.  dC/dp for a few listed rows
+    (gpx_cap_sensitivity_rows) equals those rows of the full computation and
+    the central differences of the all-pairs solve; unlisted rows are NaN."""
+    verts, cond = [], []
+    for i in range(12):
+        for j in range(12):
+            v, c = orc.plate(i * 0.3, j * 0.3, 0.05 * ((i + j) % 3), 0.2, 0.2, 2, 2, 12 * i + j)
+            verts.append(v)
+            cond.append(c)
+    verts, cond = np.vstack(verts), np.concatenate(cond)
+    nc = 144
+    # parameter: plate 17 lifted along z
+    V = np.zeros((1,) + verts.shape)
+    lift = cond == 17
+    V[0, lift, 2::3] = 1.0
+    kw = dict(dense_below=2**31 - 1, skip_ground_rhs=0)
+    C, dC, rep = ctx.cap_sensitivity(verts, cond, nc, V, **kw)
+    assert rep["n_rhs"] == 144 and rep["converged"] == 1
+    rows = [5, 17, 130]
+    Cs, dCs, _ = ctx.cap_sensitivity(verts, cond, nc, V, grad_rows=rows, **kw)
+    assert np.array_equal(C, Cs)
+    scale = np.abs(dC[0, rows]).max()
+    assert np.abs(dCs[0, rows] - dC[0, rows]).max() <= 1e-10 * scale
+    others = np.setdiff1d(np.arange(nc), rows)
+    assert np.isnan(dCs[0, others]).all()
+    h = 1e-3 * 0.05
+    ref = fd(lambda v: ctx.cap_solve(v, cond, nc, **kw)[0], verts, V[0], h)
+    err = np.abs(dCs[0, rows] - ref[rows]).max() / np.abs(ref[rows]).max()
+    assert err < 1e-5, err
+    with pytest.raises(_lib.GpxError, match="gradient row"):
+        ctx.cap_sensitivity(verts, cond, nc, V, grad_rows=[5, 5], **kw)
