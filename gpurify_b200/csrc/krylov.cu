@@ -17,7 +17,8 @@ constexpr int kRedThreads = 256;
 // Eight vectors A_i per pass over the block's rows: B is read once per eight,
 // and each thread keeps eight independent loads in flight per row.  Each
 // partial sums the same rows in the same order as a one-vector pass.
-__global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restrict__ A, int64_t strideA, int ni,
+template <class TA>
+__global__ void __launch_bounds__(kRedThreads) k_multidot(const TA* __restrict__ A, int64_t strideA, int ni,
                                                           const int32_t* __restrict__ kdev,
                                                           const double* __restrict__ B, int64_t N, int R,
                                                           double* __restrict__ partial) {
@@ -30,7 +31,7 @@ __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restri
     __shared__ double red[kV][kRedThreads];
     for (int i0 = 0; i0 < ni; i0 += kV) {
         const int nv = min(kV, ni - i0);
-        const double* A0 = A + i0 * strideA;
+        const TA* A0 = A + i0 * strideA;
         double acc[kV];
 #pragma unroll
         for (int q = 0; q < kV; ++q) acc[q] = 0.0;
@@ -41,13 +42,13 @@ __global__ void __launch_bounds__(kRedThreads) k_multidot(const double* __restri
                     const int64_t o = n * R + r;
                     const double b = B[o];
 #pragma unroll
-                    for (int q = 0; q < kV; ++q) acc[q] += A0[q * strideA + o] * b;
+                    for (int q = 0; q < kV; ++q) acc[q] += (double)A0[q * strideA + o] * b;
                 }
             } else {
                 for (int64_t n = n0 + sub; n < n1; n += nsub) {
                     const int64_t o = n * R + r;
                     const double b = B[o];
-                    for (int q = 0; q < nv; ++q) acc[q] += A0[q * strideA + o] * b;
+                    for (int q = 0; q < nv; ++q) acc[q] += (double)A0[q * strideA + o] * b;
                 }
             }
         }
@@ -80,26 +81,32 @@ __global__ void k_reduce_blocks(const double* __restrict__ partial, int nblk, in
 }
 
 // W[n][r] -= sum_{i<ni} h[i][r] * V_i[n][r]
-__global__ void k_multi_axpy(const double* __restrict__ V, int64_t strideV, int ni, const int32_t* __restrict__ kdev,
+template <class TV>
+__global__ void k_multi_axpy(const TV* __restrict__ V, int64_t strideV, int ni, const int32_t* __restrict__ kdev,
                              const double* __restrict__ h, double* __restrict__ W, int64_t N, int R) {
     if (kdev) ni = *kdev + 1;
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
     const int r = (int)(o % R);
     double w = W[o];
-    for (int i = 0; i < ni; ++i) w -= h[i * R + r] * V[i * strideV + o];
+    for (int i = 0; i < ni; ++i) w -= h[i * R + r] * (double)V[i * strideV + o];
     W[o] = w;
 }
 
 // dst[n][r] = src[n][r] / s[r] when s[r] > thresh, else src (Arnoldi
-// normalisation with the reference's happy-breakdown rule, krylov.rs:111-115).
+// normalisation with the reference's happy-breakdown rule, krylov.rs:111-115);
+// with `cur` the FP64 value also goes there (the FP32 basis keeps its newest
+// vector in FP64 for the next step's preconditioner).
+template <class TD>
 __global__ void k_scale_cols(const double* __restrict__ src, const double* __restrict__ s, double thresh,
-                             double* __restrict__ dst, DevIndex di, int64_t N, int R) {
+                             TD* __restrict__ dst, DevIndex di, double* __restrict__ cur, int64_t N, int R) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
     dst = dev_offset(dst, di);
     const double d = s[o % R];
-    dst[o] = d > thresh ? src[o] / d : src[o];
+    const double v = d > thresh ? src[o] / d : src[o];
+    dst[o] = (TD)v;
+    if (cur) cur[o] = v;
 }
 
 __global__ void k_sqrt(double* v, int n) {
@@ -118,13 +125,14 @@ __global__ void k_diag_scale(const double* __restrict__ V, DevIndex di, const do
 }
 
 // out[n][r] = sum_i y[i][r] V_i[n][r]
-__global__ void k_lincomb(const double* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ y,
+template <class TV>
+__global__ void k_lincomb(const TV* __restrict__ V, int64_t strideV, int ni, const double* __restrict__ y,
                           double* __restrict__ out, int64_t N, int R) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= N * R) return;
     const int r = (int)(o % R);
     double s = 0.0;
-    for (int i = 0; i < ni; ++i) s += y[i * R + r] * V[i * strideV + o];
+    for (int i = 0; i < ni; ++i) s += y[i * R + r] * (double)V[i * strideV + o];
     out[o] = s;
 }
 
@@ -285,11 +293,12 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 
 int reduce_blocks_for(int64_t N) { return (int)std::min<int64_t>(592, std::max<int64_t>(1, N / 64)); }
 
-void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
-                     double* partial, int nblk, double* out, int accumulate, int tag, const int32_t* kdev) {
+template <class TA>
+void multidot_t(Ctx& c, const TA* A, int64_t strideA, int ni, const double* B, int64_t N, int R, double* partial,
+                int nblk, double* out, int accumulate, int tag, const int32_t* kdev) {
     // with kdev the vector count is *kdev + 1 <= ni, read on the device
     {
-        KTimer t(c, tag, 8.0 * (ni + 1) * (double)N * R, 2.0 * ni * (double)N * R);
+        KTimer t(c, tag, ((double)sizeof(TA) * ni + 8.0) * (double)N * R, 2.0 * ni * (double)N * R);
         k_multidot<<<nblk, kRedThreads, 0, c.stream>>>(A, strideA, ni, kdev, B, N, R, partial);
         GPX_LAUNCH_CHECK();
     }
@@ -302,6 +311,16 @@ void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const dou
     c.launches += 2;
 }
 
+void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
+                     double* partial, int nblk, double* out, int accumulate, int tag, const int32_t* kdev) {
+    multidot_t(c, A, strideA, ni, B, N, R, partial, nblk, out, accumulate, tag, kdev);
+}
+
+void launch_multidot(Ctx& c, const float* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
+                     double* partial, int nblk, double* out, int accumulate, int tag, const int32_t* kdev) {
+    multidot_t(c, A, strideA, ni, B, N, R, partial, nblk, out, accumulate, tag, kdev);
+}
+
 void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, int nblk, double* out) {
     launch_multidot(c, A, 0, 1, A, N, R, partial, nblk, out, 0, K_VEC);
     KTimer t(c, K_SMALL);
@@ -310,28 +329,56 @@ void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, 
     c.launches += 1;
 }
 
-void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
-                      const int32_t* kdev) {
-    KTimer t(c, K_GS_AXPY, 8.0 * (ni + 2) * (double)N * R, 2.0 * ni * (double)N * R);
+template <class TV>
+void multi_axpy_t(Ctx& c, const TV* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
+                  const int32_t* kdev) {
+    KTimer t(c, K_GS_AXPY, ((double)sizeof(TV) * ni + 16.0) * (double)N * R, 2.0 * ni * (double)N * R);
     k_multi_axpy<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, kdev, h, W, N, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
 
+void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
+                      const int32_t* kdev) {
+    multi_axpy_t(c, V, strideV, ni, h, W, N, R, kdev);
+}
+
+void launch_multi_axpy(Ctx& c, const float* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
+                      const int32_t* kdev) {
+    multi_axpy_t(c, V, strideV, ni, h, W, N, R, kdev);
+}
+
 void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R,
                        const DevIndex& di) {
     KTimer t(c, K_VEC, 16.0 * (double)N * R, (double)N * R);
-    k_scale_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(src, sc, thresh, dst, di, N, R);
+    k_scale_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(src, sc, thresh, dst, di, (double*)nullptr, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, float* dst, double* cur, int64_t N,
+                       int R, const DevIndex& di) {
+    KTimer t(c, K_VEC, 20.0 * (double)N * R, (double)N * R);
+    k_scale_cols<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(src, sc, thresh, dst, di, cur, N, R);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+template <class TV>
+void lincomb_t(Ctx& c, const TV* V, int64_t strideV, int ni, const double* y, double* out, int64_t N, int R) {
+    KTimer t(c, K_VEC, ((double)sizeof(TV) * ni + 8.0) * (double)N * R, 2.0 * ni * (double)N * R);
+    k_lincomb<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, y, out, N, R);
     GPX_LAUNCH_CHECK();
     c.launches += 1;
 }
 
 void launch_lincomb(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, double* out, int64_t N,
                     int R) {
-    KTimer t(c, K_VEC, 8.0 * (ni + 1) * (double)N * R, 2.0 * ni * (double)N * R);
-    k_lincomb<<<blocks_for(N * R, 256), 256, 0, c.stream>>>(V, strideV, ni, y, out, N, R);
-    GPX_LAUNCH_CHECK();
-    c.launches += 1;
+    lincomb_t(c, V, strideV, ni, y, out, N, R);
+}
+
+void launch_lincomb(Ctx& c, const float* V, int64_t strideV, int ni, const double* y, double* out, int64_t N, int R) {
+    lincomb_t(c, V, strideV, ni, y, out, N, R);
 }
 
 void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add,

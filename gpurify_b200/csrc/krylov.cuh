@@ -33,18 +33,29 @@ int reduce_blocks_for(int64_t N);
 // Kernels of one Arnoldi step take the step index k either from the host or,
 // for the device-side loop, from device memory (kdev / DevIndex; host
 // arguments then give the launch sizes for the largest k).
+// The basis vectors (A, V) are FP64, or FP32 for the inner solves of the
+// mixed path (products and sums stay FP64).
 void launch_multidot(Ctx& c, const double* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
+                     double* partial, int nblk, double* out, int accumulate, int tag = K_GS_DOT,
+                     const int32_t* kdev = nullptr);
+void launch_multidot(Ctx& c, const float* A, int64_t strideA, int ni, const double* B, int64_t N, int R,
                      double* partial, int nblk, double* out, int accumulate, int tag = K_GS_DOT,
                      const int32_t* kdev = nullptr);
 void launch_colnorm(Ctx& c, const double* A, int64_t N, int R, double* partial, int nblk, double* out);
 void launch_multi_axpy(Ctx& c, const double* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
                        const int32_t* kdev = nullptr);
+void launch_multi_axpy(Ctx& c, const float* V, int64_t strideV, int ni, const double* h, double* W, int64_t N, int R,
+                       const int32_t* kdev = nullptr);
 void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, double* dst, int64_t N, int R,
                        const DevIndex& di = DevIndex());
+// FP32 basis: dst gets the rounded vector, cur (N x R, FP64) the exact one.
+void launch_scale_cols(Ctx& c, const double* src, const double* sc, double thresh, float* dst, double* cur, int64_t N,
+                       int R, const DevIndex& di = DevIndex());
 void launch_diag_scale(Ctx& c, const double* V, const double* d, double* Z, int64_t N, int R, bool add = false,
                        const DevIndex& di = DevIndex());
 void launch_lincomb(Ctx& c, const double* V, int64_t strideV, int ni, const double* y, double* out, int64_t N,
                     int R);
+void launch_lincomb(Ctx& c, const float* V, int64_t strideV, int ni, const double* y, double* out, int64_t N, int R);
 void launch_residual(Ctx& c, const int32_t* cond, const int32_t* rhs_cond, const double* AX, double* Res, int64_t N,
                      int R);
 void launch_sub(Ctx& c, const double* B, const double* AX, double* Res, int64_t n);

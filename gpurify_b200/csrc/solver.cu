@@ -918,6 +918,17 @@ struct ArnoldiGraph {
     }
 };
 
+// Restart length for a Krylov basis of (m + 1) vectors of NR values of
+// elem bytes each: the requested m, cut to what fits in the larger of 16 GB
+// and 45 % of the device memory free at the start of the solve (at least 20).
+int restart_within_budget(int m, int64_t NR, int elem) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    const double budget = std::max(16.0 * (1ull << 30), 0.45 * (double)free_b);
+    const int64_t fit = (int64_t)(budget / ((double)elem * (double)NR)) - 1;
+    return (int)std::max<int64_t>(std::min<int64_t>(20, m), std::min<int64_t>(m, fit));
+}
+
 // Restarted right-preconditioned GMRES(m) on all R columns at once
 // (krylov.rs:50-191 per column); X (N x R) receives the solution.  The
 // right-hand sides are B (N x R) when given, else the unit-conductor vectors
@@ -925,17 +936,25 @@ struct ArnoldiGraph {
 // cycle run as one graph launch (ArnoldiGraph; the first step of the call
 // runs directly, which also does the kernels' one-time set-up); otherwise
 // the host launches each step and reads the active-column count after it.
-void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_t* d_cond,
-                 const int32_t* d_rhs_cond, const double* B, int R, int64_t N, double tol, int m, int max_restarts,
-                 DBuf<double>& X, SolveStats& st, bool reorth = true, bool device_loop = false) {
+// TB is the storage type of the basis: double, or float for the inner
+// solves of the mixed path (every product, sum and Hessenberg entry stays
+// FP64; the newest vector is also kept in FP64 for the next preconditioner
+// apply, so the basis is only rounded where Gram-Schmidt and the final
+// combination read it).
+template <class TB>
+void gmres_multi_t(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_t* d_cond,
+                   const int32_t* d_rhs_cond, const double* B, int R, int64_t N, double tol, int m, int max_restarts,
+                   DBuf<double>& X, SolveStats& st, bool reorth, bool device_loop) {
+    constexpr bool f32 = sizeof(TB) == 4;
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
-    // Krylov basis within a memory budget (16 GB per solve), restart >= 20
-    constexpr double kBasisBudget = 16.0 * (1ull << 30);
-    m = (int)std::max<int64_t>(std::min<int64_t>(20, m), std::min<int64_t>(m, (int64_t)(kBasisBudget / (8.0 * NR)) - 1));
-    DBuf<double> V, W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
+    m = restart_within_budget(m, NR, (int)sizeof(TB));
+    DBuf<TB> V;
+    DBuf<double> Vcur;  // FP32 basis: the newest basis vector in FP64
+    DBuf<double> W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
     DBuf<int32_t> act, done, kused, cnt, kdev;
     V.alloc((size_t)(m + 1) * NR, s);
+    if (f32) Vcur.alloc(NR, s);
     W.alloc(NR, s);
     Z.alloc(NR, s);
     Res.alloc(NR, s);
@@ -978,7 +997,10 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
     // One Arnoldi step: k from the host, or (kd) from device memory.
     auto step = [&](int k, const int32_t* kd) {
         const DevIndex dk{kd, NR, 0}, dk1{kd, NR, 1};
-        Minv(kd ? V.p : V.p + (int64_t)k * NR, Z.p, false, dk);
+        if constexpr (f32)
+            Minv(Vcur.p, Z.p, false, DevIndex());
+        else
+            Minv(kd ? V.p : V.p + (int64_t)k * NR, Z.p, false, dk);
         A(Z.p, W.p);
         const int ni = kd ? m : k + 1;  // launch sizes cover the largest k
         launch_multidot(ctx, V.p, NR, ni, W.p, N, R, partial.p, nblk, h1.p, 0, K_GS_DOT, kd);
@@ -988,7 +1010,10 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
             launch_multi_axpy(ctx, V.p, NR, ni, h2.p, W.p, N, R, kd);
         }
         launch_colnorm(ctx, W.p, N, R, partial.p, nblk, hnorm.p);
-        launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, kd ? V.p : V.p + (int64_t)(k + 1) * NR, N, R, dk1);
+        if constexpr (f32)
+            launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, kd ? V.p : V.p + (int64_t)(k + 1) * NR, Vcur.p, N, R, dk1);
+        else
+            launch_scale_cols(ctx, W.p, hnorm.p, 1e-14, kd ? V.p : V.p + (int64_t)(k + 1) * NR, N, R, dk1);
         launch_givens(ctx, gd, k, kd);
     };
     ArnoldiGraph loop;
@@ -1062,7 +1087,10 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
         st.cycles = cycle + 1;
         launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, beta.p);
         launch_cycle_start(ctx, gd, beta.p);
-        launch_scale_cols(ctx, Res.p, beta.p, 0.0, V.p, N, R);
+        if constexpr (f32)
+            launch_scale_cols(ctx, Res.p, beta.p, 0.0, V.p, Vcur.p, N, R);
+        else
+            launch_scale_cols(ctx, Res.p, beta.p, 0.0, V.p, N, R);
         if (read_count(act.p, false) == 0) break;
         int kmax = 0;
         if (device_loop && !loop.exec) {
@@ -1114,6 +1142,17 @@ void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_
     }
 }
 
+void gmres_multi(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int32_t* d_cond,
+                 const int32_t* d_rhs_cond, const double* B, int R, int64_t N, double tol, int m, int max_restarts,
+                 DBuf<double>& X, SolveStats& st, bool reorth = true, bool device_loop = false, bool basis32 = false) {
+    if (basis32)
+        gmres_multi_t<float>(ctx, A, Minv, d_cond, d_rhs_cond, B, R, N, tol, m, max_restarts, X, st, reorth,
+                             device_loop);
+    else
+        gmres_multi_t<double>(ctx, A, Minv, d_cond, d_rhs_cond, B, R, N, tol, m, max_restarts, X, st, reorth,
+                              device_loop);
+}
+
 }  // namespace
 
 Opts normalize(const gpx_solve_opts* o) {
@@ -1143,6 +1182,7 @@ Opts normalize(const gpx_solve_opts* o) {
     r.col_begin = o->col_begin;
     r.col_count = o->col_count;
     r.mixed_far_tc = o->mixed_far_tc;
+    r.inner_basis32 = o->inner_basis64 ? 0 : 1;
     return r;
 }
 
@@ -1192,6 +1232,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.mixed_near < 0 || o.mixed_near > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1 or 2");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
     if (o.mixed_far_tc != 0 && o.mixed_far_tc != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_far_tc must be 0 or 1");
+    if (o.inner_basis32 != 0 && o.inner_basis32 != 1) throw Error(GPX_ERR_INVALID_ARG, "inner_basis64 must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -1294,13 +1335,14 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         const double need = 0.3 * o.tol / std::max(st.max_resid, 1e-300);
         const double inner_tol = std::min(0.1, std::max(need, floor_tol));
         SolveStats in;
-        // Inner solves stop at 1e-3..1e-5: one classical Gram-Schmidt pass (FP64) keeps the
-        // basis orthogonal far below that, so the re-orthogonalisation pass is skipped.
+        // Inner solves stop at 1e-3..1e-5: one classical Gram-Schmidt pass keeps the basis
+        // orthogonal far below that, so the re-orthogonalisation pass is skipped; for the
+        // same reason the basis may be stored in FP32 (half the Gram-Schmidt traffic).
         const PrecondFn pc = [&](const double* v, double* z, bool add, const DevIndex& di) {
             op.precondition(v, z, add, di);
         };
         gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, std::min(o.max_restarts, 3), D, in,
-                    false, o.graphs != 0 && !ctx.profile);
+                    false, o.graphs != 0 && !ctx.profile, o.inner_basis32 != 0);
         st.iterations += in.iterations;
         launch_add(ctx, X.p, D.p, NR);
         op.apply(X.p, W.p);

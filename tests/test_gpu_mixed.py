@@ -118,6 +118,25 @@ def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near, mixed_m2l):
     assert err.max() < 1e-6, err.max()
 
 
+@pytest.mark.parametrize("mixed_near", [0, 2])
+def test_fp32_inner_basis_matches_fp64_basis(ctx, mixed_near):
+    """The inner GMRES basis stored in FP32 (the default) against the FP64
+    basis (inner_basis64): both refinements meet the FP64 tolerance and give
+    the same Maxwell matrix to well inside it."""
+    p = window()
+    nc = len(p["nets"]) + 1
+    kw = dict(order=5, max_level=5, dense_below=-1, far_quad=1, skip_ground_rhs=1, precision=1, precond=1,
+              mixed_near=mixed_near)
+    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, **kw)
+    C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, inner_basis64=1, **kw)
+    assert r32["converged"] == 1 and r64["converged"] == 1
+    assert r32["max_rel_residual"] <= 1e-8
+    R = nc - 1
+    d = np.abs(np.diag(C64[:R, :R]))
+    assert (np.abs(C32[:R, :R] - C64[:R, :R]) / d[:, None]).max() < 1e-7
+    assert r32["iterations"] <= 1.25 * r64["iterations"] + 4, (r32["iterations"], r64["iterations"])
+
+
 def test_mixed_two_wire_small_rhs(ctx):
     lay = layouts.two_wires()
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly)
