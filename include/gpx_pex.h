@@ -125,8 +125,9 @@ typedef struct {
     int32_t mixed_far_tc;    /* mixed, orders 4 and 5, tensor-core near apply: 1 -> P2M and L2P on the tensor
                                 cores too (weights, charges and local expansions split into TF32 hi and lo
                                 parts, FP32-accurate) */
-    int32_t inner_basis64;   /* mixed: 1 -> inner GMRES basis stored in FP64; 0 -> stored in FP32 (products,
-                                sums and the Hessenberg matrix stay FP64) */
+    int32_t inner_basis32;   /* mixed: 1 -> inner GMRES basis stored in FP32 (products, sums and the
+                                Hessenberg matrix stay FP64): twice the restart length in the same memory,
+                                for inner tolerances of 1e-3 (TF32 near apply); 0 -> FP64 */
     int32_t reserved;        /* 0 */
 } gpx_solve_opts;
 

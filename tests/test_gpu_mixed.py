@@ -66,15 +66,17 @@ def test_mixed_operator_close_to_fp64_high_order(ctx, order, m2l_mode, mixed_m2l
 
 
 @pytest.mark.parametrize("order,far_quad,mixed_m2l,mixed_near", [(4, 1, 1, 2), (5, 0, 1, 2), (5, 1, 1, 2),
-                                                                  (4, 1, 0, 0), (5, 1, 2, 0), (5, 1, 3, 0)])
+                                                                  (4, 1, 0, 0), (5, 0, 0, 0), (5, 1, 3, 0)])
 def test_tensor_core_p2m_l2p_match_cuda_cores(ctx, order, far_quad, mixed_m2l, mixed_near):
     """The tensor-core P2M and L2P (weights, charges and local expansions split
-    into TF32 hi and lo parts, about 2^-21) against the FP32 CUDA-core P2M and
-    L2P.  With a linear, FP32-accurate rest of the operator (factored FP32 M2L,
-    near blocks split hi/lo) the two operators agree to well below 1e-5.  A
-    single-pass TF32 M2L rounds its inputs, so there the two differ by up to
-    that M2L's own error, and both stay within the FP32 operator's bar against
-    FP64."""
+    into TF32 hi and lo parts, about 2^-21, the weights split from FP64)
+    against the FP32 CUDA-core P2M and L2P.  With a linear, FP32-accurate rest
+    of the operator (factored FP32 M2L, near blocks split hi/lo) the two
+    agree to 5e-5 and the tensor-core one is at least as close to FP64: with
+    Gauss-point sources the FP32 weight products lose digits to cancellation
+    that the split keeps.  A single-pass TF32 M2L rounds its inputs, so there
+    both stay within the FP32 operator's bar against FP64 (centroid sources;
+    with Gauss sources that M2L alone loses 1e-2 on this window)."""
     p = window()
     rng = np.random.default_rng(6)
     sig = rng.standard_normal((len(p["verts"]), 64))
@@ -83,10 +85,13 @@ def test_tensor_core_p2m_l2p_match_cuda_cores(ctx, order, far_quad, mixed_m2l, m
     y0, _ = ctx.operator_apply(p["verts"], sig, **kw)
     y1, _ = ctx.operator_apply(p["verts"], sig, mixed_far_tc=1, **kw)
     y64, _ = ctx.operator_apply(p["verts"], sig, **dict(kw, precision=0, mixed_m2l=0, mixed_near=0))
+    n64 = np.linalg.norm(y64, axis=0)
     d01 = np.linalg.norm(y1 - y0, axis=0) / np.linalg.norm(y0, axis=0)
-    e1 = np.linalg.norm(y1 - y64, axis=0) / np.linalg.norm(y64, axis=0)
+    e0 = np.linalg.norm(y0 - y64, axis=0) / n64
+    e1 = np.linalg.norm(y1 - y64, axis=0) / n64
     if mixed_m2l == 1:
-        assert d01.max() < 5e-6, d01.max()
+        assert d01.max() < 5e-5, d01.max()
+        assert e1.max() <= 1.05 * e0.max() + 1e-7, (e1.max(), e0.max())
         assert e1.max() < 1e-4, e1.max()
     else:
         assert e1.max() < (2e-3 if mixed_m2l == 3 else 1e-3), e1.max()
@@ -118,17 +123,17 @@ def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near, mixed_m2l):
     assert err.max() < 1e-6, err.max()
 
 
-@pytest.mark.parametrize("mixed_near", [0, 2])
-def test_fp32_inner_basis_matches_fp64_basis(ctx, mixed_near):
-    """The inner GMRES basis stored in FP32 (the default) against the FP64
-    basis (inner_basis64): both refinements meet the FP64 tolerance and give
-    the same Maxwell matrix to well inside it."""
+def test_fp32_inner_basis_matches_fp64_basis(ctx):
+    """The inner GMRES basis stored in FP32 (inner_basis32, for solves whose
+    basis would not fit otherwise) against the default FP64 basis, with the
+    TF32 near apply (inner tolerance floor 1e-3): both refinements meet the
+    FP64 tolerance and give the same Maxwell matrix to well inside it."""
     p = window()
     nc = len(p["nets"]) + 1
     kw = dict(order=5, max_level=5, dense_below=-1, far_quad=1, skip_ground_rhs=1, precision=1, precond=1,
-              mixed_near=mixed_near)
-    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, **kw)
-    C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, inner_basis64=1, **kw)
+              mixed_near=0)
+    C64, r64 = ctx.cap_solve(p["verts"], p["cond"], nc, **kw)
+    C32, r32 = ctx.cap_solve(p["verts"], p["cond"], nc, inner_basis32=1, **kw)
     assert r32["converged"] == 1 and r64["converged"] == 1
     assert r32["max_rel_residual"] <= 1e-8
     R = nc - 1
