@@ -171,15 +171,18 @@ __global__ void k_givens(GmresDev g, int k, const int32_t* __restrict__ kdev) {
     if (!g.act[r]) return;
     double* H = g.H;  // H[(i*m + k)*R + r]
     auto h = [&](int i) -> double& { return H[((int64_t)i * m + k) * R + r]; };
-    for (int i = 0; i <= k; ++i) h(i) = g.h1[i * R + r] + g.h2[i * R + r];
-    h(k + 1) = g.hnorm[r];
+    // Apply the earlier rotations to the new column.  Only the running entry
+    // is carried from one rotation to the next (in a register); the loads of
+    // each step do not depend on the previous one, so they overlap.
+    double cur = g.h1[r] + g.h2[r];
+#pragma unroll 4
     for (int i = 0; i < k; ++i) {
         const double cs = g.cs[i * R + r], sn = g.sn[i * R + r];
-        const double t = cs * h(i) + sn * h(i + 1);
-        h(i + 1) = -sn * h(i) + cs * h(i + 1);
-        h(i) = t;
+        const double nx = g.h1[(i + 1) * R + r] + g.h2[(i + 1) * R + r];
+        h(i) = cs * cur + sn * nx;
+        cur = -sn * cur + cs * nx;
     }
-    const double a = h(k), b = h(k + 1);
+    const double a = cur, b = g.hnorm[r];
     double c, s;
     if (b == 0.0) {
         c = 1.0;

@@ -140,6 +140,90 @@ __global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ 
     }
 }
 
+// FP32 form for the inner solves of the mixed path (an approximate inverse
+// there anyway): Minv32 rounded once from the FP64 inverses, V read as FP64
+// and rounded on load, FP32 products, Z written (or added) as FP64.  One CTA
+// per (block, 64-column chunk), thread (ty, tx) holds rows ty + 16 a and
+// columns 4 tx .. 4 tx + 3 (so V and Z move as 32-byte rows per thread).
+template <int kB>
+__global__ void __launch_bounds__(256) k_block_apply32(const float* __restrict__ Minv,
+                                                       const int64_t* __restrict__ blk_start,
+                                                       const int32_t* __restrict__ blk_size,
+                                                       const double* __restrict__ V, DevIndex di,
+                                                       double* __restrict__ Z, int R, int add) {
+    constexpr int RA = kB / 16;
+    V = dev_offset(V, di);
+    const int bi = blockIdx.x;
+    const int rc = blockIdx.y * 64;
+    const int64_t s0 = blk_start[bi];
+    const int b = blk_size[bi];
+    extern __shared__ float bj32_smem[];
+    float(*Ms)[kB + 1] = reinterpret_cast<float(*)[kB + 1]>(bj32_smem);
+    float4* Vs = reinterpret_cast<float4*>(bj32_smem + ((kB * (kB + 1) + 3) & ~3));  // [kB][16]
+    const float* M = Minv + (int64_t)bi * kB * kB;
+    for (int e = threadIdx.x; e < kB * kB; e += blockDim.x) Ms[e / kB][e % kB] = M[e];
+    for (int e = threadIdx.x; e < kB * 16; e += blockDim.x) {
+        const int i = e >> 4, c = 4 * (e & 15);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < b) {
+            const double* src = V + (s0 + i) * R + rc + c;
+            if (rc + c + 3 < R) {
+                const double2 a = *reinterpret_cast<const double2*>(src);
+                const double2 bb = *reinterpret_cast<const double2*>(src + 2);
+                v = make_float4((float)a.x, (float)a.y, (float)bb.x, (float)bb.y);
+            } else {
+                float t[4] = {0.f, 0.f, 0.f, 0.f};
+                for (int q = 0; q < 4; ++q)
+                    if (rc + c + q < R) t[q] = (float)src[q];
+                v = make_float4(t[0], t[1], t[2], t[3]);
+            }
+        }
+        Vs[e] = v;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[RA][4];
+#pragma unroll
+    for (int a = 0; a < RA; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[a][q] = 0.f;
+    for (int k = 0; k < b; ++k) {
+        const float4 v = Vs[k * 16 + tx];
+#pragma unroll
+        for (int a = 0; a < RA; ++a) {
+            const float m = Ms[ty + 16 * a][k];
+            acc[a][0] = fmaf(m, v.x, acc[a][0]);
+            acc[a][1] = fmaf(m, v.y, acc[a][1]);
+            acc[a][2] = fmaf(m, v.z, acc[a][2]);
+            acc[a][3] = fmaf(m, v.w, acc[a][3]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < RA; ++a) {
+        const int i = ty + 16 * a;
+        if (i >= b) continue;
+        const int c = rc + 4 * tx;
+        double* z = Z + (s0 + i) * R + c;
+        if (c + 3 < R) {
+            double2 z0 = make_double2(acc[a][0], acc[a][1]), z1 = make_double2(acc[a][2], acc[a][3]);
+            if (add) {
+                const double2 o0 = *reinterpret_cast<const double2*>(z), o1 = *reinterpret_cast<const double2*>(z + 2);
+                z0.x += o0.x, z0.y += o0.y, z1.x += o1.x, z1.y += o1.y;
+            }
+            *reinterpret_cast<double2*>(z) = z0;
+            *reinterpret_cast<double2*>(z + 2) = z1;
+        } else {
+            for (int q = 0; q < 4; ++q)
+                if (c + q < R) z[q] = add ? z[q] + (double)acc[a][q] : (double)acc[a][q];
+        }
+    }
+}
+
+__global__ void k_round_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
 }  // namespace
 
 void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double* P) {
@@ -176,6 +260,32 @@ void BlockJacobi::build(Ctx& c, const Plan& pl, const DevPlan& dp, const double*
         GPX_LAUNCH_CHECK();
         c.launches += 1;
     }
+}
+
+void BlockJacobi::make_f32(Ctx& c) {
+    const int64_t n = (int64_t)nblk * block * block;
+    Minv32.alloc((size_t)n, c.stream);
+    KTimer t(c, K_VEC, 12.0 * n, 0.0);
+    k_round_f32<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c.stream>>>(Minv.p, Minv32.p, n);
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
+}
+
+void BlockJacobi::apply32(Ctx& c, const double* V, double* Z, int64_t N, int R, bool add, const DevIndex& di) const {
+    if (R % 4 != 0) throw Error(GPX_ERR_INTERNAL, "FP32 block-Jacobi apply needs R % 4 == 0");
+    const int kB = block;
+    KTimer t(c, K_VEC, 16.0 * N * R + 4.0 * (double)nblk * kB * kB, 2.0 * (double)N * kB * R);
+    const int smem = (int)(sizeof(float) * (((kB * (kB + 1) + 3) & ~3) + kB * 64));
+    const dim3 g(nblk, (R + 63) / 64);
+    if (kB == 96) {
+        set_smem_once(k_block_apply32<96>, smem);
+        k_block_apply32<96><<<g, 256, smem, c.stream>>>(Minv32.p, d_start.p, d_size.p, V, di, Z, R, add ? 1 : 0);
+    } else {
+        set_smem_once(k_block_apply32<48>, smem);
+        k_block_apply32<48><<<g, 256, smem, c.stream>>>(Minv32.p, d_start.p, d_size.p, V, di, Z, R, add ? 1 : 0);
+    }
+    GPX_LAUNCH_CHECK();
+    c.launches += 1;
 }
 
 void BlockJacobi::check(Ctx& c) const {

@@ -525,6 +525,7 @@ struct Operator {
         P.release();
         P32.release();
         bj.Minv.release();
+        bj.Minv32.release();
     }
 
     // Near blocks: the Wilton assembly, or (fwd given) the transpose of the
@@ -549,6 +550,7 @@ struct Operator {
         if (precond >= 1) {
             bj.block = precond == 2 ? 96 : 48;
             bj.build(ctx, pl, d.v, P.p);
+            if (mixed) bj.make_f32(ctx);  // every GMRES of the mixed path is an inner solve
         }
         // The host-side set-up below (far-field lists) runs while the device
         // assembles; the assembly time and the preconditioner check are read
@@ -835,7 +837,9 @@ struct Operator {
     // Z (+)= M^-1 V with the chosen right preconditioner (V offset on the
     // device by di when given).
     void precondition(const double* V, double* Z, bool add, const DevIndex& di = DevIndex()) {
-        if (precond >= 1)
+        if (precond >= 1 && mixed)
+            bj.apply32(ctx, V, Z, pl.N, R, add, di);
+        else if (precond >= 1)
             bj.apply(ctx, V, Z, pl.N, R, add, di);
         else
             launch_diag_scale(ctx, V, inv_diag.p, Z, pl.N, R, add, di);
