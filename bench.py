@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--block-side", type=float, default=200.0, help="block workload: side in um")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every kernel directly (no CUDA graphs, no device-side Arnoldi loop); for profilers "
+                         "that list kernel launches")
     return ap.parse_args()
 
 
@@ -420,11 +423,13 @@ def time_solves(ctx, verts, cond, ncond, solve_kw, steps, warmup, stream, dist, 
 
 
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) on the 20 um / 36k-panel window, per unit of the
-# kernel's algorithmic work, so that bench scales them by the work of the
-# launch it times: near apply per stored near entry (its algorithmic bytes are
-# 4 B per entry plus the right-hand sides), M2L per box pair.
-TRAFFIC_PER_ALGO_BYTE = {}
+# dram__bytes_write.sum, one --set full capture of two launches of each
+# kernel on this bench window, cold cache) divided by the launch's
+# algorithmic bytes as this bench counts them (near apply: 4 B per stored
+# near entry plus 16 B per panel and right-hand side; M2L: each box's
+# expansion read once and its local expansion written once).  bench scales
+# the ratio by the algorithmic bytes of the launches it times.
+TRAFFIC_PER_ALGO_BYTE = {"near_apply": 1.163, "m2l": 0.968}
 
 
 def roofline_of(ks, ms_total, m2l_engine):
@@ -525,7 +530,9 @@ def run_workload(args):
         V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params)
         rows = sorted(int(r) for r in np.random.default_rng(16).choice(nc - 1, min(16, nc - 1), replace=False))
         out.update(panels=len(p["verts"]), rhs=nc - 1, params=len(params), gradient_nets=rows)
-        kw = dict(base, precision=_lib.PREC_MIXED, precond=1)
+        # FP32 inner basis: twice the restart length in the memory left beside
+        # the 53 GB of near blocks (GMRES(20) stalls on this problem)
+        kw = dict(base, precision=_lib.PREC_MIXED, precond=1, inner_basis32=1)
         free0, total = torch.cuda.mem_get_info(0)
         with DeviceMemoryWatch() as mw:
             dt0, (C, rep) = timed(lambda: ctx.cap_solve(p["verts"], p["cond"], nc, **kw), 1)
@@ -599,7 +606,8 @@ def main():
     ctx = _lib.Context(local)
     base_kw = dict(order=args.order, max_level=args.depth, skip_ground_rhs=1, tol=1e-8, restart=args.restart,
                    far_quad=args.far_quad, precond=args.precond, inner_tol_exp=args.inner_tol_exp,
-                   mixed_near=args.mixed_near, m2l_mode=args.m2l_mode, mixed_m2l=args.mixed_m2l)
+                   mixed_near=args.mixed_near, m2l_mode=args.m2l_mode, mixed_m2l=args.mixed_m2l,
+                   no_graphs=1 if args.no_graphs else 0)
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     lay = workload(rank, args.nets, args.side)
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,

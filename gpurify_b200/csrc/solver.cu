@@ -925,11 +925,11 @@ struct ArnoldiGraph {
 
 // Restart length for a Krylov basis of (m + 1) vectors of NR values of
 // elem bytes each: the requested m, cut to what fits in the larger of 16 GB
-// and 45 % of the device memory free at the start of the solve (at least 20).
+// and 60 % of the device memory free at the start of the solve (at least 20).
 int restart_within_budget(int m, int64_t NR, int elem) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
-    const double budget = std::max(16.0 * (1ull << 30), 0.45 * (double)free_b);
+    const double budget = std::max(16.0 * (1ull << 30), 0.6 * (double)free_b);
     const int64_t fit = (int64_t)(budget / ((double)elem * (double)NR)) - 1;
     return (int)std::max<int64_t>(std::min<int64_t>(20, m), std::min<int64_t>(m, fit));
 }
