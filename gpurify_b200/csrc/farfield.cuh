@@ -112,13 +112,16 @@ void launch_m2l_tc(Ctx& c, const TcLevel& lv, int ns, const float* E, float* L, 
                    const double* box_scale, int* err);
 
 // Shared-basis M2L (SharedBasis in plan.h), rank kShared: expansion rows
-// (box, right-hand side) [row0, row0 + nrows) compressed, E^ = V^T E (Vpad:
-// ns x kShared, V with zero rows past n3), and decompressed, L = U L^ (Utpad:
-// kShared x round_up(ns, 64), U^T with zero columns past n3).  E / L rows have
-// stride ns, E^ / L^ rows stride kShared.  FP32 on the CUDA cores.
+// (box, right-hand side) [row0, row0 + nrows) compressed, E^ = V^T E, and
+// decompressed, L = U L^, on the tensor cores with both operands split into
+// TF32 hi and lo parts.  Vt_hi / Vt_lo: kShared x ns (V^T, zero columns past
+// n3); U_hi / U_lo: round_up(ns, 64) x kShared (U, zero rows past n3).  E / L
+// rows have stride ns, E^ / L^ rows stride kShared.  *err becomes nonzero if
+// a bounded pipeline wait expired.
 constexpr int kShared = 64;
-void launch_m2l_compress(Ctx& c, const float* E, int ns, const float* Vpad, float* Eh, int64_t row0, int64_t nrows);
-void launch_m2l_decompress(Ctx& c, const float* Lh, const float* Utpad, int ns, float* L, int64_t row0,
-                           int64_t nrows);
+void launch_m2l_compress(Ctx& c, const float* E, int ns, const float* Vt_hi, const float* Vt_lo, float* Eh,
+                         int64_t row0, int64_t nrows, int* err);
+void launch_m2l_decompress(Ctx& c, const float* Lh, const float* U_hi, const float* U_lo, int ns, float* L,
+                           int64_t row0, int64_t nrows, int* err);
 
 }  // namespace gpx

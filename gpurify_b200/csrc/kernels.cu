@@ -22,7 +22,7 @@ constexpr int kAsmTile = 64;
 
 // One CTA per work item (target leaf, <= 64 rows): rows of the leaf's
 // P block m_t x S_t, row-major.
-__global__ void __launch_bounds__(kAsmThreads) k_near_assemble(DevPlan p, double* __restrict__ P, double coef) {
+__global__ void __launch_bounds__(kAsmThreads, 2) k_near_assemble(DevPlan p, double* __restrict__ P, double coef) {
     const int t = p.item_leaf[blockIdx.x];
     const int r0 = p.item_row0[blockIdx.x];
     const int64_t tb = p.leaf_begin[t];

@@ -103,7 +103,8 @@ void launch_to_f32(Ctx& c, const double* a, float* b, int64_t n);
 void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n);
 // Y = P_near X on the tensor cores (TF32 inputs, FP32 accumulation, FP64 Y),
 // work items of <= 128 rows (it_leaf, it_row0); P holds TF32-rounded values;
-// X is given as its TF32 split Xhi + Xlo (launch_split_tf32); R a multiple
+// X is given as its TF32 split Xhi + Xlo (launch_split_tf32), or with Xlo
+// null as its FP32 copy in Xhi, split into hi and lo on chip; R a multiple
 // of 4.  *err becomes nonzero if a bounded pipeline wait expired.
 // split_p: P holds full FP32 values and is split into TF32 hi and lo parts on
 // chip (three products instead of two; accurate to about 2^-21 in P too).

@@ -42,10 +42,15 @@ constexpr int kProducers = 128;            // four producer warps, also the epil
 constexpr int kThreads = kProducers + 32;  // + the MMA warp
 constexpr uint32_t kATile = 128 * 128;      // 128 rows x 128 B
 constexpr uint32_t kBTile = 32 * 256;       // 32 K rows x 64 FP32
-// Stage layout: A, [A_lo when P is split], B_hi, B_lo.  Without the split a
-// stage is 32 KB and three stages fit twice per SM; with it 48 KB and two.
-template <bool SP>
+// Operand modes: 0 = P (TF32) and the split X_hi, X_lo gathered from global
+// memory; 1 = P kept in FP32 and split into hi and lo on chip (three
+// products); 2 = X gathered once as FP32 and split into hi and lo on chip
+// (half the gather traffic of mode 0, the same products).
+// Stage layout: A, [A_lo in mode 1], B_hi, B_lo.  Modes 0 and 2 stage 32 KB
+// and three stages fit twice per SM; mode 1 stages 48 KB, two stages.
+template <int MODE>
 struct NearCfg {
+    static constexpr bool SP = MODE == 1;
     static constexpr int kStages = SP ? 2 : 3;
     static constexpr uint32_t kALo = kATile;                          // offset of A_lo (SP)
     static constexpr uint32_t kBOff = SP ? 2 * kATile : kATile;       // offset of B_hi
@@ -137,18 +142,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
-// SP (split P): P holds full FP32 values; the producers split each staged A
-// tile into TF32 hi (in place) and lo (A_lo) parts once its copies landed,
-// and the MMA thread adds the third product A_lo B_hi, so the near apply is
-// accurate to about 2^-21 in both P and X.
-template <bool SP>
+// Mode 1 (split P): P holds full FP32 values; the producers split each
+// staged A tile into TF32 hi (in place) and lo (A_lo) parts once its copies
+// landed, and the MMA thread adds the third product A_lo B_hi, so the near
+// apply is accurate to about 2^-21 in both P and X.  Mode 2 (split X on
+// chip): Xhi is the FP32 copy of X, Xlo is unused; each producer splits the
+// B chunks it copied once they landed.  In modes 1 and 2 a producer signals
+// a stage after its own copies of that stage completed and were split (one
+// stage of copies stays in flight per producer); in mode 0 the copies
+// signal the stage themselves.
+template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int32_t* __restrict__ it_leaf,
                                                             const int32_t* __restrict__ it_row0,
                                                             const float* __restrict__ P,
                                                             const float* __restrict__ Xhi,
                                                             const float* __restrict__ Xlo, double* __restrict__ Y,
                                                             int R, int* __restrict__ err) {
-    using Cfg = NearCfg<SP>;
+    using Cfg = NearCfg<MODE>;
+    constexpr bool SP = Cfg::SP;
+    constexpr bool SB = MODE == 2;
     constexpr int kStages = Cfg::kStages;
     constexpr uint32_t kStage = Cfg::kStage;
     extern __shared__ uint8_t smem_raw[];
@@ -216,7 +228,25 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[sst])) : "memory");
         };
-        int signalled = 0;  // SP: stages split and signalled
+        // SB: split the B chunks this thread copied into stage `jj` (K row kb,
+        // chunks q0 .. q0 + 3: FP32 x into hi in place and lo beside it).
+        auto split_b_and_signal = [&](int jj) {
+            const int sst = jj % kStages;
+            uint8_t* bt = sbase + (size_t)sst * kStage + Cfg::kBOff;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint32_t d = swz_mn((uint32_t)kb, (uint32_t)(q0 + i));
+                float4* hp = reinterpret_cast<float4*>(bt + d);
+                float4* lp = reinterpret_cast<float4*>(bt + kBTile + d);
+                const float4 v = *hp;
+                const float4 h = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
+                *lp = make_float4(to_tf32(v.x - h.x), to_tf32(v.y - h.y), to_tf32(v.z - h.z), to_tf32(v.w - h.w));
+                *hp = h;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[sst])) : "memory");
+        };
+        int signalled = 0;  // modes 1 and 2: stages split and signalled
         for (int j = 0; j < nsl; ++j) {
             const int st = j % kStages;
             if (j >= kStages && !mbar_wait(smem_u32(&empty[st]), (uint32_t)(((j / kStages) - 1) & 1))) {
@@ -249,13 +279,16 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
                 const int64_t off = ok ? gid * R + col : 0;
                 const uint32_t d = swz_mn((uint32_t)kb, (uint32_t)q);
                 cp16(bh + d, Xhi + off, ok);
-                cp16(bl + d, Xlo + off, ok);
+                if constexpr (!SB) cp16(bl + d, Xlo + off, ok);
             }
-            if constexpr (SP) {
+            if constexpr (SP || SB) {
                 asm volatile("cp.async.commit_group;" ::: "memory");
                 if (j >= 1) {
                     asm volatile("cp.async.wait_group 1;" ::: "memory");
-                    split_and_signal(j - 1);
+                    if constexpr (SP)
+                        split_and_signal(j - 1);
+                    else
+                        split_b_and_signal(j - 1);
                     signalled = j;
                 }
             } else {
@@ -264,12 +297,17 @@ __global__ void __launch_bounds__(kThreads) k_near_apply_tc(DevPlan p, const int
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-        if constexpr (SP) {
+        if constexpr (SP || SB) {
             // the last issued stage (also after an expired wait: every
             // issued stage is signalled, so the MMA thread never waits on a
             // stage whose copies went out)
             const int issued_p = *(volatile int*)&s_bad ? signalled + 1 : nsl;
-            for (int jj = signalled; jj < issued_p && jj < nsl; ++jj) split_and_signal(jj);
+            for (int jj = signalled; jj < issued_p && jj < nsl; ++jj) {
+                if constexpr (SP)
+                    split_and_signal(jj);
+                else
+                    split_b_and_signal(jj);
+            }
         }
     } else if (tid == kProducers) {
         int issued = 0;
@@ -370,23 +408,28 @@ void launch_to_tf32(Ctx& c, const double* a, float* b, int64_t n) {
     c.launches += 1;
 }
 
+template <int MODE>
+void near_tc_launch(Ctx& c, const DevPlan& p, int nitems, const int32_t* it_leaf, const int32_t* it_row0,
+                    const float* P, const float* Xa, const float* Xb, double* Y, int R, int* err) {
+    const dim3 grid(nitems, (R + 63) / 64);
+    set_smem_once(k_near_apply_tc<MODE>, (int)NearCfg<MODE>::kSmemBytes);
+    k_near_apply_tc<MODE><<<grid, kThreads, NearCfg<MODE>::kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xa, Xb, Y,
+                                                                                  R, err);
+    GPX_LAUNCH_CHECK();
+}
+
 void launch_near_apply_tc(Ctx& c, const DevPlan& p, int64_t nnz, int nitems, const int32_t* it_leaf,
                           const int32_t* it_row0, const float* P, const float* Xhi, const float* Xlo, double* Y, int R,
                           int* err, bool split_p) {
     if (nitems == 0) return;
     if (R % 4 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core near apply needs R a multiple of 4");
     KTimer t(c, K_NEAR_APPLY, 4.0 * nnz + 16.0 * (double)p.N * R, (split_p ? 6.0 : 4.0) * (double)nnz * R);
-    const dim3 grid(nitems, (R + 63) / 64);
-    if (split_p) {
-        set_smem_once(k_near_apply_tc<true>, (int)NearCfg<true>::kSmemBytes);
-        k_near_apply_tc<true><<<grid, kThreads, NearCfg<true>::kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xhi,
-                                                                                      Xlo, Y, R, err);
-    } else {
-        set_smem_once(k_near_apply_tc<false>, (int)NearCfg<false>::kSmemBytes);
-        k_near_apply_tc<false><<<grid, kThreads, NearCfg<false>::kSmemBytes, c.stream>>>(p, it_leaf, it_row0, P, Xhi,
-                                                                                        Xlo, Y, R, err);
-    }
-    GPX_LAUNCH_CHECK();
+    if (split_p)
+        near_tc_launch<1>(c, p, nitems, it_leaf, it_row0, P, Xhi, Xlo, Y, R, err);
+    else if (!Xlo)
+        near_tc_launch<2>(c, p, nitems, it_leaf, it_row0, P, Xhi, nullptr, Y, R, err);
+    else
+        near_tc_launch<0>(c, p, nitems, it_leaf, it_row0, P, Xhi, Xlo, Y, R, err);
     c.launches += 1;
 }
 

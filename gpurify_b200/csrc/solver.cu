@@ -37,12 +37,12 @@ struct DevM2L {
     int max_rank = 0;
     DBuf<float> K32;  // the same, rounded to TF32 (round to nearest, ties away), 343 x ns x ns, orders 4-5
     std::vector<int32_t> rank;
-    // Shared-basis compression (orders 5-6, built on first use): V padded to
-    // ns x kShared, U^T padded to kShared x round_up(ns, 64), and the cores
-    // C_o rounded to TF32, 343 x kShared x kShared.
+    // Shared-basis compression (orders 5-6, built on first use): V^T
+    // (kShared x ns) and U (round_up(ns, 64) x kShared), each split into TF32
+    // hi and lo parts, and the cores C_o rounded to TF32, 343 x kShared x kShared.
     bool shared_ok = false;
     double shared_err = 0.0;
-    DBuf<float> Vpad32, Utpad32, C32;
+    DBuf<float> Vt_hi, Vt_lo, U_hi, U_lo, C32;
 };
 
 namespace {
@@ -99,15 +99,21 @@ void ensure_shared(Ctx& ctx, DevM2L& d) {
     if (d.n < 5 || d.n > 6) throw Error(GPX_ERR_INVALID_ARG, "the shared-basis M2L runs orders 5 and 6");
     auto b = host_shared(d.n, d.mode);
     const int n3 = d.n * d.n * d.n, ns = node_stride(d.n), r = kShared, ldb = (ns + 63) / 64 * 64;
-    std::vector<float> vp((size_t)ns * r, 0.f), up((size_t)r * ldb, 0.f), c((size_t)343 * r * r, 0.f);
+    std::vector<float> vh((size_t)r * ns, 0.f), vl((size_t)r * ns, 0.f), uh((size_t)ldb * r, 0.f),
+        ul((size_t)ldb * r, 0.f), c((size_t)343 * r * r, 0.f);
     for (int l = 0; l < n3; ++l)
         for (int k = 0; k < r; ++k) {
-            vp[(size_t)l * r + k] = (float)b->V[(size_t)l * r + k];
-            up[(size_t)k * ldb + l] = (float)b->U[(size_t)l * r + k];
+            const double v = b->V[(size_t)l * r + k], u = b->U[(size_t)l * r + k];
+            vh[(size_t)k * ns + l] = tf32_rna(v);
+            vl[(size_t)k * ns + l] = tf32_rna(v - (double)vh[(size_t)k * ns + l]);
+            uh[(size_t)l * r + k] = tf32_rna(u);
+            ul[(size_t)l * r + k] = tf32_rna(u - (double)uh[(size_t)l * r + k]);
         }
     for (size_t i = 0; i < c.size(); ++i) c[i] = tf32_rna(b->C[i]);
-    d.Vpad32.upload(vp, ctx.stream);
-    d.Utpad32.upload(up, ctx.stream);
+    d.Vt_hi.upload(vh, ctx.stream);
+    d.Vt_lo.upload(vl, ctx.stream);
+    d.U_hi.upload(uh, ctx.stream);
+    d.U_lo.upload(ul, ctx.stream);
     d.C32.upload(c, ctx.stream);
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     d.shared_err = b->rel_err;
@@ -436,7 +442,8 @@ struct Operator {
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
-    int mixed_near = 0;  // 0: TF32 tensor-core near apply, 1: FP32 CUDA cores, 2: tensor cores with P split hi/lo
+    int mixed_near = 0;  // 0: TF32 tensor-core near apply (X split on chip), 1: FP32 CUDA cores, 2: tensor cores
+                         // with P split hi/lo, 3: as 0 with the split X gathered from global memory
     BlockJacobi bj;
     bool factored = false;  // M2L through the low-rank factors (compressed operators)
     bool tc32 = false;      // mixed: FP32 M2L on the tensor cores (orders 4 and 5)
@@ -598,12 +605,12 @@ struct Operator {
         }
         if (mixed) {
             P32.alloc((size_t)pl.nnz(), s);
-            if (mixed_near == 0)
+            if (mixed_near == 0 || mixed_near == 3)
                 launch_to_tf32(ctx, P.p, P32.p, pl.nnz());
             else  // FP32 CUDA-core apply, or the tensor-core apply that splits P on chip
                 launch_to_f32(ctx, P.p, P32.p, pl.nnz());
             X32.alloc((size_t)pl.N * R, s);
-            if (mixed_near != 1) {
+            if (mixed_near >= 2 || p2m_tc) {  // the split X of the tensor-core P2M or near modes 1 and 0
                 Xhi32.alloc((size_t)pl.N * R, s);
                 Xlo32.alloc((size_t)pl.N * R, s);
             }
@@ -802,10 +809,19 @@ struct Operator {
         applies32 += 1;
     }
     void apply32_direct(const double* X, double* Y) {
-        if (mixed_near != 1) {
+        if (mixed_near == 0 && !p2m_tc) {
+            // X gathered once as FP32 and split on chip
+            launch_to_f32(ctx, X, X32.p, pl.N * R);
+            launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, X32.p,
+                                 nullptr, Y, R, tc_err.p, false);
+        } else if (mixed_near != 1) {
             launch_split_tf32(ctx, X, X32.p, Xhi32.p, Xlo32.p, pl.N * R);
-            launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, Xhi32.p,
-                                 Xlo32.p, Y, R, tc_err.p, mixed_near == 2);
+            if (mixed_near == 0)
+                launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p,
+                                     X32.p, nullptr, Y, R, tc_err.p, false);
+            else
+                launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p,
+                                     Xhi32.p, Xlo32.p, Y, R, tc_err.p, mixed_near == 2);
         } else {
             launch_to_f32(ctx, X, X32.p, pl.N * R);
             launch_near_apply32(ctx, d.v, pl.nnz(), P32.p, X32.p, Y, R);
@@ -816,11 +832,11 @@ struct Operator {
                     // E^ = V^T E, L^ = sum_o C_o E^ (tensor cores), L = U L^ for the boxes [b0, b0 + nb)
                     const int ns = node_stride(pl.n);
                     const int64_t row0 = (int64_t)b0 * Rb32, nrows = (int64_t)nb * Rb32;
-                    launch_m2l_compress(ctx, E32.p, ns, m2l->Vpad32.p, Eh32.p, row0, nrows);
+                    launch_m2l_compress(ctx, E32.p, ns, m2l->Vt_hi.p, m2l->Vt_lo.p, Eh32.p, row0, nrows, tc_err.p);
                     launch_zero(ctx, Lh32.p + row0 * kShared, (size_t)nrows * kShared * sizeof(float));
                     launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], kShared, Eh32.p, Lh32.p, m2l->C32.p,
                                   Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
-                    launch_m2l_decompress(ctx, Lh32.p, m2l->Utpad32.p, ns, L32.p, row0, nrows);
+                    launch_m2l_decompress(ctx, Lh32.p, m2l->U_hi.p, m2l->U_lo.p, ns, L32.p, row0, nrows, tc_err.p);
                 } else if (tc32)
                     launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], node_stride(pl.n), E32.p, L32.p,
                                   m2l->K32.p, Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
@@ -1176,7 +1192,7 @@ Opts normalize(const gpx_solve_opts* o) {
     // The TF32 near apply perturbs the inner operator by ~2^-11 per entry, so
     // inner solves past 1e-3 buy little; the FP32-accurate near applies
     // (CUDA cores, or tensor cores with P split) support 1e-5.
-    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : (o->mixed_near == 0 ? 3 : 5);
+    r.inner_tol_exp = o->inner_tol_exp > 0 ? o->inner_tol_exp : ((o->mixed_near == 0 || o->mixed_near == 3) ? 3 : 5);
     r.mesh_max_edge = o->mesh_max_edge_m;
     r.max_panels = o->max_panels;
     r.far_quad = o->far_quad;
@@ -1234,7 +1250,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
                     "with centroid far-field sources (far_quad 0)");
     if (o.far_quad != 0 && o.far_quad != 1) throw Error(GPX_ERR_INVALID_ARG, "far_quad must be 0 or 1");
     if (o.precond < 0 || o.precond > 2) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0, 1 or 2");
-    if (o.mixed_near < 0 || o.mixed_near > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1 or 2");
+    if (o.mixed_near < 0 || o.mixed_near > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1, 2 or 3");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
     if (o.mixed_far_tc != 0 && o.mixed_far_tc != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_far_tc must be 0 or 1");
     if (o.inner_basis32 != 0 && o.inner_basis32 != 1) throw Error(GPX_ERR_INVALID_ARG, "inner_basis32 must be 0 or 1");
@@ -1885,7 +1901,7 @@ void autotune(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int
     for (int order : {4, 5, 6})
         for (int depth = std::max(2, d0 - 1); depth <= d0 + 1; ++depth)
             for (int fq : {0, 1})
-                for (int mn : (mixed ? std::vector<int>{0, 1} : std::vector<int>{0})) cands.push_back({order, depth, fq, mn});
+                for (int mn : (mixed ? std::vector<int>{0, 3, 1} : std::vector<int>{0})) cands.push_back({order, depth, fq, mn});
     double best_score = INFINITY;
     bool found = false;
     cudaEvent_t e0, e1;

@@ -98,21 +98,23 @@ typedef struct {
     int32_t skip_ground_rhs; /* 1: do not solve the substrate column (the reference solves it);
                                 the per-net result needs only the nets' columns */
     int32_t inner_tol_exp;   /* mixed: floor of the adaptive inner tolerance, 10^-x; 0 -> 3 with the
-                                TF32 near apply (mixed_near 0), 5 with the FP32-accurate ones */
+                                TF32 near apply (mixed_near 0 and 3), 5 with the FP32-accurate ones */
     double mesh_max_edge_m;  /* bridge panelisation: 0 -> reference `subdivisions` rule */
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
                                 (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
-    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05), 1 -> FP32 CUDA cores,
-                                2 -> TF32 tensor cores with the near blocks kept in FP32 and split into TF32
-                                hi and lo parts on chip (three products; FP32-accurate) */
+    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05; X gathered as FP32 and
+                                split into TF32 hi and lo on chip), 1 -> FP32 CUDA cores, 2 -> TF32 tensor
+                                cores with the near blocks kept in FP32 and split into TF32 hi and lo parts
+                                on chip (three products; FP32-accurate), 3 -> as 0 with X split before the
+                                apply and gathered as hi and lo */
     int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5 with centroid
                                 far-field sources, else the factored low-rank form on FP32 CUDA cores;
                                 1 -> always the factored form (compressed operators); 2 -> tensor cores
                                 at orders 4 and 5 also with Gauss-point sources; 3 -> at orders 5 and 6
                                 the operators in one shared rank-64 basis (K_o ~ U C_o V^T): expansions
-                                compressed and decompressed in FP32, the 64 x 64 cores C_o on the tensor
-                                cores (order 4 as 2) */
+                                compressed and decompressed on the tensor cores with TF32 hi and lo
+                                parts, the 64 x 64 cores C_o on the tensor cores (order 4 as 2) */
     int32_t no_graphs;       /* 1: launch every operator apply directly instead of replaying it as a
                                 captured CUDA graph (results are identical) */
     int32_t batch_streams;   /* gpx_cap_solve_batched: windows solved concurrently, one stream each;
@@ -203,7 +205,7 @@ gpx_status gpx_cap_sensitivity_rows(gpx_ctx* ctx, const gpx_panel_problem* probl
  * Chooses the far-field configuration for a representative panel problem: for
  * every candidate (Chebyshev order 4..6, octree depth around the automatic
  * choice, centroid or Gauss-point far-field sources, and in mixed precision
- * the tensor-core or FP32 near apply) it measures the operator's error on 512
+ * the near-apply engine: mixed_near 0, 3 or 1) it measures the operator's error on 512
  * sampled rows against the exact all-pairs rows (three smooth probe charge
  * densities) and times the operator apply on the device; the fastest
  * candidate whose error is at most target_rel_err / 2 wins (score: set-up +

@@ -29,7 +29,7 @@ def window(nets=12, side=15.0, edge=0.3e-6):
                                 mesh_max_edge_m=edge, max_panels=-1)
 
 
-@pytest.mark.parametrize("mixed_near", [0, 1, 2])
+@pytest.mark.parametrize("mixed_near", [0, 1, 2, 3])
 @pytest.mark.parametrize("nrhs", [3, 64, 100])
 def test_mixed_operator_close_to_fp64(ctx, nrhs, mixed_near):
     p = window()
@@ -122,6 +122,20 @@ def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near, mixed_m2l):
     d = np.abs(np.diag(C64[:R, :R]))
     err = np.abs(C32[:R, :R] - C64[:R, :R]) / d[:, None]
     assert err.max() < 1e-6, err.max()
+
+
+def test_near_x_split_on_chip_matches_split_in_memory(ctx):
+    """The TF32 near apply with X gathered as FP32 and split on chip
+    (mixed_near 0) and with X split before the apply (mixed_near 3) compute
+    the same products: the applies agree to FP32 accumulation order."""
+    p = window()
+    rng = np.random.default_rng(9)
+    sig = rng.standard_normal((len(p["verts"]), 100))
+    kw = dict(order=5, max_level=5, dense_below=-1, far_quad=1, precision=1, mixed_m2l=1)
+    y0, _ = ctx.operator_apply(p["verts"], sig, mixed_near=0, **kw)
+    y3, _ = ctx.operator_apply(p["verts"], sig, mixed_near=3, **kw)
+    d = np.linalg.norm(y0 - y3, axis=0) / np.linalg.norm(y3, axis=0)
+    assert d.max() < 1e-6, d.max()
 
 
 def test_fp32_inner_basis_matches_fp64_basis(ctx):
