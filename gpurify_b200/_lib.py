@@ -63,7 +63,7 @@ class SolveReport(C.Structure):
         ("operator_applies", C.c_int64), ("max_rel_residual", C.c_double), ("converged", C.c_int32),
         ("dense", C.c_int32), ("t_panelize_s", C.c_double), ("t_setup_s", C.c_double), ("t_solve_s", C.c_double),
         ("t_total_s", C.c_double), ("t_near_assembly_s", C.c_double), ("kernel_launches", C.c_int64),
-        ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+        ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("restart_used", C.c_int32), ("reserved", C.c_int32),
     ]
 
     def as_dict(self):

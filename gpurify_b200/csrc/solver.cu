@@ -918,6 +918,7 @@ struct SolveStats {
     double max_resid = 0.0;
     bool converged = false;
     std::string hist;  // mixed path: the residual after each refinement step (for error messages)
+    int m_used = 0;    // GMRES restart length after the memory budget (largest over the solves)
 };
 
 using ApplyFn = std::function<void(const double*, double*)>;
@@ -969,7 +970,11 @@ void gmres_multi_t(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int3
     constexpr bool f32 = sizeof(TB) == 4;
     cudaStream_t s = ctx.stream;
     const int64_t NR = N * R;
+    // A shorter restart than asked for keeps the asked-for iteration cap
+    // (max_restarts x m): more, shorter cycles.
+    const int m_asked = m;
     m = restart_within_budget(m, NR, (int)sizeof(TB));
+    if (m < m_asked) max_restarts = (int)std::min<int64_t>(1000, (int64_t)max_restarts * ((m_asked + m - 1) / m));
     DBuf<TB> V;
     DBuf<double> Vcur;  // FP32 basis: the newest basis vector in FP64
     DBuf<double> W, Z, Res, H, cs, sn, g, y, h1, h2, hnorm, bnorm, bcur, est, resid, beta, partial;
@@ -1104,6 +1109,7 @@ void gmres_multi_t(Ctx& ctx, const ApplyFn& A, const PrecondFn& Minv, const int3
         ctx.launches += 1;
     }
     st = SolveStats();
+    st.m_used = m;
     for (int cycle = 0; cycle < max_restarts; ++cycle) {
         st.cycles = cycle + 1;
         launch_colnorm(ctx, Res.p, N, R, partial.p, nblk, beta.p);
@@ -1371,6 +1377,7 @@ void mixed_solve(Ctx& ctx, Operator& op, const int32_t* d_cond, const int32_t* d
         gmres_multi(ctx, a32, pc, d_cond, d_rhs, Res.p, R, N, inner_tol, o.restart, std::min(o.max_restarts, 3), D, in,
                     false, o.graphs != 0 && !ctx.profile, o.inner_basis32 != 0);
         st.iterations += in.iterations;
+        st.m_used = std::max(st.m_used, in.m_used);
         launch_add(ctx, X.p, D.p, NR);
         op.apply(X.p, W.p);
         if (B)
@@ -1460,6 +1467,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
         int oc = 0;
         solve_columns(ctx, op, o, dense, pr.dp.cond.p, d_rhs.p, nullptr, R, n, X, sc, oc);
         st.iterations = std::max(st.iterations, sc.iterations);
+        st.m_used = std::max(st.m_used, sc.m_used);
         st.max_resid = std::max(st.max_resid, sc.max_resid);
         if (!sc.converged && st.converged) st.hist = sc.hist;
         st.converged = st.converged && sc.converged;
@@ -1512,11 +1520,12 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
         r.t_total_s = t2 - t0;
         r.t_near_assembly_s = op.t_assembly_s;
         r.kernel_launches = ctx.launches - l0;
+        r.restart_used = st.m_used;
     }
     if (!st.converged)
         throw Error(GPX_ERR_CAPACITANCE, "GMRES did not converge: max relative residual " +
                                              std::to_string(st.max_resid) + " after " + std::to_string(st.iterations) +
-                                             " iterations" +
+                                             " iterations (restart length " + std::to_string(st.m_used) + ")" +
                                              (st.hist.empty() ? "" : "; residual after each refinement step: " + st.hist));
 }
 

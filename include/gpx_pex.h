@@ -149,6 +149,8 @@ typedef struct {
     double t_near_assembly_s;  /* device time of the Wilton near-field assembly */
     int64_t kernel_launches;
     int64_t h2d_bytes, d2h_bytes;  /* host<->device copies made by the call */
+    int32_t restart_used;      /* GMRES restart length after the Krylov memory budget (gpx_cap_solve) */
+    int32_t reserved;
 } gpx_solve_report;
 
 /* Pre-built panels: `verts` n x 12 doubles (4 vertices x xyz, metres; a
