@@ -95,13 +95,15 @@ void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int 
 
 // Tensor-core (tcgen05, TF32 inputs, FP32 accumulation) M2L work list of one
 // level: pairs of target boxes sharing one offset loop.
+// Target boxes per tensor-core M2L work item (of one octant class, so that
+// their interaction lists use the same offsets).
+constexpr int kGroup = 4;
 struct TcLevel {
     int nitems = 0;
-    const int32_t* item_t = nullptr;    // 2 per item: target boxes (second may be -1)
+    const int32_t* item_t = nullptr;    // kGroup per item: target boxes (trailing ones may be -1)
     const int32_t* item_off = nullptr;  // nitems + 1: entry ranges
     const int32_t* slot = nullptr;      // per entry: operator slot
-    const int32_t* srcA = nullptr;      // per entry: source box of the first target or -1
-    const int32_t* srcB = nullptr;      // per entry: source box of the second target or -1
+    const int32_t* src = nullptr;       // kGroup per entry: each target's source box at the slot's offset, or -1
 };
 // L[t][r][m] = scale * sum K[m][l] E[s][r][l] for order-4 (node stride 64)
 // or order-5 (node stride 128) expansions; K32: 343 x ns x ns TF32-rounded

@@ -4,19 +4,22 @@
 //
 // For one offset o every target box t with a source s = t + o needs
 //     L_t^T (R x NS) += E_s^T (R x NS) * K_o^T (NS x NS).
-// A CTA owns two target boxes (tA, tB) and a 64-wide chunk of right-hand
-// sides: D (128 x NS, FP32, in TMEM) = [E_sA^T; E_sB^T] (128 x NS, A operand)
-// times K_o^T (NS x NS, B operand), accumulated over the union of the two
-// boxes' offsets.  Expansions are stored E[box][r][node] and the operator
-// table K[o][m][l] (target node m, source node l), both with node stride NS,
-// so every A row (one right-hand side) and every B row (one target node) is a
-// contiguous K-major row: the contraction over source nodes runs in chunks of
-// 32 TF32 (one 128-byte swizzle atom per row), and each chunk is one pipeline
-// stage: A (128 rows x 128 B) and B (NS rows x 128 B).
+// A CTA owns kGroup = 4 target boxes of one octant class (so their
+// interaction lists use the same offsets) and a 64-wide chunk of right-hand
+// sides: two accumulators D_0, D_1 (128 x NS each, FP32, in TMEM), D_h =
+// [E_s(2h)^T; E_s(2h+1)^T] (128 x NS, A operand) times K_o^T (NS x NS, B
+// operand), accumulated over the union of the boxes' offsets; each operator
+// tile staged in shared memory feeds both accumulators.  Expansions are
+// stored E[box][r][node] and the operator table K[o][m][l] (target node m,
+// source node l), both with node stride NS, so every A row (one right-hand
+// side) and every B row (one target node) is a contiguous K-major row: the
+// contraction over source nodes runs in chunks of 32 TF32 (one 128-byte
+// swizzle atom per row), and each chunk is one pipeline stage: two A tiles
+// (128 rows x 128 B each) and B (NS rows x 128 B).
 // Warp-specialised: four producer warps copy each stage with cp.async
 // straight into the 128-byte-swizzled layout the MMA descriptors name and
 // signal the stage's `full` mbarrier with cp.async.mbarrier.arrive (128
-// arrivals); one thread of the fifth warp waits on `full`, issues the four
+// arrivals); one thread of the fifth warp waits on `full`, issues the eight
 // K=8 MMAs of the chunk and commits them to the stage's `empty` mbarrier,
 // which the producers wait on before refilling the stage.  kStages stages
 // are in flight, with no block-wide barrier in the main loop.
@@ -82,11 +85,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 template <int NS>
 struct TcCfg {
     static constexpr int kStages = 2;
+    static constexpr int kTiles = kGroup / 2;                  // A tiles (accumulators) per stage
     static constexpr uint32_t kATile = 128 * 128;              // 128 rows x 128 B
     static constexpr uint32_t kBTile = NS * 128;               // NS rows x 128 B
-    static constexpr uint32_t kStage = kATile + kBTile;        // multiple of 1024
+    static constexpr uint32_t kStage = kTiles * kATile + kBTile;  // multiple of 1024
     static constexpr uint32_t kSmem = kStages * kStage + 1024 + 256;  // + alignment slack + barriers
-    static constexpr uint32_t kTmemCols = NS;                  // 64 or 128 FP32 columns
+    static constexpr uint32_t kTmemCols = kTiles * NS;         // 128 or 256 FP32 columns
     static constexpr int kChunks = NS / 32;                    // contraction chunks per entry
     // Instruction descriptor: D F32, A/B TF32, both K-major, N = NS, M = 128.
     static constexpr uint32_t kIdesc =
@@ -108,7 +112,6 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int item = blockIdx.x;
     const int r0 = blockIdx.y * 64;
-    const int tA = lv.item_t[2 * item], tB = lv.item_t[2 * item + 1];
     const int e0 = lv.item_off[item], e1 = lv.item_off[item + 1];
     const int total = (e1 - e0) * C::kChunks;
 
@@ -134,22 +137,21 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     const uint32_t tmem = *tslot;
 
     // Copies of chunk q (entry q / kChunks, source nodes 32 (q % kChunks) ..)
-    // into stage q % S: A rows 0..63 from tA's source, 64..127 from tB's
-    // source (zero-filled where the target has no source at this offset), B
-    // rows = the operator's target nodes.  Every producer thread copies 8 A and
-    // NS/16 B 16-byte pieces; 8 consecutive threads read one 128-byte row
-    // segment.
+    // into stage q % S: A tile h, rows 0..63 from target 2h's source, rows
+    // 64..127 from target 2h+1's (zero-filled where a target has no source at
+    // this offset); B rows = the operator's target nodes.  Every producer
+    // thread copies 8 pieces of 16 bytes per A tile and NS/16 of B; 8
+    // consecutive threads read one 128-byte row segment.
     auto issue = [&](int q) {
         const int e = e0 + q / C::kChunks, kc = q % C::kChunks;
-        const int sa = lv.srcA[e], sb = lv.srcB[e];
         const uint32_t a = base + (uint32_t)(q % S) * C::kStage;
-        const uint32_t b = a + C::kATile;
+        const uint32_t b = a + C::kTiles * C::kATile;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int id = tid + kProducers * i, row = id >> 3, pc = id & 7;
-            const int src = row < 64 ? sa : sb;
+        for (int i = 0; i < 8 * C::kTiles; ++i) {
+            const int id = tid + kProducers * i, h = id >> 10, row = (id >> 3) & 127, pc = id & 7;
+            const int src = lv.src[(int64_t)e * kGroup + 2 * h + (row >> 6)];
             const float* g = src >= 0 ? E + ((int64_t)src * R + r0 + (row & 63)) * NS + kc * 32 + pc * 4 : E;
-            cp16(a + swz(row, pc), g, src >= 0);
+            cp16(a + (uint32_t)h * C::kATile + swz(row, pc), g, src >= 0);
         }
         const float* Ko = K32 + (int64_t)lv.slot[e] * NS * NS + kc * 32;
 #pragma unroll
@@ -182,16 +184,19 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t abase = base + (uint32_t)st * C::kStage, bbase = abase + C::kATile;
+            const uint32_t abase = base + (uint32_t)st * C::kStage, bbase = abase + C::kTiles * C::kATile;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const uint64_t ad = desc_sw128(abase + (uint32_t)k * 32u);
                 const uint64_t bd = desc_sw128(bbase + (uint32_t)k * 32u);
                 const uint32_t acc = (q > 0 || k > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(C::kIdesc), "r"(acc));
+#pragma unroll
+                for (int h = 0; h < C::kTiles; ++h) {
+                    const uint64_t ad = desc_sw128(abase + (uint32_t)h * C::kATile + (uint32_t)k * 32u);
+                    asm volatile(
+                        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + (uint32_t)(h * NS)),
+                        "l"(ad), "l"(bd), "r"(C::kIdesc), "r"(acc));
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&empty[st]))
@@ -210,22 +215,25 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
     if (s_bad) {
         if (tid == 0) atomicExch(err, 1);
     } else if (tid < kProducers && total > 0) {
-        // Epilogue: warp w (0..3) reads TMEM lanes 32w..32w+31 = rows of D.
+        // Epilogue: warp w (0..3) reads TMEM lanes 32w..32w+31 = rows of D_h.
         const int row = warp * 32 + lane;
-        const int t = row < 64 ? tA : tB;
-        float* dst = (t >= 0) ? L + ((int64_t)t * R + r0 + (row & 63)) * NS : nullptr;
-        const float sc = (t >= 0 && box_scale) ? (float)box_scale[t] : scale;
 #pragma unroll
-        for (int cb = 0; cb < NS / 16; ++cb) {
-            uint32_t v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 16), v);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (dst) {
+        for (int h = 0; h < C::kTiles; ++h) {
+            const int t = lv.item_t[(int64_t)item * kGroup + 2 * h + (row >> 6)];
+            float* dst = (t >= 0) ? L + ((int64_t)t * R + r0 + (row & 63)) * NS : nullptr;
+            const float sc = (t >= 0 && box_scale) ? (float)box_scale[t] : scale;
 #pragma unroll
-                for (int k = 0; k < 16; k += 4) {
-                    const float4 o = make_float4(sc * __uint_as_float(v[k]), sc * __uint_as_float(v[k + 1]),
-                                                 sc * __uint_as_float(v[k + 2]), sc * __uint_as_float(v[k + 3]));
-                    *reinterpret_cast<float4*>(dst + cb * 16 + k) = o;
+            for (int cb = 0; cb < NS / 16; ++cb) {
+                uint32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * NS + cb * 16), v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (dst) {
+#pragma unroll
+                    for (int k = 0; k < 16; k += 4) {
+                        const float4 o = make_float4(sc * __uint_as_float(v[k]), sc * __uint_as_float(v[k + 1]),
+                                                     sc * __uint_as_float(v[k + 2]), sc * __uint_as_float(v[k + 3]));
+                        *reinterpret_cast<float4*>(dst + cb * 16 + k) = o;
+                    }
                 }
             }
         }

@@ -331,23 +331,23 @@ void upload_plan(Ctx& ctx, const Plan& p, const DevM2L* m2l, DevPlanBufs& d) {
     d.far.m2l_off = p.m2l_off.data();
 }
 
-// Tensor-core M2L work lists of every level (pairs of target boxes of the
-// same octant class in Morton order sharing one offset loop).
+// Tensor-core M2L work lists of every level (groups of kGroup target boxes of
+// the same octant class in Morton order sharing one offset loop).
 struct TcLists {
     std::vector<TcLevel> level;  // per level (empty below 2)
     TcLevel all;                 // levels 2..L in one list
-    DBuf<int32_t> item_t, item_off, slot, srcA, srcB;
+    DBuf<int32_t> item_t, item_off, slot, src;
 };
 
 void build_tc_lists(Ctx& ctx, const Plan& pl, TcLists& out) {
-    std::vector<int32_t> it, ioff, sl, sa, sb;
+    std::vector<int32_t> it, ioff, sl, src;
     struct LevelRange {
         size_t it0, off0;
         int n;
     };
     std::vector<LevelRange> ranges(pl.L + 1, {0, 0, 0});
     for (int l = 2; l <= pl.L; ++l) {
-        ranges[l].it0 = it.size() / 2;
+        ranges[l].it0 = it.size() / kGroup;
         ranges[l].off0 = ioff.size();
         std::vector<int32_t> cls[8];
         for (int32_t b = pl.lvl_off[l]; b < pl.lvl_off[l + 1]; ++b) {
@@ -356,24 +356,25 @@ void build_tc_lists(Ctx& ctx, const Plan& pl, TcLists& out) {
             cls[(c[0] & 1) | ((c[1] & 1) << 1) | ((c[2] & 1) << 2)].push_back(b);
         }
         int n = 0;
+        std::vector<int32_t> per((size_t)kGroup * 343);
         for (auto& v : cls)
-            for (size_t k = 0; k < v.size(); k += 2) {
-                const int32_t tA = v[k], tB = k + 1 < v.size() ? v[k + 1] : -1;
-                int32_t srcA[343], srcB[343];
-                std::fill(srcA, srcA + 343, -1);
-                std::fill(srcB, srcB + 343, -1);
-                for (int64_t e = pl.m2l_off[tA]; e < pl.m2l_off[tA + 1]; ++e) srcA[pl.m2l_slot[e]] = pl.m2l_src[e];
-                if (tB >= 0)
-                    for (int64_t e = pl.m2l_off[tB]; e < pl.m2l_off[tB + 1]; ++e) srcB[pl.m2l_slot[e]] = pl.m2l_src[e];
-                it.push_back(tA);
-                it.push_back(tB);
+            for (size_t k = 0; k < v.size(); k += kGroup) {
+                std::fill(per.begin(), per.end(), -1);  // per[slot * kGroup + i]
+                for (int i = 0; i < kGroup; ++i) {
+                    const int32_t t = k + i < v.size() ? v[k + i] : -1;
+                    it.push_back(t);
+                    if (t < 0) continue;
+                    for (int64_t e = pl.m2l_off[t]; e < pl.m2l_off[t + 1]; ++e)
+                        per[(size_t)pl.m2l_slot[e] * kGroup + i] = pl.m2l_src[e];
+                }
                 ioff.push_back((int32_t)sl.size());
-                for (int q = 0; q < 343; ++q)
-                    if (srcA[q] >= 0 || srcB[q] >= 0) {
-                        sl.push_back(q);
-                        sa.push_back(srcA[q]);
-                        sb.push_back(srcB[q]);
-                    }
+                for (int q = 0; q < 343; ++q) {
+                    bool any = false;
+                    for (int i = 0; i < kGroup; ++i) any = any || per[(size_t)q * kGroup + i] >= 0;
+                    if (!any) continue;
+                    sl.push_back(q);
+                    for (int i = 0; i < kGroup; ++i) src.push_back(per[(size_t)q * kGroup + i]);
+                }
                 ++n;
             }
         ranges[l].n = n;
@@ -383,17 +384,15 @@ void build_tc_lists(Ctx& ctx, const Plan& pl, TcLists& out) {
     out.item_t.upload(it, s);
     out.item_off.upload(ioff, s);
     out.slot.upload(sl, s);
-    out.srcA.upload(sa, s);
-    out.srcB.upload(sb, s);
+    out.src.upload(src, s);
     out.level.assign(pl.L + 1, TcLevel());
     for (int l = 2; l <= pl.L; ++l) {
         TcLevel& v = out.level[l];
         v.nitems = ranges[l].n;
-        v.item_t = out.item_t.p + 2 * ranges[l].it0;
+        v.item_t = out.item_t.p + (size_t)kGroup * ranges[l].it0;
         v.item_off = out.item_off.p + ranges[l].off0;
         v.slot = out.slot.p;
-        v.srcA = out.srcA.p;
-        v.srcB = out.srcB.p;
+        v.src = out.src.p;
     }
     // every level in one launch (the per-level item lists are contiguous)
     out.all = TcLevel();
