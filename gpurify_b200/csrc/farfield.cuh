@@ -96,8 +96,12 @@ void launch_m2l_fac(Ctx& c, const FacM2L<T>& f, const FacLevel& lv, int b0, int 
 // Tensor-core (tcgen05, TF32 inputs, FP32 accumulation) M2L work list of one
 // level: pairs of target boxes sharing one offset loop.
 // Target boxes per tensor-core M2L work item (of one octant class, so that
-// their interaction lists use the same offsets).
-constexpr int kGroup = 4;
+// their interaction lists use the same offsets): 2, one TMEM accumulator.
+// Four boxes with two accumulators sharing each operator tile measured
+// slower on the bench window (0.385 against 0.309 ms per launch: half the
+// CTAs per SM by shared memory, and more zero-filled rows in the union of
+// four boxes' offsets).
+constexpr int kGroup = 2;
 struct TcLevel {
     int nitems = 0;
     const int32_t* item_t = nullptr;    // kGroup per item: target boxes (trailing ones may be -1)

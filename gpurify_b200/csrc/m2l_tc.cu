@@ -4,23 +4,23 @@
 //
 // For one offset o every target box t with a source s = t + o needs
 //     L_t^T (R x NS) += E_s^T (R x NS) * K_o^T (NS x NS).
-// A CTA owns kGroup = 4 target boxes of one octant class (so their
-// interaction lists use the same offsets) and a 64-wide chunk of right-hand
-// sides: two accumulators D_0, D_1 (128 x NS each, FP32, in TMEM), D_h =
+// A CTA owns kGroup target boxes of one octant class (so their interaction
+// lists use the same offsets) and a 64-wide chunk of right-hand sides:
+// kGroup / 2 accumulators D_h (128 x NS each, FP32, in TMEM), D_h =
 // [E_s(2h)^T; E_s(2h+1)^T] (128 x NS, A operand) times K_o^T (NS x NS, B
 // operand), accumulated over the union of the boxes' offsets; each operator
-// tile staged in shared memory feeds both accumulators.  Expansions are
+// tile staged in shared memory feeds every accumulator.  Expansions are
 // stored E[box][r][node] and the operator table K[o][m][l] (target node m,
 // source node l), both with node stride NS, so every A row (one right-hand
 // side) and every B row (one target node) is a contiguous K-major row: the
 // contraction over source nodes runs in chunks of 32 TF32 (one 128-byte
-// swizzle atom per row), and each chunk is one pipeline stage: two A tiles
-// (128 rows x 128 B each) and B (NS rows x 128 B).
+// swizzle atom per row), and each chunk is one pipeline stage: kGroup / 2 A
+// tiles (128 rows x 128 B each) and B (NS rows x 128 B).
 // Warp-specialised: four producer warps copy each stage with cp.async
 // straight into the 128-byte-swizzled layout the MMA descriptors name and
 // signal the stage's `full` mbarrier with cp.async.mbarrier.arrive (128
-// arrivals); one thread of the fifth warp waits on `full`, issues the eight
-// K=8 MMAs of the chunk and commits them to the stage's `empty` mbarrier,
+// arrivals); one thread of the fifth warp waits on `full`, issues the
+// 4 kGroup / 2 K=8 MMAs of the chunk and commits them to the stage's `empty` mbarrier,
 // which the producers wait on before refilling the stage.  kStages stages
 // are in flight, with no block-wide barrier in the main loop.
 // The tensor cores read FP32 operands as TF32 (the operator table is stored

@@ -441,8 +441,8 @@ struct Operator {
     DBuf<int32_t> tc_err;
     TcLists tc;
     int precond = 0;
-    int mixed_near = 0;  // 0: TF32 tensor-core near apply (X split on chip), 1: FP32 CUDA cores, 2: tensor cores
-                         // with P split hi/lo, 3: as 0 with the split X gathered from global memory
+    int mixed_near = 0;  // 0: TF32 tensor-core near apply (X split before it), 1: FP32 CUDA cores, 2: tensor cores
+                         // with P split hi/lo, 3: as 0 with X gathered as FP32 and split on chip
     BlockJacobi bj;
     bool factored = false;  // M2L through the low-rank factors (compressed operators)
     bool tc32 = false;      // mixed: FP32 M2L on the tensor cores (orders 4 and 5)
@@ -609,7 +609,7 @@ struct Operator {
             else  // FP32 CUDA-core apply, or the tensor-core apply that splits P on chip
                 launch_to_f32(ctx, P.p, P32.p, pl.nnz());
             X32.alloc((size_t)pl.N * R, s);
-            if (mixed_near >= 2 || p2m_tc) {  // the split X of the tensor-core P2M or near modes 1 and 0
+            if (mixed_near == 0 || mixed_near == 2 || p2m_tc) {  // the split X in memory
                 Xhi32.alloc((size_t)pl.N * R, s);
                 Xlo32.alloc((size_t)pl.N * R, s);
             }
@@ -808,14 +808,14 @@ struct Operator {
         applies32 += 1;
     }
     void apply32_direct(const double* X, double* Y) {
-        if (mixed_near == 0 && !p2m_tc) {
+        if (mixed_near == 3 && !p2m_tc) {
             // X gathered once as FP32 and split on chip
             launch_to_f32(ctx, X, X32.p, pl.N * R);
             launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p, X32.p,
                                  nullptr, Y, R, tc_err.p, false);
         } else if (mixed_near != 1) {
             launch_split_tf32(ctx, X, X32.p, Xhi32.p, Xlo32.p, pl.N * R);
-            if (mixed_near == 0)
+            if (mixed_near == 3)
                 launch_near_apply_tc(ctx, d.v, pl.nnz(), d.nitems128, d.item128_leaf.p, d.item128_row0.p, P32.p,
                                      X32.p, nullptr, Y, R, tc_err.p, false);
             else

@@ -103,11 +103,11 @@ typedef struct {
     int64_t max_panels;      /* bridge: 0 -> 20 000 (bridge.rs:29), -1 -> unlimited */
     int32_t far_quad;        /* far-field source model: 0 -> each panel's charge at its centroid
                                 (the reference, fmm_solver.rs:109-115); 1 -> 2x2 Gauss points */
-    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05; X gathered as FP32 and
-                                split into TF32 hi and lo on chip), 1 -> FP32 CUDA cores, 2 -> TF32 tensor
-                                cores with the near blocks kept in FP32 and split into TF32 hi and lo parts
-                                on chip (three products; FP32-accurate), 3 -> as 0 with X split before the
-                                apply and gathered as hi and lo */
+    int32_t mixed_near;      /* mixed: near-field apply 0 -> TF32 tensor cores (tcgen05; X split into TF32 hi
+                                and lo before the apply and gathered as both), 1 -> FP32 CUDA cores, 2 ->
+                                TF32 tensor cores with the near blocks kept in FP32 and split into TF32 hi
+                                and lo parts on chip (three products; FP32-accurate), 3 -> as 0 with X
+                                gathered once as FP32 and split on chip */
     int32_t mixed_m2l;       /* mixed: M2L 0 -> TF32 tensor cores (tcgen05) at orders 4 and 5 with centroid
                                 far-field sources, else the factored low-rank form on FP32 CUDA cores;
                                 1 -> always the factored form (compressed operators); 2 -> tensor cores

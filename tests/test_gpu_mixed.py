@@ -125,9 +125,9 @@ def test_mixed_solve_matches_fp64(ctx, order, far_quad, mixed_near, mixed_m2l):
 
 
 def test_near_x_split_on_chip_matches_split_in_memory(ctx):
-    """The TF32 near apply with X gathered as FP32 and split on chip
-    (mixed_near 0) and with X split before the apply (mixed_near 3) compute
-    the same products: the applies agree to FP32 accumulation order."""
+    """The TF32 near apply with X split before the apply (mixed_near 0) and
+    with X gathered as FP32 and split on chip (mixed_near 3) compute the same
+    products: the applies agree to FP32 rounding of X and accumulation order."""
     p = window()
     rng = np.random.default_rng(9)
     sig = rng.standard_normal((len(p["verts"]), 100))
