@@ -69,8 +69,11 @@ def parse():
     ap.add_argument("--inner-tol-exp", type=int, default=0, help="mixed: inner GMRES tolerance 10^-x (0: default)")
     ap.add_argument("--mixed-near", type=int, default=0, help="mixed near apply: 0 TF32 tensor cores, 1 FP32 CUDA cores")
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 QR-compressed M2L operators (reference), 1 exact")
-    ap.add_argument("--mixed-m2l", type=int, default=2,
-                    help="mixed M2L: 0 auto, 1 factored on CUDA cores, 2 tensor cores also with Gauss sources")
+    ap.add_argument("--mixed-m2l", type=int, default=3,
+                    help="mixed M2L: 0 auto, 1 factored on CUDA cores, 2 tensor cores also with Gauss sources, "
+                         "3 shared rank-64 basis on the tensor cores (fastest, measured)")
+    ap.add_argument("--mixed-far-tc", type=int, default=1,
+                    help="mixed: 1 P2M and L2P on the tensor cores (hi/lo split operands), 0 FP32 CUDA cores")
     ap.add_argument("--workload", default="window64", choices=["window64", "twowires", "batch", "bus", "block"],
                     help="window64: the headline 64-net window; twowires: two met1 wires on a 0.05 um mesh; "
                          "batch: many uneven windows in one batched call; bus: met2 bus sensitivities; "
@@ -607,7 +610,7 @@ def main():
     base_kw = dict(order=args.order, max_level=args.depth, skip_ground_rhs=1, tol=1e-8, restart=args.restart,
                    far_quad=args.far_quad, precond=args.precond, inner_tol_exp=args.inner_tol_exp,
                    mixed_near=args.mixed_near, m2l_mode=args.m2l_mode, mixed_m2l=args.mixed_m2l,
-                   no_graphs=1 if args.no_graphs else 0)
+                   mixed_far_tc=args.mixed_far_tc, no_graphs=1 if args.no_graphs else 0)
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     lay = workload(rank, args.nets, args.side)
     p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
@@ -660,11 +663,18 @@ def main():
             accuracy["mixed_vs_fp64"] = entry_errors(runs["mixed"]["C"][:R, :R], runs["fp64"]["C"][:R, :R])
 
     if rank == 0:
+        shared_m2l = head == "mixed" and args.mixed_m2l == 3 and args.order in (5, 6)
         tc_m2l = head == "mixed" and args.order in (4, 5) and args.mixed_m2l != 1 and (
-            args.far_quad == 0 or args.m2l_mode == 1 or args.mixed_m2l == 2)
-        roof = roofline_of(hr["ks"], hr["ms_prof"], "tcgen05 TF32" if tc_m2l else
-                           ("FP32 CUDA cores, factored low-rank operators" if head == "mixed" else
-                            "FP64 CUDA cores, factored low-rank operators"))
+            args.far_quad == 0 or args.m2l_mode == 1 or args.mixed_m2l >= 2)
+        if shared_m2l:
+            engine = ("tcgen05 TF32 on the 64 x 64 shared-basis cores, with tcgen05 hi/lo compress and "
+                      "decompress; flops counted as the dense-equivalent full operators")
+        elif tc_m2l:
+            engine = "tcgen05 TF32"
+        else:
+            engine = ("FP32 CUDA cores, factored low-rank operators" if head == "mixed" else
+                      "FP64 CUDA cores, factored low-rank operators")
+        roof = roofline_of(hr["ks"], hr["ms_prof"], engine)
         names = [k for k in hr["ks"] if k != "total_launches"]
         breakdown = {n: {"ms_per_step": hr["ks"][n]["ms"] / args.steps,
                          "launches_per_step": hr["ks"][n]["launches"] / args.steps}
@@ -693,7 +703,7 @@ def main():
                        "panels": N, "rhs": R, "precision": head, "order": args.order, "depth": args.depth,
                        "far_quad": args.far_quad, "restart": args.restart,
                        "precond": {pr: runs[pr]["kw"]["precond"] for pr in runs},
-                       "mixed_m2l": args.mixed_m2l,
+                       "mixed_m2l": args.mixed_m2l, "mixed_far_tc": args.mixed_far_tc,
                        "parallelism": f"replicas x{world}", "l2": "working set (Krylov basis > 1 GB) >> L2"},
             "panel_rhs_per_s": world * N * R / (ms_step * 1e-3),
             "precisions": per_prec,

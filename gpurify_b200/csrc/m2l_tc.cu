@@ -146,10 +146,13 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(TcLevel lv, const float* __
         const int e = e0 + q / C::kChunks, kc = q % C::kChunks;
         const uint32_t a = base + (uint32_t)(q % S) * C::kStage;
         const uint32_t b = a + C::kTiles * C::kATile;
+        int srcs[kGroup];
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) srcs[g] = lv.src[(int64_t)e * kGroup + g];
 #pragma unroll
         for (int i = 0; i < 8 * C::kTiles; ++i) {
             const int id = tid + kProducers * i, h = id >> 10, row = (id >> 3) & 127, pc = id & 7;
-            const int src = lv.src[(int64_t)e * kGroup + 2 * h + (row >> 6)];
+            const int src = srcs[2 * h + (row >> 6)];
             const float* g = src >= 0 ? E + ((int64_t)src * R + r0 + (row & 63)) * NS + kc * 32 + pc * 4 : E;
             cp16(a + (uint32_t)h * C::kATile + swz(row, pc), g, src >= 0);
         }
