@@ -534,6 +534,20 @@ struct Operator {
         bj.Minv32.release();
     }
 
+    // Frees everything only the mixed path's FP32 applies use (near blocks in
+    // FP32, FP32 expansions, split inputs and weights, FP32 inverses), keeping
+    // the FP64 near blocks and far field: after its last FP32 apply the
+    // operator can still be transposed and still run apply_far_with.
+    void release_mixed() {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+        P32.release();
+        bj.Minv32.release();
+        for (auto* b : {&E32, &L32, &X32, &W32, &Sc32, &Xhi32, &Xlo32, &Whi32, &Wlo32, &Shi32, &Slo32, &Eh32, &Lh32})
+            b->release();
+    }
+
     // Near blocks: the Wilton assembly, or (fwd given) the transpose of the
     // forward operator's blocks; then the preconditioners and the far-field
     // end weights (swapped for the transpose).
@@ -1674,6 +1688,11 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
         opT->tc32 = op.tc32;
         opT->shared = op.shared;
         opT->p2m_tc = op.p2m_tc;
+        // the transposed operator is assembled from the forward FP64 blocks;
+        // the forward operator's FP32 state goes first, its FP64 blocks right
+        // after, so that at most one operator's near blocks of each kind are
+        // resident beside sigma
+        op.release_mixed();
         opT->assemble(&op);
         applies += op.applies + op.applies32;
         op.release_near();
