@@ -402,6 +402,12 @@ def time_solves(ctx, verts, cond, ncond, solve_kw, steps, warmup, stream, dist, 
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
+    # let nvidia-smi start up (its first sample) before the timed region: the
+    # solver builds its octree on the host, and a process starting beside it
+    # would slow the first timed solve
+    t_wait = time.perf_counter()
+    while sampler.proc and not sampler.lines and time.perf_counter() - t_wait < 3.0:
+        time.sleep(0.02)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
