@@ -440,10 +440,12 @@ def time_solves(ctx, verts, cond, ncond, solve_kw, steps, warmup, stream, dist, 
 # near entry plus 16 B per panel and right-hand side; M2L: each box's
 # expansion read once and its local expansion written once).  bench scales
 # the ratio by the algorithmic bytes of the launches it times.
-TRAFFIC_PER_ALGO_BYTE = {"near_apply": 1.163, "m2l": 0.968}
+TRAFFIC_PER_ALGO_BYTE = {"near_apply": 1.163, "m2l": 0.968,
+                         # shared-basis M2L: compress + 64 x 64 cores + decompress per apply
+                         "m2l_shared": 1.151}
 
 
-def roofline_of(ks, ms_total, m2l_engine):
+def roofline_of(ks, ms_total, m2l_engine, shared_m2l=False):
     """Roofline of the kernel class with the largest device time, the classes
     split by precision (the mixed path's FP32/TF32 launches apart from its
     FP64 refinement residuals).  M2L is measured as a dense contraction
@@ -459,7 +461,7 @@ def roofline_of(ks, ms_total, m2l_engine):
     per_launch_ms = k["ms"] / max(1, k["launches"])
     src = "measured (MEASURED_PEAKS.json)" if pk["kind"] == "measured" else "fallback"
     algo_bytes = k["bytes"] / max(1, k["launches"])
-    traffic = TRAFFIC_PER_ALGO_BYTE.get(top)
+    traffic = TRAFFIC_PER_ALGO_BYTE.get("m2l_shared" if (top == "m2l" and shared_m2l) else top)
     common = {"kernel": top, "peak_source": src,
               "traffic": traffic * algo_bytes if traffic else None, "launches": k["launches"],
               "ms_per_launch": per_launch_ms, "share_of_step": k["ms"] / ms_total if ms_total > 0 else None}
@@ -687,7 +689,7 @@ def main():
         else:
             engine = ("FP32 CUDA cores, factored low-rank operators" if head == "mixed" else
                       "FP64 CUDA cores, factored low-rank operators")
-        roof = roofline_of(hr["ks"], hr["ms_prof"], engine)
+        roof = roofline_of(hr["ks"], hr["ms_prof"], engine, shared_m2l)
         names = [k for k in hr["ks"] if k != "total_launches"]
         breakdown = {n: {"ms_per_step": hr["ks"][n]["ms"] / args.steps,
                          "launches_per_step": hr["ks"][n]["launches"] / args.steps}
