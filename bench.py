@@ -73,7 +73,8 @@ def parse():
                     help="mixed M2L: 0 auto, 1 factored on CUDA cores, 2 tensor cores also with Gauss sources, "
                          "3 shared rank-64 basis on the tensor cores (fastest, measured)")
     ap.add_argument("--mixed-far-tc", type=int, default=1,
-                    help="mixed: 1 P2M and L2P on the tensor cores (hi/lo split operands), 0 FP32 CUDA cores")
+                    help="mixed: 1 P2M and L2P on the tensor cores (hi/lo split operands), 2 P2M only, "
+                         "0 FP32 CUDA cores")
     ap.add_argument("--workload", default="window64", choices=["window64", "twowires", "batch", "bus", "block"],
                     help="window64: the headline 64-net window; twowires: two met1 wires on a 0.05 um mesh; "
                          "batch: many uneven windows in one batched call; bus: met2 bus sensitivities; "

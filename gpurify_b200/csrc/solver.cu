@@ -418,6 +418,7 @@ struct Operator {
     DBuf<float> P32, E32, L32, X32, W32, Sc32;
     DBuf<float> Xhi32, Xlo32;  // TF32 split of the FP32 apply's input (tensor-core near apply)
     bool p2m_tc = false;       // mixed: P2M on the tensor cores from the split weights below
+    bool l2p_tc = false;       // mixed, with p2m_tc: L2P on the tensor cores too
     DBuf<float> Whi32, Wlo32;  // TF32 split of the P2M weights (area folded in), N x 128
     DBuf<float> Shi32, Slo32;  // TF32 split of the L2P weights, N x 128
     DBuf<double> Sc;  // transposed operator: collocation weights as P2M weights
@@ -857,7 +858,8 @@ struct Operator {
                     launch_m2l_fac<float>(ctx, fac32, level < 0 ? fac_all : fac_level[level], b0, nb, L32.p, E32.p,
                                           Rb32, scale);
             };
-            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p, Shi32.p, Slo32.p};
+            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p, l2p_tc ? Shi32.p : nullptr,
+                              l2p_tc ? Slo32.p : nullptr};
             launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true,
                                     p2m_tc ? &sp : nullptr);
         }
@@ -1271,7 +1273,7 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
     if (o.precond < 0 || o.precond > 2) throw Error(GPX_ERR_INVALID_ARG, "precond must be 0, 1 or 2");
     if (o.mixed_near < 0 || o.mixed_near > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_near must be 0, 1, 2 or 3");
     if (o.mixed_m2l < 0 || o.mixed_m2l > 3) throw Error(GPX_ERR_INVALID_ARG, "mixed_m2l must be 0, 1, 2 or 3");
-    if (o.mixed_far_tc != 0 && o.mixed_far_tc != 1) throw Error(GPX_ERR_INVALID_ARG, "mixed_far_tc must be 0 or 1");
+    if (o.mixed_far_tc < 0 || o.mixed_far_tc > 2) throw Error(GPX_ERR_INVALID_ARG, "mixed_far_tc must be 0, 1 or 2");
     if (o.inner_basis32 != 0 && o.inner_basis32 != 1) throw Error(GPX_ERR_INVALID_ARG, "inner_basis32 must be 0 or 1");
     for (int64_t i = 0; i < n; ++i) {
         if (cond && (cond[i] < 0 || cond[i] >= ncond))
@@ -1304,8 +1306,9 @@ void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int 
     // expansions carry large alternating node values (sources slightly outside
     // their leaf box) and the TF32 inputs lose 1e-2 of the far field.
     pr.op->shared = o.precision == GPX_PREC_MIXED && o.mixed_m2l == 3 && (o.order == 5 || o.order == 6);
-    pr.op->p2m_tc = o.precision == GPX_PREC_MIXED && o.mixed_far_tc == 1 && o.mixed_near != 1 &&
+    pr.op->p2m_tc = o.precision == GPX_PREC_MIXED && o.mixed_far_tc >= 1 && o.mixed_near != 1 &&
                     (o.order == 4 || o.order == 5);
+    pr.op->l2p_tc = pr.op->p2m_tc && o.mixed_far_tc == 1;
     pr.op->tc32 = !pr.op->shared && o.precision == GPX_PREC_MIXED && o.mixed_m2l != 1 &&
                   (o.order == 4 || o.order == 5) &&
                   (o.far_quad == 0 || o.m2l_mode == GPX_M2L_EXACT || o.mixed_m2l >= 2);
@@ -1688,6 +1691,7 @@ void cap_sensitivity(Ctx& ctx, int64_t n, const double* verts, const int32_t* co
         opT->tc32 = op.tc32;
         opT->shared = op.shared;
         opT->p2m_tc = op.p2m_tc;
+        opT->l2p_tc = op.l2p_tc;
         // the transposed operator is assembled from the forward FP64 blocks;
         // the forward operator's FP32 state goes first, its FP64 blocks right
         // after, so that at most one operator's near blocks of each kind are

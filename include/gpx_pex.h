@@ -126,7 +126,7 @@ typedef struct {
     int32_t col_count;       /* 0 -> every column (all but the substrate with skip_ground_rhs) */
     int32_t mixed_far_tc;    /* mixed, orders 4 and 5, tensor-core near apply: 1 -> P2M and L2P on the tensor
                                 cores too (weights, charges and local expansions split into TF32 hi and lo
-                                parts, FP32-accurate) */
+                                parts, FP32-accurate); 2 -> P2M only (L2P on the FP32 CUDA cores) */
     int32_t inner_basis32;   /* mixed: 1 -> inner GMRES basis stored in FP32 (products, sums and the
                                 Hessenberg matrix stay FP64): twice the restart length in the same memory,
                                 for inner tolerances of 1e-3 (TF32 near apply); 0 -> FP64 */

@@ -85,17 +85,21 @@ def test_tensor_core_p2m_l2p_match_cuda_cores(ctx, order, far_quad, mixed_m2l, m
               mixed_near=mixed_near)
     y0, _ = ctx.operator_apply(p["verts"], sig, **kw)
     y1, _ = ctx.operator_apply(p["verts"], sig, mixed_far_tc=1, **kw)
+    y2, _ = ctx.operator_apply(p["verts"], sig, mixed_far_tc=2, **kw)  # P2M only
     y64, _ = ctx.operator_apply(p["verts"], sig, **dict(kw, precision=0, mixed_m2l=0, mixed_near=0))
     n64 = np.linalg.norm(y64, axis=0)
     d01 = np.linalg.norm(y1 - y0, axis=0) / np.linalg.norm(y0, axis=0)
     e0 = np.linalg.norm(y0 - y64, axis=0) / n64
     e1 = np.linalg.norm(y1 - y64, axis=0) / n64
+    e2 = np.linalg.norm(y2 - y64, axis=0) / n64
     if mixed_m2l == 1:
         assert d01.max() < 5e-5, d01.max()
+        assert e2.max() <= 2.0 * e0.max() + 1e-7, (e2.max(), e0.max())
         assert e1.max() <= 2.0 * e0.max() + 1e-7, (e1.max(), e0.max())
         assert e1.max() < 1e-4, e1.max()
     else:
         assert e1.max() < (2e-3 if mixed_m2l == 3 else 1e-3), e1.max()
+        assert e2.max() < (2e-3 if mixed_m2l == 3 else 1e-3), e2.max()
 
 
 def test_mixed_exact_m2l_needs_centroid_sources(ctx):
