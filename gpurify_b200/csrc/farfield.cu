@@ -689,7 +689,8 @@ inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b);
 
 template <class T, int N>
 void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y, int R,
-                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all, const P2MSplit* p2m_tc) {
+                 int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all, const P2MSplit* p2m_tc,
+                 bool l_written) {
     cudaStream_t s = c.stream;
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>();
     constexpr size_t smem = tree_smem<T, N>();
@@ -697,7 +698,8 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
     const double wb = (double)sizeof(T);
     const double box_bytes = wb * N3 * R;
     const unsigned rchunks64 = cdiv(Rb, 64), rchunks_tree = cdiv(Rb, RC);
-    launch_zero(c, L, (size_t)p.nbox * NS * Rb * sizeof(T));  // a kernel: also valid inside a device-side loop
+    if (!l_written)
+        launch_zero(c, L, (size_t)p.nbox * NS * Rb * sizeof(T));  // a kernel: also valid inside a device-side loop
     {
         KTimer t(c, prec_tag<T>(K_P2M), (double)p.N * (wb * R + wb * N3 + 8.0) + (p.nleaf + 2.0 * f.npart) * box_bytes,
                  2.0 * (double)p.N * N3 * R);
@@ -785,13 +787,13 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
                       int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all,
-                      const P2MSplit* p2m_tc) {
+                      const P2MSplit* p2m_tc, bool l_written) {
     switch (p.n) {
-        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
-        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
-        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
-        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
-        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc); break;
+        case 2: far_field_n<T, 2>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc, l_written); break;
+        case 3: far_field_n<T, 3>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc, l_written); break;
+        case 4: far_field_n<T, 4>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc, l_written); break;
+        case 5: far_field_n<T, 5>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc, l_written); break;
+        case 6: far_field_n<T, 6>(c, p, f, X, w, Y, R, Rb, E, L, coef, m2l, m2l_all, p2m_tc, l_written); break;
         default: throw Error(GPX_ERR_INVALID_ARG, "far field runs Chebyshev orders 2 to 6");
     }
 }
@@ -834,9 +836,9 @@ void launch_m2l64(Ctx& c, const DevPlan& p, int b0, int nb, double* L, const dou
 
 template void launch_far_field<double>(Ctx&, const DevPlan&, const FarLaunch&, const double*,
                                        const FarWeights<double>&, double*, int, int, double*, double*, double,
-                                       const M2LLevelFn<double>&, bool, const P2MSplit*);
+                                       const M2LLevelFn<double>&, bool, const P2MSplit*, bool);
 template void launch_far_field<float>(Ctx&, const DevPlan&, const FarLaunch&, const float*, const FarWeights<float>&,
                                       double*, int, int, float*, float*, double, const M2LLevelFn<float>&, bool,
-                                      const P2MSplit*);
+                                      const P2MSplit*, bool);
 
 }  // namespace gpx

@@ -47,7 +47,10 @@ struct P2MSplit {
 template <class T>
 void launch_far_field(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const FarWeights<T>& w, double* Y,
                       int R, int Rb, T* E, T* L, double coef, const M2LLevelFn<T>& m2l, bool m2l_all_levels = false,
-                      const P2MSplit* p2m_tc = nullptr);
+                      const P2MSplit* p2m_tc = nullptr, bool l_written = false);
+// l_written: the M2L callback overwrites every local-expansion row of levels
+// 2 and deeper (the shared-basis decompression does), and L's rows of levels
+// 0 and 1 are zero: L is then not cleared before the M2L.
 // Whi / Wlo [N][128] = TF32 split of (area if mul_area) x W[N][n3] (n3 <= 128).
 void launch_split_weights(Ctx& c, const double* W, int n3, const double* area, bool mul_area, float* Whi, float* Wlo,
                           int64_t N);

@@ -666,6 +666,8 @@ struct Operator {
                     ensure_shared(ctx, *const_cast<DevM2L*>(m2l));
                     Eh32.alloc((size_t)pl.nbox() * Rb32 * kShared, s);
                     Lh32.alloc((size_t)pl.nbox() * Rb32 * kShared, s);
+                    Lh32.zero();
+                    L32.zero();
                 }
             }
         }
@@ -846,8 +848,9 @@ struct Operator {
                     // E^ = V^T E, L^ = sum_o C_o E^ (tensor cores), L = U L^ for the boxes [b0, b0 + nb)
                     const int ns = node_stride(pl.n);
                     const int64_t row0 = (int64_t)b0 * Rb32, nrows = (int64_t)nb * Rb32;
+                    // L^ rows of boxes with M2L work are overwritten; the others stay
+                    // at the zero they were allocated with
                     launch_m2l_compress(ctx, E32.p, ns, m2l->Vt_hi.p, m2l->Vt_lo.p, Eh32.p, row0, nrows, tc_err.p);
-                    launch_zero(ctx, Lh32.p + row0 * kShared, (size_t)nrows * kShared * sizeof(float));
                     launch_m2l_tc(ctx, level < 0 ? tc.all : tc.level[level], kShared, Eh32.p, Lh32.p, m2l->C32.p,
                                   Rb32, (float)scale, level < 0 ? box_scale.p : nullptr, tc_err.p);
                     launch_m2l_decompress(ctx, Lh32.p, m2l->U_hi.p, m2l->U_lo.p, ns, L32.p, row0, nrows, tc_err.p);
@@ -860,8 +863,10 @@ struct Operator {
             };
             const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p, l2p_tc ? Shi32.p : nullptr,
                               l2p_tc ? Slo32.p : nullptr};
+            // the shared-basis decompression overwrites every local expansion of
+            // levels 2 and deeper (L and L^ were cleared once, when allocated)
             launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true,
-                                    p2m_tc ? &sp : nullptr);
+                                    p2m_tc ? &sp : nullptr, shared);
         }
     }
 
