@@ -356,7 +356,10 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
     p.ncond = ncond;
     p.far = depth >= 2;
     // centroids / areas in caller order
-    std::vector<double> c0((size_t)N * 3), a0(N);
+    // scratch of this thread, kept between calls (no fresh pages per solve)
+    thread_local std::vector<double> c0, a0;
+    c0.resize((size_t)N * 3);
+    a0.resize((size_t)N);
     for (int64_t i = 0; i < N; ++i) panel_centroid_area(verts + 12 * i, &c0[3 * i], &a0[i]);
     // cubic bounding box (fmm/tree.rs:43-62)
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -377,8 +380,10 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
     const double origin[3] = {center[0] - half, center[1] - half, center[2] - half};
     for (int dd = 0; dd < 3; ++dd) p.origin[dd] = origin[dd];
     // leaf cell per panel (fmm/tree.rs:86-95)
-    std::vector<uint32_t> cell((size_t)N * 3);
-    std::vector<uint64_t> key(N);
+    thread_local std::vector<uint32_t> cell;
+    thread_local std::vector<uint64_t> key;
+    cell.resize((size_t)N * 3);
+    key.resize((size_t)N);
     for (int64_t i = 0; i < N; ++i) {
         for (int d = 0; d < 3; ++d) {
             long long idx = (long long)std::floor((c0[3 * i + d] - origin[d]) / leaf_size);

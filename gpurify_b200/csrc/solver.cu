@@ -1291,11 +1291,25 @@ static void check_problem(int64_t n, const double* verts, const int32_t* cond, i
 
 namespace {
 
+// Host plans of one thread reuse the storage of the thread's previous plan:
+// build_plan overwrites every field, and the pages of its vectors are
+// already mapped, which saves the page faults of tens of MB per solve.  One
+// plan per thread is kept between calls.
+thread_local std::unique_ptr<Plan> t_spare_plan;
+
 struct Prepared {
-    Plan plan;
+    std::unique_ptr<Plan> plan_owner;
+    Plan& plan;
     std::shared_ptr<DevM2L> m2l;
     DevPlanBufs dp;
     std::unique_ptr<Operator> op;
+    Prepared()
+        : plan_owner(t_spare_plan ? std::move(t_spare_plan) : std::unique_ptr<Plan>(new Plan())), plan(*plan_owner) {}
+    // the plan goes back to the thread's spare slot; op and dp, destroyed
+    // after this body, still find it alive there
+    ~Prepared() { t_spare_plan = std::move(plan_owner); }
+    Prepared(const Prepared&) = delete;
+    Prepared& operator=(const Prepared&) = delete;
 };
 
 void prepare(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, int R,

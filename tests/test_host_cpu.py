@@ -130,6 +130,22 @@ def test_plan_covers_every_pair_once(depth):
         assert st["m2l_box_pairs"] == 0
 
 
+def test_plan_rebuilt_after_another_problem_is_identical():
+    """The plan builder keeps its per-thread scratch between calls: a plan
+    built after a larger and a smaller problem equals the first build, and
+    still covers every panel pair exactly once."""
+    def panels(nets, side, seed):
+        lay = layouts.routing_window(nets, side, seed=seed)
+        return _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                    mesh_max_edge_m=0.4e-6, max_panels=-1)["verts"]
+
+    a, big, small = panels(8, 10.0, 3), panels(24, 20.0, 4), panels(3, 5.0, 5)
+    first = _lib.plan_check(a, 5, 4)
+    _lib.plan_check(big, 5, 5)
+    _lib.plan_check(small, 4, 3)
+    assert _lib.plan_check(a, 5, 4) == first
+
+
 def test_sensitivity_velocity_fields():
     """Width stretches one wire across its axis (long sides +-1/2), spacing
     translates the same-layer wires past it, thickness moves top faces by +1
