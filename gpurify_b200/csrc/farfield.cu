@@ -768,7 +768,7 @@ void far_field_n(Ctx& c, const DevPlan& p, const FarLaunch& f, const T* X, const
         KTimer t(c, prec_tag<T>(K_L2P), (double)p.N * (16.0 * R + 24.0 * N) + p.nleaf * box_bytes, 2.0 * (double)p.N * N3 * R);
         bool done = false;
         if constexpr (sizeof(T) == 4 && (N == 4 || N == 5)) {
-            if (p2m_tc && p2m_tc->l2p) {
+            if (p2m_tc && p2m_tc->shi) {
                 launch_l2p_tc(c, p, reinterpret_cast<const float*>(L), p2m_tc->shi, p2m_tc->slo, Y, R, Rb, coef,
                               p2m_tc->err);
                 done = true;

@@ -39,10 +39,8 @@ struct P2MSplit {
     const float* xhi = nullptr;
     const float* xlo = nullptr;
     int* err = nullptr;
-    // L2P on the tensor cores too when l2p: the target weights split into
-    // TF32 hi and lo parts (rows of 128 nodes), or, with shi null, the
-    // centroids' separable weights formed on chip from the plan's 1-D weights
-    bool l2p = false;
+    // L2P on the tensor cores too when given: the target weights split into
+    // TF32 hi and lo parts (rows of 128 nodes)
     const float* shi = nullptr;
     const float* slo = nullptr;
 };

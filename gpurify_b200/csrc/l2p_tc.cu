@@ -83,19 +83,12 @@ __device__ __forceinline__ float to_tf32(float x) {
     return __uint_as_float(r);
 }
 
-// sep: the target weights are the centroids' separable Chebyshev weights,
-// S[j][(a n + b) n + c] = wx[a] wy[b] wz[c] from the plan's 1-D weights
-// (p.w1d), formed in FP64 and split into TF32 hi and lo in shared memory
-// (Shi, Slo unused): 15 doubles per panel instead of two 128-float rows.
 template <int NS>
 __global__ void __launch_bounds__(kThreads) k_l2p_tc(DevPlan p, const float* __restrict__ L,
                                                      const float* __restrict__ Shi, const float* __restrict__ Slo,
-                                                     bool sep, double* __restrict__ Y, int R, int Rb, double coef,
+                                                     double* __restrict__ Y, int R, int Rb, double coef,
                                                      int* __restrict__ err) {
     constexpr int nsl = NS / 32;
-    constexpr int N = NS == 64 ? 4 : 5;  // Chebyshev order of the node stride
-    constexpr int N3 = N * N * N;
-    __shared__ double wv[64][3 * N];
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -120,39 +113,21 @@ __global__ void __launch_bounds__(kThreads) k_l2p_tc(DevPlan p, const float* __r
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (sep)
-        for (int e = tid; e < cnt * 3 * N; e += kThreads) wv[e / (3 * N)][e % (3 * N)] = p.w1d[jb * 3 * N + e];
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tslot;
-    // slice q into stage q % 2: A rows = the item's panels (rows past cnt are
-    // not filled: their D rows are never stored), copied pre-split or formed
-    // here; B rows = the leaf's right-hand sides (all 64 rows valid: L has Rb
-    // rows per box), copied and split once they landed
+    // copies of slice q into stage q % 2: A rows = the item's panels (rows
+    // past cnt are not loaded: their D rows are never stored), B rows = the
+    // leaf's right-hand sides (all 64 rows valid: L has Rb rows per box)
     auto issue = [&](int q) {
         const uint32_t a = base + (uint32_t)(q & 1) * kStage;
-        uint8_t* as = sbase + (size_t)(q & 1) * kStage;
         for (int e = tid; e < 64 * 8; e += kThreads) {
             const int row = e >> 3, c = e & 7;
             if (row < cnt) {
-                if (sep) {
-                    float h[4], l[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int m = 32 * q + 4 * c + u;
-                        double v = 0.0;
-                        if (m < N3) v = wv[row][m / (N * N)] * wv[row][N + (m / N) % N] * wv[row][2 * N + m % N];
-                        h[u] = to_tf32((float)v);
-                        l[u] = to_tf32((float)(v - (double)h[u]));
-                    }
-                    *reinterpret_cast<float4*>(as + swz(row, c)) = make_float4(h[0], h[1], h[2], h[3]);
-                    *reinterpret_cast<float4*>(as + kATile + swz(row, c)) = make_float4(l[0], l[1], l[2], l[3]);
-                } else {
-                    const int64_t off = (jb + row) * kWS + 32 * q + 4 * c;
-                    cp16(a + swz(row, c), Shi + off, true);
-                    cp16(a + kATile + swz(row, c), Slo + off, true);
-                }
+                const int64_t off = (jb + row) * kWS + 32 * q + 4 * c;
+                cp16(a + swz(row, c), Shi + off, true);
+                cp16(a + kATile + swz(row, c), Slo + off, true);
             }
             cp16(a + 2 * kATile + swz(row, c), src + (int64_t)row * NS + 32 * q + 4 * c, true);
         }
@@ -261,16 +236,15 @@ __global__ void __launch_bounds__(kThreads) k_l2p_tc(DevPlan p, const float* __r
 
 void launch_l2p_tc(Ctx& c, const DevPlan& p, const float* L, const float* Shi, const float* Slo, double* Y, int R,
                    int Rb, double coef, int* err) {
-    const bool sep = Shi == nullptr;  // centroid weights formed from the plan's 1-D weights
     if (p.nitems == 0) return;
     if (R % 4 != 0 || Rb % 64 != 0) throw Error(GPX_ERR_INTERNAL, "tensor-core L2P needs R % 4 == 0, Rb % 64 == 0");
     const dim3 grid(p.nitems, (R + 63) / 64);
     if (p.ns == 128) {
         set_smem_once(k_l2p_tc<128>, (int)kSmemBytes);
-        k_l2p_tc<128><<<grid, kThreads, kSmemBytes, c.stream>>>(p, L, Shi, Slo, sep, Y, R, Rb, coef, err);
+        k_l2p_tc<128><<<grid, kThreads, kSmemBytes, c.stream>>>(p, L, Shi, Slo, Y, R, Rb, coef, err);
     } else if (p.ns == 64) {
         set_smem_once(k_l2p_tc<64>, (int)kSmemBytes);
-        k_l2p_tc<64><<<grid, kThreads, kSmemBytes, c.stream>>>(p, L, Shi, Slo, sep, Y, R, Rb, coef, err);
+        k_l2p_tc<64><<<grid, kThreads, kSmemBytes, c.stream>>>(p, L, Shi, Slo, Y, R, Rb, coef, err);
     } else {
         throw Error(GPX_ERR_INTERNAL, "tensor-core L2P runs node strides 64 and 128 (orders 4 and 5)");
     }

@@ -647,13 +647,16 @@ struct Operator {
                 if (p2m_tc) {
                     Whi32.alloc((size_t)pl.N * 128, s);
                     Wlo32.alloc((size_t)pl.N * 128, s);
+                    Shi32.alloc((size_t)pl.N * 128, s);
+                    Slo32.alloc((size_t)pl.N * 128, s);
                     if (!transposed) {
-                        // P2M: source weights with the area; L2P: the centroids' separable
-                        // collocation weights, formed by the L2P kernel from the 1-D weights
+                        // P2M: source weights with the area; L2P: collocation weights at the centroids
                         launch_split_weights(ctx, d.wsrc.p, pl.n3, d.area.p, true, Whi32.p, Wlo32.p, pl.N);
+                        DBuf<double> S64;
+                        S64.alloc((size_t)pl.N * pl.n3, s);
+                        launch_centroid_weights(ctx, d.v, nullptr, S64.p);
+                        launch_split_weights(ctx, S64.p, pl.n3, d.area.p, false, Shi32.p, Slo32.p, pl.N);
                     } else {
-                        Shi32.alloc((size_t)pl.N * 128, s);
-                        Slo32.alloc((size_t)pl.N * 128, s);
                         launch_split_weights(ctx, Sc.p, pl.n3, d.area.p, false, Whi32.p, Wlo32.p, pl.N);
                         launch_split_weights(ctx, d.wsrc.p, pl.n3, d.area.p, true, Shi32.p, Slo32.p, pl.N);
                     }
@@ -858,7 +861,8 @@ struct Operator {
                     launch_m2l_fac<float>(ctx, fac32, level < 0 ? fac_all : fac_level[level], b0, nb, L32.p, E32.p,
                                           Rb32, scale);
             };
-            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p, l2p_tc, Shi32.p, Slo32.p};
+            const P2MSplit sp{Whi32.p, Wlo32.p, Xhi32.p, Xlo32.p, tc_err.p, l2p_tc ? Shi32.p : nullptr,
+                              l2p_tc ? Slo32.p : nullptr};
             // the shared-basis decompression overwrites every local expansion of
             // levels 2 and deeper (L and L^ were cleared once, when allocated)
             launch_far_field<float>(ctx, d.v, d.far, X32.p, w32, Y, R, Rb32, E32.p, L32.p, kCoulomb, m2l_fn, true,
