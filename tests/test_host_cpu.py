@@ -1,5 +1,6 @@
 """CPU tests of the product library's host side: the C ABI loads and exports
-every symbol include/gpx_pex.h declares; the bridge panelisation is bit-exact
+every symbol include/gpx_pex.h declares, and the Python binding's structs have
+the header's layout; the bridge panelisation is bit-exact
 with the oracle; the octree plan covers every panel pair exactly once; bridge
 errors carry the reference's messages (bridge.rs:35-56, rects.rs:10-31)."""
 import re
@@ -24,6 +25,43 @@ def test_header_symbols_exported():
     L = _lib.load()
     for name in declared:
         assert hasattr(L, name), name
+
+
+ABI_STRUCTS = {
+    "gpx_solve_opts": _lib.SolveOpts, "gpx_solve_report": _lib.SolveReport, "gpx_tune_report": _lib.TuneReport,
+    "gpx_panel_problem": _lib.PanelProblem, "gpx_volume_group": _lib.VolumeGroup,
+    "gpx_geometry_store": _lib.GeometryStoreC, "gpx_layer_params": _lib.LayerParamsC, "gpx_deck": _lib.DeckC,
+    "gpx_net_parasitics": _lib.NetParasiticsC,
+}
+
+
+def test_ctypes_structs_match_header_layout(tmp_path):
+    """Every struct the Python binding passes across the ABI has the size and
+    field offsets the C compiler gives the header's declaration."""
+    import ctypes
+    import os
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "gpx_pex.h"', "int main(void) {"]
+    for cname, py in ABI_STRUCTS.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                  text=True).stdout.splitlines())
+    for cname, py in ABI_STRUCTS.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
 
 
 def test_no_device_is_reported_not_faked():
