@@ -45,10 +45,17 @@ __global__ void __launch_bounds__(kRedThreads) k_multidot(const TA* __restrict__
                     for (int q = 0; q < kV; ++q) acc[q] += (double)A0[q * strideA + o] * b;
                 }
             } else {
+                // The last chunk of fewer than eight vectors (and the column
+                // norms, one vector): fully unrolled and predicated, so the
+                // accumulators stay in registers and the loads of a row issue
+                // together.  Same rows, same order as the loop over nv.
+#pragma unroll 2
                 for (int64_t n = n0 + sub; n < n1; n += nsub) {
                     const int64_t o = n * R + r;
                     const double b = B[o];
-                    for (int q = 0; q < nv; ++q) acc[q] += (double)A0[q * strideA + o] * b;
+#pragma unroll
+                    for (int q = 0; q < kV; ++q)
+                        if (q < nv) acc[q] += (double)A0[q * strideA + o] * b;
                 }
             }
         }
