@@ -30,6 +30,16 @@ __device__ __forceinline__ void cp16(void* dst, const void* src, bool valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
 
+// One 4- or 8-byte element copied global -> shared asynchronously: a CTA
+// puts all its copies in flight before one wait instead of a load round trip
+// per loop pass.
+template <class T>
+__device__ __forceinline__ void cp_elem(T* dst, const T* src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async.ca copies 4, 8 or 16 bytes");
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"((int)sizeof(T)) : "memory");
+}
+
 // Panels per near-field work item (the plan's kRowsPerItem).
 constexpr int kItemPanels = 64;
 
@@ -244,6 +254,13 @@ template <class T, int N>
 constexpr size_t tree_smem() {
     return sizeof(T) * (size_t)(8 + 4 + 2) * tree_rc<T, N>() * Ord<N>::n3;
 }
+// Resident M2M / L2L blocks per SM asked of the register allocator: three
+// for FP32 order 5 (56 KB of shared memory each), where the default
+// allocation (80-92 registers) leaves two.
+template <class T, int N>
+constexpr int tree_min_blocks() {
+    return (sizeof(T) == 4 && N == 5) ? 3 : 1;
+}
 
 // 1-D operators of the three axes as T: M1[axis][bit][m][k] (m parent node,
 // k child node), from the plan's per-octant table mat[(o*3+axis)*n*n + m*n + k].
@@ -262,7 +279,7 @@ __device__ __forceinline__ void load_m1(const double* m2m1d, T (*M1)[2][N * N]) 
 // E_par = sum_ox X_ox C[ox].  The parent row is overwritten (the parent has
 // no other contribution), padding nodes written as zero.
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_m2m_tree(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
+__global__ void __launch_bounds__(256, tree_min_blocks<T, N>()) k_m2m_tree(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
                                                   const int32_t* __restrict__ child_count, T* __restrict__ E, int Rb) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>(), NN = N * N;
     const int pb = pb0 + blockIdx.x;
@@ -273,18 +290,19 @@ __global__ void __launch_bounds__(256) k_m2m_tree(DevPlan p, int pb0, const int3
     T* B = A + 8 * RC * N3;                      // [4][RC][N3]
     T* C = B + 4 * RC * N3;                      // [2][RC][N3]
     __shared__ T M1[3][2][NN];
+    __shared__ int oct_s[8];
     load_m1<T, N>(p.m2m1d, M1);
-    const int cf = child_first[pb], cc = child_count[pb];
+    const int cf = child_first[pb], cc = child_count[pb];  // cc <= 8 (octree)
+    if (threadIdx.x < cc) oct_s[threadIdx.x] = p.box_octant[cf + threadIdx.x];
     for (int e = threadIdx.x; e < 8 * RC * N3; e += blockDim.x) A[e] = (T)0;
     __syncthreads();
-    for (int ch = cf; ch < cf + cc; ++ch) {
-        const int oc = p.box_octant[ch];
-        const T* src = E + ((int64_t)ch * Rb + r0) * NS;
-        for (int e = threadIdx.x; e < rc * N3; e += blockDim.x) {
-            const int r = e / N3, m = e % N3;
-            A[(oc * RC + r) * N3 + m] = src[(int64_t)r * NS + m];
-        }
+    // every child row of the chunk in flight at once, then one wait
+    const int per = rc * N3;
+    for (int e = threadIdx.x; e < cc * per; e += blockDim.x) {
+        const int k = e / per, rm = e - k * per, r = rm / N3, m = rm - r * N3;
+        cp_elem(A + (oct_s[k] * RC + r) * N3 + m, E + ((int64_t)(cf + k) * Rb + r0 + r) * NS + m);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     // Each stage runs one 1-D line per thread (the n values along the
     // contracted axis), so the index arithmetic is per line, not per value.
@@ -361,23 +379,40 @@ __global__ void __launch_bounds__(256) k_m2m_tree(DevPlan p, int pb0, const int3
 // C[ox] = X_ox^T L_par; B[ox|oy<<1] = Y_oy^T C[ox]; child of octant oct:
 // L_child += Z_oz^T B[oct & 3].
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_l2l_tree(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
+__global__ void __launch_bounds__(256, tree_min_blocks<T, N>()) k_l2l_tree(DevPlan p, int pb0, const int32_t* __restrict__ child_first,
                                                   const int32_t* __restrict__ child_count, T* __restrict__ L, int Rb) {
     constexpr int N3 = Ord<N>::n3, NS = Ord<N>::ns, RC = tree_rc<T, N>(), NN = N * N;
     const int pb = pb0 + blockIdx.x;
     const int r0 = blockIdx.y * RC;
     const int rc = min(RC, Rb - r0);
     extern __shared__ __align__(16) unsigned char tree_smem_raw[];
-    T* P = reinterpret_cast<T*>(tree_smem_raw);  // [RC][N3]
-    T* B = P + 8 * RC * N3;                      // [4][RC][N3]
-    T* C = B + 4 * RC * N3;                      // [2][RC][N3]
+    T* Ch = reinterpret_cast<T*>(tree_smem_raw);  // [8][RC][N3]: the children's rows of the chunk
+    T* B = Ch + 8 * RC * N3;                      // [4][RC][N3]
+    T* C = B + 4 * RC * N3;                       // [2][RC][N3]
+    T* P = B;                                     // [RC][N3]: the parent, dead once C is formed
     __shared__ T M1[3][2][NN];
+    __shared__ int oct_s[8];
     load_m1<T, N>(p.m2m1d, M1);
+    const int cf = child_first[pb], cc = child_count[pb];  // cc <= 8 (octree)
+    if (threadIdx.x < cc) oct_s[threadIdx.x] = p.box_octant[cf + threadIdx.x];
     const T* src = L + ((int64_t)pb * Rb + r0) * NS;
     for (int e = threadIdx.x; e < RC * N3; e += blockDim.x) {
         const int r = e / N3, m = e % N3;
-        P[e] = r < rc ? src[(int64_t)r * NS + m] : (T)0;
+        if (r < rc)
+            cp_elem(P + e, src + (int64_t)r * NS + m);
+        else
+            P[e] = (T)0;
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    // The children's current rows, needed only by the last stage: their
+    // copies stay in flight through the x and y stages.
+    const int per = rc * N3;
+    for (int e = threadIdx.x; e < cc * per; e += blockDim.x) {
+        const int k = e / per, rm = e - k * per, r = rm / N3, m = rm - r * N3;
+        cp_elem(Ch + (k * RC + r) * N3 + m, L + ((int64_t)(cf + k) * Rb + r0 + r) * NS + m);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
     // x: C[ox][r][(a,b,c)] = sum_a' X_ox[a'][a] P[r][(a',b,c)]  (one line per thread)
     for (int e = threadIdx.x; e < RC * NN; e += blockDim.x) {
@@ -418,14 +453,15 @@ __global__ void __launch_bounds__(256) k_l2l_tree(DevPlan p, int pb0, const int3
             }
         }
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     // z, straight into each existing child: L_child[r][(a,b,c)] += sum_c' Z_oz[c'][c] B[oct&3][r][(a,b,c')]
-    const int cf = child_first[pb], cc = child_count[pb];
     for (int e = threadIdx.x; e < cc * rc * NN; e += blockDim.x) {
         const int k = e / (rc * NN), r = (e / NN) % rc, ab = e % NN;
         const int ch = cf + k;
-        const int oc = p.box_octant[ch], q = oc & 3, oz = oc >> 2;
+        const int oc = oct_s[k], q = oc & 3, oz = oc >> 2;
         const T* br = B + (q * RC + r) * N3 + ab * N;
+        const T* old = Ch + (k * RC + r) * N3 + ab * N;
         T x[N];
 #pragma unroll
         for (int cp = 0; cp < N; ++cp) x[cp] = br[cp];
@@ -435,7 +471,7 @@ __global__ void __launch_bounds__(256) k_l2l_tree(DevPlan p, int pb0, const int3
             T s = (T)0;
 #pragma unroll
             for (int cp = 0; cp < N; ++cp) s += M1[2][oz][cp * N + c] * x[cp];
-            dst[c] += s;
+            dst[c] = old[c] + s;
         }
     }
 }
