@@ -229,6 +229,27 @@ class Context:
         self._check(self.L.gpx_cap_solve(self.h, C.byref(pb), C.byref(opts(**kw)), Cm.ctypes.data, C.byref(rep)))
         return Cm, rep.as_dict()
 
+    def cap_solve_groups(self, groups, rects, xy_scale_m, **kw):
+        """gpx_cap_solve_groups (bridge.rs:307-443 `solve_capacitance`).
+        ``groups``: (net, z0_m, z1_m, dielectric_k, rect_offset, rect_count)
+        tuples in BTreeMap<(net, layer)> order; ``rects``: (n, 4) int32 DBU
+        rectangles (x0, y0, x1, y1).  Returns (nets, cap_af, maxwell, report):
+        per net (ascending id) C[i][i] in aF, and the k-scaled Maxwell matrix
+        in farads (last row/column = substrate)."""
+        g = (VolumeGroup * max(1, len(groups)))(*[VolumeGroup(*t) for t in groups])
+        r = np.ascontiguousarray(rects, dtype=np.int32).reshape(-1, 4)
+        cap = max(1, len({t[0] for t in groups}))
+        nets = np.zeros(cap, dtype=np.uint32)
+        af = np.zeros(cap)
+        mw = np.zeros((cap + 1) * (cap + 1))
+        n = C.c_int64()
+        rep = SolveReport()
+        self._check(self.L.gpx_cap_solve_groups(self.h, g, len(groups), r.ctypes.data, float(xy_scale_m),
+                                                C.byref(opts(**kw)), nets.ctypes.data, af.ctypes.data, cap,
+                                                C.byref(n), mw.ctypes.data, C.byref(rep)))
+        k = n.value
+        return nets[:k].copy(), af[:k].copy(), mw[: (k + 1) * (k + 1)].reshape(k + 1, k + 1), rep.as_dict()
+
     def autotune(self, verts, cond, ncond, target=1e-4, cache_path=None, **kw):
         """gpx_autotune: returns (options dict to pass to cap_solve, report)."""
         v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)

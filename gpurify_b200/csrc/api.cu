@@ -76,16 +76,22 @@ std::vector<VolumeGroup> groups_from_abi(const gpx_volume_group* g, int64_t n, c
 }
 
 // Maxwell solve of panelised groups with the bridge's k scaling and per-net
-// diagonal extraction (bridge.rs:393-442).
+// diagonal extraction (bridge.rs:393-442).  One k everywhere: the vacuum
+// solve scaled by that k.  Several k: every panel is a conductor panel in its
+// own surrounding k and its charge counts k times (bridge.rs:409-430 ->
+// cap/dielectric.rs:76-150 with conductor roles); the reference takes that
+// path only below 500 panels (all pairs), this solver at any size.
 void solve_panelized(Ctx& ctx, const PanelizeResult& pr, const Opts& o, std::vector<double>& C,
                      gpx_solve_report* rep) {
     const int ncond = (int)pr.nets.size() + 1;
-    if (!pr.homogeneous)
-        throw Error(GPX_ERR_CAPACITANCE,
-                    "non-homogeneous dielectric stacks are not supported by the GPU field solver");
     C.assign((size_t)ncond * ncond, 0.0);
-    cap_solve(ctx, pr.panels.size(), pr.panels.verts.data(), pr.panels.cond.data(), ncond, o, C.data(), rep);
-    for (double& v : C) v *= pr.first_eps;
+    if (pr.homogeneous) {
+        cap_solve(ctx, pr.panels.size(), pr.panels.verts.data(), pr.panels.cond.data(), ncond, o, C.data(), rep);
+        for (double& v : C) v *= pr.first_eps;
+    } else {
+        cap_solve(ctx, pr.panels.size(), pr.panels.verts.data(), pr.panels.cond.data(), ncond, o, C.data(), rep,
+                  pr.panels.eps.data());
+    }
     for (size_t i = 0; i < pr.nets.size(); ++i) {
         const double af = C[i * ncond + i] * 1.0e18;
         if (!std::isfinite(af) || af < 0.0)

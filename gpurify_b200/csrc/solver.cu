@@ -1462,7 +1462,7 @@ __global__ void k_rhs_areas(const int32_t* __restrict__ cond, const double* __re
 }  // namespace
 
 void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, double* C,
-               gpx_solve_report* rep) {
+               gpx_solve_report* rep, const double* panel_eps) {
     const double t0 = now_s();
     const int64_t l0 = ctx.launches;
     check_problem(n, verts, cond, ncond, o);
@@ -1485,6 +1485,21 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     Prepared pr;
     prepare(ctx, n, verts, cond, ncond, o, R, depth, pr);
     Operator& op = *pr.op;
+    // charge weight of each panel in the solver's order: its area, or its
+    // area times its own permittivity
+    const double* d_weight = pr.dp.area.p;
+    DBuf<double> eps_area;
+    if (panel_eps) {
+        std::vector<double> w(n);
+        for (int64_t k = 0; k < n; ++k) {
+            const double e = panel_eps[pr.plan.perm[k]];
+            if (!std::isfinite(e) || e <= 0.0)
+                throw Error(GPX_ERR_INVALID_ARG, "panel permittivities must be finite and positive");
+            w[k] = pr.plan.area[k] * e;
+        }
+        eps_area.upload(w, ctx.stream);
+        d_weight = eps_area.p;
+    }
     GPX_CUDA(cudaStreamSynchronize(ctx.stream));
     const double t1 = now_s();
     SolveStats st;
@@ -1511,7 +1526,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
         dC.alloc((size_t)ncond * R, ctx.stream);
         {
             KTimer kt(ctx, K_VEC, (8.0 * R + 12.0) * (double)n, 2.0 * (double)n * R);
-            k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, pr.dp.area.p, X.p, n, R, dC.p);
+            k_accum_c<<<ncond, 256, 0, ctx.stream>>>(pr.dp.cond.p, d_weight, X.p, n, R, dC.p);
             GPX_LAUNCH_CHECK();
             ctx.launches += 1;
         }
@@ -1527,7 +1542,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
             double v;
             if (j >= cb && j < cb + Rn)
                 v = hc[(size_t)i * Rn + (j - cb)];
-            else if (full && i < Rn)
+            else if (full && i < Rn && !panel_eps)
                 v = hc[(size_t)j * Rn + i];  // substrate column by symmetry
             else
                 v = std::nan("");

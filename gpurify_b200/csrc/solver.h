@@ -35,8 +35,13 @@ int choose_depth(const Opts& o, int64_t n, const double* verts);
 
 // Solve the Maxwell matrix of a panel problem (farads, not k-scaled) into C
 // (ncond x ncond row-major).  Columns not solved are filled by symmetry.
+// With panel_eps (n values, caller panel order) each panel's charge counts
+// with its own relative permittivity, C[i][j] = sum_{k on i} eps_k sigma_k a_k
+// (the bridge's solve of a stack of several k, bridge.rs:409-430 ->
+// cap/dielectric.rs:76-150 with conductor roles): C is then k-scaled, not
+// symmetric, and columns not solved are NaN.
 void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, int ncond, const Opts& o, double* C,
-               gpx_solve_report* rep);
+               gpx_solve_report* rep, const double* panel_eps = nullptr);
 
 // Maxwell matrix C and its derivatives dC/dp for np vertex velocity fields V
 // (np x n x 12, caller panel order): one forward and one transposed solve

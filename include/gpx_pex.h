@@ -290,7 +290,12 @@ typedef struct {
 /* Replaces bridge.rs:307-443 `solve_capacitance`: groups in the caller's
  * BTreeMap<(net, layer)> order.  Outputs per net (ascending net id) the net id
  * and C[i][i] in aF (scaled by k), and optionally the full (nets+1)^2 Maxwell
- * matrix in farads (k-scaled; last row/column = substrate). */
+ * matrix in farads (k-scaled; last row/column = substrate).  Groups of several
+ * k: each panel's charge is scaled by its own group's k (the substrate's by the
+ * lowest group's), as bridge.rs:409-430 does through cap/dielectric.rs:76-150;
+ * the reference allows that only below 500 panels, this call at any size.
+ * That matrix is not symmetric, so with skip_ground_rhs its substrate column
+ * is NaN instead of filled by symmetry. */
 gpx_status gpx_cap_solve_groups(gpx_ctx* ctx, const gpx_volume_group* groups, int64_t n_groups,
                                 const int32_t* rects, double xy_scale_m, const gpx_solve_opts* opts,
                                 uint32_t* nets_out, double* cap_af_out, int64_t nets_cap, int64_t* n_nets,

@@ -101,6 +101,7 @@ def lib():
                                           C.c_char_p, C.c_int64]
         L.orc_cap_dense.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
         L.orc_cap_dense_gmres.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+        L.orc_cap_dense_eps.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         L.orc_cap_fmm.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(FmmOpts), C.c_void_p,
                                   C.POINTER(FmmReport)]
         L.orc_fmm_new.restype = C.c_void_p
@@ -229,6 +230,22 @@ def cap_dense(verts, cond, ncond) -> np.ndarray:
     rc = lib().orc_cap_dense(len(v), v.ctypes.data, c.ctypes.data, ncond, C_.ctypes.data)
     if rc != 0:
         raise RuntimeError(f"orc_cap_dense rc={rc}")
+    return C_
+
+
+def cap_dense_eps(verts, cond, ncond, eps) -> np.ndarray:
+    """The bridge's solve for a stack of several k (bridge.rs:409-430 ->
+    cap/dielectric.rs:76-150, conductor roles only): dense Wilton P + LU, each
+    panel's charge weighted by its surrounding permittivity ``eps`` (per panel,
+    caller order).  Already k-scaled: no further multiplication by k."""
+    v, c = _prep(verts, cond)
+    e = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
+    if e.shape != (len(v),):
+        raise ValueError("eps needs one value per panel")
+    C_ = np.zeros((ncond, ncond))
+    rc = lib().orc_cap_dense_eps(len(v), v.ctypes.data, c.ctypes.data, ncond, e.ctypes.data, C_.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"orc_cap_dense_eps rc={rc}")
     return C_
 
 

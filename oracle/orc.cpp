@@ -1500,6 +1500,26 @@ int orc_cap_dense(int64_t n, const double* verts, const int32_t* cond, int32_t n
     return 0;
 }
 
+// cap/dielectric.rs:76-150 with conductor roles only, as the bridge calls it
+// for a stack of several k (bridge.rs:409-430): the same potential rows and
+// unit-conductor right-hand sides as the homogeneous solve, but each panel's
+// charge counts with its own surrounding permittivity,
+// C[id][j] += eps_k * sigma_k * a_k.
+int orc_cap_dense_eps(int64_t n, const double* verts, const int32_t* cond, int32_t ncond, const double* eps,
+                      double* C) {
+    if (n <= 0) return -1;
+    PanelSet s = build_set(n, verts, cond);
+    std::vector<double> p = assemble_p(s);
+    LU f = lu_factor(p, (size_t)n);
+    if (!f.ok) return -2;
+    std::fill(C, C + (size_t)ncond * ncond, 0.0);
+    for (int j = 0; j < ncond; ++j) {
+        std::vector<double> x = lu_solve(f, rhs_unit(s, j));
+        for (size_t k = 0; k < s.size(); ++k) C[(size_t)s.cond[k] * ncond + j] += eps[k] * x[k] * s.ar[k];
+    }
+    return 0;
+}
+
 // cap/solver.rs:118-125 (Method::Iterative)
 int orc_cap_dense_gmres(int64_t n, const double* verts, const int32_t* cond, int32_t ncond, double* C) {
     if (n <= 0) return -1;

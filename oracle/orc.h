@@ -74,6 +74,10 @@ int64_t orc_bridge_panelize(const int32_t* verts_x, const int32_t* verts_y,
 /* ---- solvers ---- C is ncond x ncond row-major, in farads (no eps scaling). */
 int orc_dense_P(int64_t n, const double* verts, double* P_out);
 int orc_cap_dense(int64_t n, const double* verts, const int32_t* cond, int32_t ncond, double* C_out);
+/* cap/dielectric.rs:76-150, conductor roles (bridge.rs:409-430): each panel's
+ * charge weighted by its surrounding permittivity eps[k]; C comes out k-scaled. */
+int orc_cap_dense_eps(int64_t n, const double* verts, const int32_t* cond, int32_t ncond, const double* eps,
+                      double* C_out);
 typedef struct {
     int32_t order, max_level, restart, max_restarts;
     double tol;

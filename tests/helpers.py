@@ -26,3 +26,41 @@ def rel_max(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def with_layer_k(lay, ks):
+    """The layout with its deck's dielectric constants set per metal layer
+    name (a stack of several k)."""
+    for name, k in ks.items():
+        lay.deck.pex[lay.deck.layers[name]].dielectric_k = k
+    return lay
+
+
+def rect_groups(store, deck, net_of_poly):
+    """bridge.rs:94-142 for layouts of rectangles: one (net, layer) group per
+    volume-conductor layer of a net (bridge.rs:171-178), z from the layer's
+    height and thickness, in BTreeMap<(net, layer)> order.  Returns (groups,
+    rects, xy_scale_m) for gpx_cap_solve_groups."""
+    a = store.arrays()
+    grouped = {}
+    for i, layer in enumerate(a["poly_layer"].tolist()):
+        p = deck.pex.get(layer)
+        if p is None:
+            continue
+        volume = (p.sheet_res_ohm_sq != 0.0 or p.area_cap_af_um2 != 0.0 or p.fringe_cap_af_um != 0.0
+                  or p.coupling_cap_af_um != 0.0 or p.interlayer_cap_af_um2 != 0.0
+                  or (p.thickness_nm > 0.0 and p.via_res_ohm == 0.0))
+        if not volume:
+            continue
+        s, n = int(a["poly_vert_start"][i]), int(a["poly_vert_len"][i])
+        xs, ys = a["verts_x"][s:s + n], a["verts_y"][s:s + n]
+        assert n == 4, "rectangles only"
+        key = (int(net_of_poly[i]), layer)
+        g = grouped.setdefault(key, {"z": (p.height_nm * 1e-9, (p.height_nm + p.thickness_nm) * 1e-9),
+                                     "k": p.dielectric_k, "rects": []})
+        g["rects"].append((int(xs.min()), int(ys.min()), int(xs.max()), int(ys.max())))
+    groups, rects = [], []
+    for (net, _), g in sorted(grouped.items()):
+        groups.append((net, g["z"][0], g["z"][1], g["k"], len(rects), len(g["rects"])))
+        rects.extend(g["rects"])
+    return groups, np.array(rects, dtype=np.int32).reshape(-1, 4), deck.dbu_nm * 1e-9
