@@ -29,7 +29,7 @@ EXPORTS = (
     "gpx_cap_solve_batched", "gpx_operator_apply", "gpx_potential_matrix", "gpx_cap_solve_groups",
     "gpx_extract_quasistatic", "gpx_bridge_panelize", "gpx_plan_check", "gpx_ctx_stream",
     "gpx_ctx_set_profiling", "gpx_ctx_kernel_stats", "gpx_ctx_reset_stats", "gpx_cap_solve_small_static",
-    "gpx_cap_sensitivity", "gpx_cap_sensitivity_rows", "gpx_autotune",
+    "gpx_cap_sensitivity", "gpx_cap_sensitivity_rows", "gpx_autotune", "gpx_cap_solve_eps",
 )
 KERNEL_CLASSES = ("near_assemble", "near_apply", "p2m", "m2m", "m2l", "l2l", "l2p", "gs_dot", "gs_axpy", "vec",
                   "small", "near_apply_f64", "p2m_f64", "m2m_f64", "m2l_f64", "l2l_f64", "l2p_f64")
@@ -134,6 +134,8 @@ def load(build_if_missing: bool = True):
         L.gpx_last_error.restype = C.c_char_p
         L.gpx_version.restype = C.c_char_p
         L.gpx_cap_solve.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), vp, C.POINTER(SolveReport)]
+        L.gpx_cap_solve_eps.argtypes = [vp, C.POINTER(PanelProblem), vp, C.POINTER(SolveOpts), vp,
+                                        C.POINTER(SolveReport)]
         L.gpx_cap_solve_batched.argtypes = [vp, vp, i32, C.POINTER(SolveOpts), vp, vp]
         L.gpx_operator_apply.argtypes = [vp, C.POINTER(PanelProblem), C.POINTER(SolveOpts), i32, vp, vp,
                                          C.POINTER(SolveReport)]
@@ -220,13 +222,23 @@ class Context:
         out["total_launches"] = total.value
         return out
 
-    def cap_solve(self, verts, cond, ncond, **kw):
+    def cap_solve(self, verts, cond, ncond, eps=None, **kw):
+        """gpx_cap_solve; with ``eps`` (one relative permittivity per panel)
+        gpx_cap_solve_eps, each panel's charge counted eps times."""
         v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)
         c = np.ascontiguousarray(cond, dtype=np.int32)
         pb = PanelProblem(len(v), v.ctypes.data, c.ctypes.data, ncond)
         Cm = np.zeros((ncond, ncond))
         rep = SolveReport()
-        self._check(self.L.gpx_cap_solve(self.h, C.byref(pb), C.byref(opts(**kw)), Cm.ctypes.data, C.byref(rep)))
+        if eps is None:
+            self._check(self.L.gpx_cap_solve(self.h, C.byref(pb), C.byref(opts(**kw)), Cm.ctypes.data,
+                                             C.byref(rep)))
+        else:
+            e = np.ascontiguousarray(eps, dtype=np.float64)
+            if e.shape != (len(v),):
+                raise ValueError("eps needs one value per panel")
+            self._check(self.L.gpx_cap_solve_eps(self.h, C.byref(pb), e.ctypes.data, C.byref(opts(**kw)),
+                                                 Cm.ctypes.data, C.byref(rep)))
         return Cm, rep.as_dict()
 
     def cap_solve_groups(self, groups, rects, xy_scale_m, **kw):

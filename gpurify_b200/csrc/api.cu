@@ -162,6 +162,17 @@ gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* pb, const gpx_so
     });
 }
 
+gpx_status gpx_cap_solve_eps(gpx_ctx* ctx, const gpx_panel_problem* pb, const double* eps, const gpx_solve_opts* opts,
+                             double* maxwell_out, gpx_solve_report* report) {
+    if (!ctx || !pb || !eps || !maxwell_out) return fail(ctx, GPX_ERR_INVALID_ARG, "null argument");
+    if (report) std::memset(report, 0, sizeof(*report));
+    CopyMeter meter(report);
+    return guarded(ctx, [&] {
+        Opts o = normalize(opts);
+        cap_solve(ctx->impl, pb->n_panels, pb->verts, pb->conductor, pb->n_conductors, o, maxwell_out, report, eps);
+    });
+}
+
 // Windows are independent: a work queue, largest estimated cost first, is
 // drained by batch_streams worker threads, each with its own stream (a
 // private context on the same device), so small and large windows overlap on

@@ -11,9 +11,11 @@
   (cap/listfile.rs:1-115): ``C <file> <outerperm> <xt> <yt> <zt> [+|-]`` adds
   the conductors of one ``.qui`` file, translated, as new conductors named
   ``<file>:<index>``.  The reference sends list files to its multi-dielectric
-  solver; this library solves conductors in one homogeneous medium only, so
-  every ``C`` line must give the same permittivity, which scales the Maxwell
-  matrix, and ``D`` (dielectric interface) lines are rejected.
+  solver (cap/dielectric.rs:76-150), where every ``C`` panel is a conductor
+  panel in its line's permittivity: one permittivity for all lines scales
+  the Maxwell matrix; several are kept per panel and each panel's charge
+  counts with its own (``gpx_cap_solve_eps``).  ``D`` (dielectric interface)
+  lines are rejected.
 * ``solve`` computes the Maxwell capacitance matrix in farads through
   ``gpx_cap_solve`` (cap::solve, cap/solver.rs:100-134): one right-hand side
   per conductor, no ground.  Below ``dense_below`` panels (default 500) the
@@ -42,12 +44,14 @@ class FastCapError(ValueError):
 class Geometry:
     """Panels of a FastCap deck: ``verts`` N x 12 (four corners, metres after
     scaling), ``cond`` N conductor indices, one name per conductor, and the
-    relative permittivity of the surrounding medium."""
+    relative permittivity of the surrounding medium: ``eps_r`` when it is one
+    for the whole deck, else ``panel_eps`` (N values, one per panel)."""
     verts: np.ndarray
     cond: np.ndarray
     conductor_names: List[str]
     eps_r: float = 1.0
     numbers: List[int] = field(default_factory=list)  # FastCap conductor number of each index
+    panel_eps: Optional[np.ndarray] = None
 
     def num_conductors(self) -> int:
         return len(self.conductor_names)
@@ -136,7 +140,7 @@ def parse_list_str(text: str, base_dir: str = ".") -> Geometry:
     blocks: List[np.ndarray] = []
     conds: List[np.ndarray] = []
     names: List[str] = []
-    eps: Optional[float] = None
+    block_eps: List[float] = []
     for n, raw in enumerate(text.splitlines(), start=1):
         line = raw.strip()
         if not line or line[0] in "*%":
@@ -153,11 +157,6 @@ def parse_list_str(text: str, base_dir: str = ".") -> Geometry:
         fname = tokens[1]
         outer = _list_number(tokens, 2, n, "outer permittivity")
         shift = np.array([_list_number(tokens, 3 + k, n, w) for k, w in enumerate(("xtrans", "ytrans", "ztrans"))])
-        if eps is None:
-            eps = outer
-        elif outer != eps:
-            raise FastCapError(f"line {n}: outer permittivity {outer:g} differs from {eps:g}; this library solves "
-                               "conductors in one homogeneous medium")
         path = os.path.join(base_dir, fname)
         try:
             with open(path) as f:
@@ -174,9 +173,13 @@ def parse_list_str(text: str, base_dir: str = ".") -> Geometry:
         v.reshape(-1, 4, 3)[:] += shift
         blocks.append(v)
         conds.append(sub.cond + first)
+        block_eps.append(outer)
     verts = np.concatenate(blocks) if blocks else np.zeros((0, 12))
     cond = np.concatenate(conds).astype(np.int32) if conds else np.zeros(0, dtype=np.int32)
-    return Geometry(verts, cond, names, 1.0 if eps is None else eps, list(range(len(names))))
+    if len(set(block_eps)) <= 1:
+        return Geometry(verts, cond, names, block_eps[0] if block_eps else 1.0, list(range(len(names))))
+    panel_eps = np.concatenate([np.full(len(b), e) for b, e in zip(blocks, block_eps)])
+    return Geometry(verts, cond, names, 1.0, list(range(len(names))), panel_eps)
 
 
 def parse_list_file(path: str) -> Geometry:
@@ -190,8 +193,9 @@ def parse_list_file(path: str) -> Geometry:
 
 
 def solve(geo: Geometry, ctx: Optional[_lib.Context] = None, **opts) -> Tuple[np.ndarray, dict]:
-    """Maxwell capacitance matrix (farads, scaled by the medium's permittivity)
-    and the solve report.  ``opts`` are ``gpx_solve_opts`` fields."""
+    """Maxwell capacitance matrix (farads, scaled by the media's
+    permittivities) and the solve report.  ``opts`` are ``gpx_solve_opts``
+    fields."""
     if len(geo.verts) == 0:
         raise FastCapError("no panels in the deck")
     if ctx is None:
@@ -199,5 +203,7 @@ def solve(geo: Geometry, ctx: Optional[_lib.Context] = None, **opts) -> Tuple[np
         ctx = default_context()
     kw = dict(skip_ground_rhs=0)
     kw.update(opts)
+    if geo.panel_eps is not None:
+        return ctx.cap_solve(geo.verts, geo.cond, geo.num_conductors(), eps=geo.panel_eps, **kw)
     C, rep = ctx.cap_solve(geo.verts, geo.cond, geo.num_conductors(), **kw)
     return C * geo.eps_r, rep

@@ -17,6 +17,9 @@
  *   gpx_cap_solve_groups     crates/pex/src/bridge.rs:307-443 `solve_capacitance`
  *   gpx_cap_solve            crates/pex/src/quasistatic/cap/fmm_solver.rs:147-172
  *                            `fmm_solver::solve` and cap/solver.rs:100-134 `solve`
+ *   gpx_cap_solve_eps        crates/pex/src/quasistatic/cap/dielectric.rs:76-150
+ *                            `solve` with conductor roles only (FastCap list files
+ *                            of C lines, cap/listfile.rs:56-77)
  *   gpx_cap_solve_batched    (no single reference function: many independent
  *                            windows; each window is one gpx_cap_solve)
  *   gpx_cap_sensitivity      (no reference counterpart: adjoint dC/dp beside the
@@ -168,6 +171,17 @@ typedef struct {
  * column is filled by symmetry from its row and C[last][last] is NaN. */
 gpx_status gpx_cap_solve(gpx_ctx* ctx, const gpx_panel_problem* problem, const gpx_solve_opts* opts,
                          double* maxwell_out, gpx_solve_report* report);
+
+/* Maxwell capacitance matrix of panels that each sit in their own medium:
+ * eps[k] (n_panels values, finite and > 0, caller panel order) is panel k's
+ * surrounding relative permittivity, and its charge counts eps[k] times,
+ * C[i][j] = sum_{k on i} eps[k] sigma_k a_k (cap/dielectric.rs:76-150 with
+ * every panel a PanelRole::Conductor; the potential system is the vacuum one).
+ * maxwell_out comes out k-scaled and is not symmetric: with
+ * opts.skip_ground_rhs the last column is NaN.  Dielectric-interface panels
+ * (PanelRole::Dielectric) are not supported. */
+gpx_status gpx_cap_solve_eps(gpx_ctx* ctx, const gpx_panel_problem* problem, const double* eps,
+                             const gpx_solve_opts* opts, double* maxwell_out, gpx_solve_report* report);
 
 /* Many independent problems in one call; maxwell_out[i] per problem. */
 gpx_status gpx_cap_solve_batched(gpx_ctx* ctx, const gpx_panel_problem* problems, int32_t n_problems,

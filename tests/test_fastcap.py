@@ -6,8 +6,9 @@ cap/listfile.rs:42-115): line kinds, conductor numbering and naming, scaling,
 translation, and the error messages with their line numbers.
 GPU: a parsed deck solved through gpx_cap_solve equals the oracle's dense
 LU solve (cap::solve, Method::Direct) of the same panels to 1e-9, for
-quadrilateral and triangular panels, and a list file's permittivity scales
-the matrix."""
+quadrilateral and triangular panels; a list file's permittivity scales the
+matrix, and a list of several permittivities (gpx_cap_solve_eps) equals the
+oracle's restatement of cap/dielectric.rs:76-150 with conductor roles."""
 import numpy as np
 import pytest
 
@@ -91,7 +92,6 @@ def test_list_file_translates_and_numbers_per_file(tmp_path):
 
 @pytest.mark.parametrize("lst,msg", [
     ("D a.qui 1 3.9 0 0 0 0 0 0\n", "line 1: dielectric interfaces"),
-    ("C a.qui 1 0 0 0\nC a.qui 3.9 0 0 0\n", "line 2: outer permittivity 3.9 differs from 1"),
     ("C\n", "line 1: C: missing file"),
     ("C a.qui 1 0 zero 0\n", "line 1: expected number for ytrans"),
     ("L a.qui\n", "line 1: unrecognized list line: L a.qui"),
@@ -105,6 +105,16 @@ def test_list_errors(tmp_path, lst, msg):
     with pytest.raises(fastcap.FastCapError) as e:
         fastcap.parse_list_str(lst, str(tmp_path))
     assert msg in str(e.value)
+
+
+def test_list_with_several_permittivities_keeps_them_per_panel(tmp_path):
+    (tmp_path / "a.qui").write_text(plate_qui(1, 0, 0, 0, 1, 1, 2, 1))
+    (tmp_path / "b.qui").write_text(plate_qui(1, 0, 0, 0, 1, 1, 1, 3))
+    g = fastcap.parse_list_str("C a.qui 3.9 0 0 0\nC b.qui 2.5 0 0 1\nC a.qui 3.9 0 0 2\n", str(tmp_path))
+    assert g.panel_eps.tolist() == [3.9, 3.9, 2.5, 2.5, 2.5, 3.9, 3.9]
+    assert len(g.panel_eps) == len(g.verts)
+    one = fastcap.parse_list_str("C a.qui 3.9 0 0 0\nC b.qui 3.9 0 0 1\n", str(tmp_path))
+    assert one.panel_eps is None and one.eps_r == 3.9
 
 
 @pytest.fixture(scope="module")
@@ -142,3 +152,21 @@ def test_list_permittivity_scales_the_matrix(ctx, tmp_path):
     # parallel plates 1 cm square, 0.5 mm apart: eps0 A / d plus a few percent of fringing
     eps0 = 8.8541878128e-12
     assert 1.0 < -C1[0, 1] / (eps0 * 1e-4 / 5e-4) < 1.3
+
+
+@pytest.mark.gpu
+def test_list_with_several_permittivities_matches_the_oracle(ctx, orc, tmp_path):
+    """cap/dielectric.rs:76-150 with conductor roles: each panel's charge
+    counts with its own line's permittivity; all pairs, against the oracle's
+    LU restatement to 1e-9."""
+    (tmp_path / "bot.qui").write_text(plate_qui(1, 0, 0, 0, 0.01, 0.01, 6, 6))
+    (tmp_path / "top.qui").write_text(plate_qui(1, 0, 0, 0, 0.01, 0.01, 5, 7))
+    g = fastcap.parse_list_str("C bot.qui 3.9 0 0 0\nC top.qui 2.2 0 0 0.0005\n", str(tmp_path))
+    C, rep = fastcap.solve(g, ctx)
+    assert rep["dense"] == 1 and rep["converged"] == 1
+    ref = orc.cap_dense_eps(g.verts, g.cond, 2, g.panel_eps)
+    assert rel_max(C, ref) < 1e-9
+    # one permittivity per conductor: row i is the vacuum row times conductor i's
+    C1, _ = fastcap.solve(fastcap.parse_list_str("C bot.qui 1 0 0 0\nC top.qui 1 0 0 0.0005\n", str(tmp_path)),
+                          ctx)
+    np.testing.assert_allclose(C, np.array([[3.9], [2.2]]) * C1, rtol=1e-12)
