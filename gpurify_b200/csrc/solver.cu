@@ -1482,6 +1482,11 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     constexpr int kMaxChunk = 128;
     const int Rc = std::min(Rn, kMaxChunk);
     const int R = (Rc + 3) & ~3;
+    if (panel_eps)
+        for (int64_t k = 0; k < n; ++k)
+            if (!std::isfinite(panel_eps[k]) || panel_eps[k] <= 0.0)
+                throw Error(GPX_ERR_INVALID_ARG, "panel permittivities must be finite and positive (panel " +
+                                                     std::to_string(k) + ")");
     Prepared pr;
     prepare(ctx, n, verts, cond, ncond, o, R, depth, pr);
     Operator& op = *pr.op;
@@ -1491,12 +1496,7 @@ void cap_solve(Ctx& ctx, int64_t n, const double* verts, const int32_t* cond, in
     DBuf<double> eps_area;
     if (panel_eps) {
         std::vector<double> w(n);
-        for (int64_t k = 0; k < n; ++k) {
-            const double e = panel_eps[pr.plan.perm[k]];
-            if (!std::isfinite(e) || e <= 0.0)
-                throw Error(GPX_ERR_INVALID_ARG, "panel permittivities must be finite and positive");
-            w[k] = pr.plan.area[k] * e;
-        }
+        for (int64_t k = 0; k < n; ++k) w[k] = pr.plan.area[k] * panel_eps[pr.plan.perm[k]];
         eps_area.upload(w, ctx.stream);
         d_weight = eps_area.p;
     }
