@@ -90,3 +90,15 @@ def test_groups_entry_matches_extract_and_leaves_skipped_column_nan(ctx):
     n = len(nets)
     assert np.all(np.isfinite(C[:, :n]))
     assert np.all(np.isnan(C[:, n]))
+
+
+def test_invalid_permittivity_is_refused_before_any_work(ctx, orc):
+    a, ca = orc.plate(0, 0, 0, 0.2, 0.2, 4, 4, 0)
+    b, cb = orc.plate(0, 0, 0.02, 0.2, 0.2, 4, 4, 1)
+    v, c = np.vstack([a, b]), np.concatenate([ca, cb])
+    for bad in (0.0, -1.0, float("nan"), float("inf")):
+        eps = np.full(len(v), 2.0)
+        eps[3] = bad
+        with pytest.raises(_lib.GpxError) as e:
+            ctx.cap_solve(v, c, 2, eps=eps)
+        assert e.value.status == 1 and "panel 3" in e.value.message
