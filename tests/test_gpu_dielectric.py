@@ -17,6 +17,8 @@ panels only (all pairs, LU); this solver at any size.
 * gpx_cap_solve_groups gives the per-net values of gpx_extract_quasistatic on
   the same groups; the matrix of several k is not symmetric, so a skipped
   substrate column comes back NaN instead of filled by symmetry.
+* gpx_cap_solve_eps refuses a permittivity that is not finite and positive,
+  naming the panel, before any set-up.
 """
 import numpy as np
 import pytest
