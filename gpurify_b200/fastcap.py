@@ -149,7 +149,7 @@ def parse_list_str(text: str, base_dir: str = ".") -> Geometry:
         kind = tokens[0]
         if kind in ("D", "d"):
             raise FastCapError(f"line {n}: dielectric interfaces (D lines) are not solved by this library; "
-                               "it takes conductors in one homogeneous medium")
+                               "it takes conductor panels (C lines), each in its own medium")
         if kind not in ("C", "c"):
             raise FastCapError(f"line {n}: unrecognized list line: {line}")
         if len(tokens) < 2:

@@ -170,7 +170,8 @@ def run_pex_sensitivity_checked(store: GeometryStore, deck: Deck, net_of_poly: S
             raise _lib.GpxError(15, "no panels in geometry")
         eps = p["eps"]
         if np.any(np.abs(eps - eps[0]) > 1e-12 * abs(eps[0])):
-            raise _lib.GpxError(15, "sensitivities need a homogeneous dielectric")
+            raise _lib.GpxError(15, "sensitivities need one dielectric constant for the whole stack "
+                                    "(a stack of several k is solved by run_pex_by_net_checked, not differentiated)")
         k = float(eps[0])
         ncond = len(p["nets"]) + 1
         V = sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], params)
