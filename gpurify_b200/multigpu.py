@@ -91,14 +91,19 @@ ColumnSolver = Callable[[int, int], np.ndarray]
 
 def solve_window_sharded(ncond: int, dist, skip_ground_rhs: bool = True,
                          column_solver: Optional[ColumnSolver] = None, ctx=None, verts=None, cond=None,
-                         **solve_kw) -> np.ndarray:
+                         symmetric: Optional[bool] = None, **solve_kw) -> np.ndarray:
     """Maxwell matrix of one window with its conductor columns spread over the
     ranks.  Each rank solves ``column_blocks(R, world)[rank]`` (R = nets, or
     every conductor without ``skip_ground_rhs``) with ``column_solver(begin,
     count)`` -> ncond x count, by default ``ctx.cap_solve`` with
     ``col_begin/col_count`` on this rank's GPU; the blocks are all-gathered
     and, with ``skip_ground_rhs``, the substrate column is filled by symmetry
-    (C[last][last] NaN), exactly as a single-rank ``gpx_cap_solve`` fills it."""
+    (C[last][last] NaN), exactly as a single-rank ``gpx_cap_solve`` fills it.
+    A matrix of panels in several media (``eps`` per panel in ``solve_kw``,
+    or ``symmetric=False``) is not symmetric: that column stays NaN, as
+    ``gpx_cap_solve_eps`` leaves it."""
+    if symmetric is None:
+        symmetric = solve_kw.get("eps") is None
     world, rank = dist.get_world_size(), dist.get_rank()
     R = ncond - 1 if (skip_ground_rhs and ncond > 1) else ncond
     blocks = column_blocks(R, world)
@@ -118,7 +123,7 @@ def solve_window_sharded(ncond: int, dist, skip_ground_rhs: bool = True,
         return cols
     C = np.empty((ncond, ncond))
     C[:, :R] = cols
-    C[:R, R] = cols[R, :R]
+    C[:R, R] = cols[R, :R] if symmetric else np.nan
     C[R, R] = np.nan
     return C
 

@@ -87,6 +87,11 @@ def _rank(rank, world, port, q):
 
         C = multigpu.solve_window_sharded(nc, dist, skip_ground_rhs=True, column_solver=column_solver)
         Cfull = multigpu.solve_window_sharded(nc, dist, skip_ground_rhs=False, column_solver=column_solver)
+        # panels in several media: the matrix is not symmetric, the skipped column stays NaN
+        eps = np.where(cond % 2 == 0, 3.9, 2.5)
+        Deps = oracle.cap_dense_eps(verts, cond, nc, eps)
+        Ceps = multigpu.solve_window_sharded(nc, dist, skip_ground_rhs=True, symmetric=False,
+                                             column_solver=lambda b, c: Deps[:, b : b + c])
         probs = [_small_problem(k) for k in (1, 3, 2, 5, 1)]
         costs = [len(v) * (n - 1) for v, _, n in probs]
 
@@ -95,7 +100,7 @@ def _rank(rank, world, port, q):
 
         W = multigpu.solve_windows_partitioned(costs, dist, window_solver)
         dist.barrier()
-        q.put((rank, calls, C, Cfull, D, W, [oracle.cap_dense(*p) for p in probs]))
+        q.put((rank, calls, C, Cfull, D, W, [oracle.cap_dense(*p) for p in probs], Ceps, Deps))
     finally:
         dist.destroy_process_group()
 
@@ -111,8 +116,10 @@ def test_two_ranks_shard_columns_and_windows():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, calls, C, Cfull, D, W, Wref in res:
+    for rank, calls, C, Cfull, D, W, Wref, Ceps, Deps in res:
         R = D.shape[0] - 1
+        np.testing.assert_array_equal(Ceps[:, :R], Deps[:, :R])
+        assert np.all(np.isnan(Ceps[:, R]))
         # rank r solved only its own block: nets split 3 + 2, all conductors 3 + 3
         assert calls == ([(0, 3), (0, 3)] if rank == 0 else [(3, 2), (3, 3)])
         np.testing.assert_array_equal(C[:, :R], D[:, :R])
