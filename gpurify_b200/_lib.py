@@ -399,5 +399,8 @@ def plan_check(verts, order, depth):
     s = L.gpx_plan_check(len(v), v.ctypes.data, order, depth, stats.ctypes.data)
     if s != GPX_OK:
         raise GpxError(s, L.gpx_last_error(None).decode())
-    keys = ("leaves", "boxes", "near_pairs", "m2l_box_pairs", "far_panel_pairs", "max_leaf", "max_near_row")
-    return dict(zip(keys, (int(x) for x in stats[:7])))
+    keys = ("leaves", "boxes", "near_pairs", "m2l_box_pairs", "far_panel_pairs", "max_leaf", "max_near_row",
+            "checksum")
+    out = dict(zip(keys, (int(x) for x in stats[:7])))
+    out["checksum"] = int(stats[7].view(np.uint64))
+    return out

@@ -488,6 +488,43 @@ gpx_status gpx_plan_check(int64_t n_panels, const double* verts, int32_t order, 
         stats[4] = covered_far;
         stats[5] = p.max_leaf;
         stats[6] = p.max_S;
+        // FNV-1a over every array the device kernels index, in a fixed order:
+        // a plan built another way must reproduce it bit for bit
+        uint64_t h = 1469598103934665603ull;
+        auto mix = [&h](const void* d, size_t bytes) {
+            const unsigned char* c = static_cast<const unsigned char*>(d);
+            for (size_t i = 0; i < bytes; ++i) h = (h ^ c[i]) * 1099511628211ull;
+        };
+        auto vec = [&mix](const auto& v) { mix(v.data(), v.size() * sizeof(v[0])); };
+        vec(p.perm);
+        vec(p.verts);
+        vec(p.cent);
+        vec(p.area);
+        vec(p.cond);
+        vec(p.w1d);
+        vec(p.lvl_off);
+        vec(p.box_cell);
+        vec(p.box_parent);
+        vec(p.box_octant);
+        vec(p.lvl_half);
+        vec(p.child_first);
+        vec(p.child_count);
+        vec(p.leaf_begin);
+        vec(p.leaf_of);
+        vec(p.near_off);
+        vec(p.near_src);
+        vec(p.near_S);
+        vec(p.nval_off);
+        vec(p.item_leaf);
+        vec(p.item_row0);
+        vec(p.m2l_off);
+        vec(p.m2l_src);
+        vec(p.m2l_slot);
+        vec(p.m2m1d);
+        mix(p.origin, sizeof(p.origin));
+        mix(&p.max_leaf, sizeof(p.max_leaf));
+        mix(&p.max_S, sizeof(p.max_S));
+        std::memcpy(&stats[7], &h, sizeof(h));
         if (near_pairs + covered_far != n_panels * n_panels) bad("pair coverage");
     });
 }

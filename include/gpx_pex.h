@@ -383,8 +383,10 @@ gpx_status gpx_ctx_reset_stats(gpx_ctx* ctx);
 /* Host-only self-check of the octree plan the solver would build for these
  * panels at (order, depth): index bounds, list disjointness and exact pair
  * coverage (every ordered panel pair is near or in exactly one M2L pair).
- * stats[0..6] = leaves, boxes, near pairs, M2L box pairs, far panel pairs,
- * largest leaf, largest near row.  Needs no device. */
+ * stats (8 entries): leaves, boxes, near pairs, M2L box pairs, far panel
+ * pairs, largest leaf, largest near row, and a 64-bit FNV-1a checksum of every
+ * plan array the device kernels index (sorted panels, weights, tree, near and
+ * M2L lists).  Needs no device. */
 gpx_status gpx_plan_check(int64_t n_panels, const double* verts, int32_t order, int32_t depth, int64_t* stats);
 
 #ifdef __cplusplus

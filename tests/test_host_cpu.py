@@ -209,3 +209,23 @@ def test_sensitivity_velocity_fields():
     assert np.all(V[4] == 0)
     with pytest.raises(ValueError):
         sensitivity.velocity_fields(p["verts"], p["cond"], p["nets"], [("length", 0)])
+
+
+def test_plan_matches_pinned_checksums():
+    """The plan builder reproduces, bit for bit, every plan array of the
+    pinned problems (tests/golden/plan_checksums.json, made by
+    tests/golden/make_plan_checksums.py), so the device kernels index the same
+    plan however the host builds it."""
+    import json
+    import os
+
+    from tests.golden.make_plan_checksums import cases
+
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "plan_checksums.json")))["cases"]
+    seen = set()
+    for name, verts, order, depth in cases():
+        st = _lib.plan_check(verts, order, depth)
+        st["n_panels"] = len(verts)
+        assert st == gold[name], name
+        seen.add(name)
+    assert seen == set(gold)
