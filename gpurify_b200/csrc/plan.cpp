@@ -142,6 +142,70 @@ std::vector<double> cheb_roots(int n) {
     return v;
 }
 
+namespace {
+
+// T_k(x_m) of the n roots, k = 0..n-1 (row m), by the recurrence
+// cheb_weights runs: the same values, computed once per plan.
+std::vector<double> cheb_root_table(int n, const double* roots) {
+    std::vector<double> t((size_t)n * n);
+    for (int m = 0; m < n; ++m) {
+        const double xm = roots[m];
+        double prev = 1.0, cur = xm;
+        t[(size_t)m * n] = 1.0;
+        for (int k = 1; k < n; ++k) {
+            double tk;
+            if (k == 1) {
+                tk = xm;
+            } else {
+                tk = 2.0 * xm * cur - prev;
+                prev = cur;
+                cur = tk;
+            }
+            t[(size_t)m * n + k] = tk;
+        }
+    }
+    return t;
+}
+
+// cheb_weights with the roots' T_k from cheb_root_table: identical sums in
+// the identical order.
+inline void cheb_weights_tab(double x, int n, const double* tab, double* out) {
+    double tx[32];
+    tx[0] = 1.0;
+    if (n > 1) {
+        tx[1] = x;
+        for (int k = 2; k < n; ++k) tx[k] = 2.0 * x * tx[k - 1] - tx[k - 2];
+    }
+    const double inv_n = 1.0 / n;
+    for (int m = 0; m < n; ++m) {
+        const double* tm = tab + (size_t)m * n;
+        double sum = 0.5;
+        for (int k = 1; k < n; ++k) sum += tm[k] * tx[k];
+        out[m] = 2.0 * inv_n * sum;
+    }
+}
+
+// fn(chunk, begin, end) over [0, n) in contiguous chunks of at least
+// min_chunk items, on up to 16 threads (the caller's among them).  Returns
+// the number of chunks.  Chunks are independent; fn must not throw.
+template <class F>
+int parallel_chunks(int64_t n, int64_t min_chunk, F&& fn) {
+    const int64_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(hw, n / std::max<int64_t>(1, min_chunk)));
+    const int64_t per = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    for (int t = 1; t < nt; ++t) {
+        const int64_t b = std::min(n, t * per), e = std::min(n, b + per);
+        th.emplace_back([&fn, t, b, e] { fn(t, b, e); });
+    }
+    fn(0, 0, std::min(n, per));
+    for (auto& x : th) x.join();
+    return nt;
+}
+
+}  // namespace
+
 // S_n(x, x_m) = 1/n + 2/n sum_{k=1}^{n-1} T_k(x_m) T_k(x), by recurrence.
 void cheb_weights(double x, int n, const double* roots, double* out) {
     double tx[32];
@@ -360,13 +424,33 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
     thread_local std::vector<double> c0, a0;
     c0.resize((size_t)N * 3);
     a0.resize((size_t)N);
-    for (int64_t i = 0; i < N; ++i) panel_centroid_area(verts + 12 * i, &c0[3 * i], &a0[i]);
-    // cubic bounding box (fmm/tree.rs:43-62)
-    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (int64_t i = 0; i < N; ++i)
+    // the helper threads see this thread's scratch through plain pointers (a
+    // thread_local named inside them would be their own, empty, instance)
+    double* const cen = c0.data();
+    double* const are = a0.data();
+    // cubic bounding box (fmm/tree.rs:43-62), per chunk then combined (the
+    // extremes of finite values do not depend on the order)
+    constexpr int64_t kChunk = 8192;
+    double clo[16][3], chi[16][3];
+    const int nch = parallel_chunks(N, kChunk, [&](int t, int64_t b, int64_t e) {
+        double l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int64_t i = b; i < e; ++i) {
+            panel_centroid_area(verts + 12 * i, &cen[3 * i], &are[i]);
+            for (int d = 0; d < 3; ++d) {
+                l[d] = std::fmin(l[d], cen[3 * i + d]);
+                h[d] = std::fmax(h[d], cen[3 * i + d]);
+            }
+        }
         for (int d = 0; d < 3; ++d) {
-            lo[d] = std::fmin(lo[d], c0[3 * i + d]);
-            hi[d] = std::fmax(hi[d], c0[3 * i + d]);
+            clo[t][d] = l[d];
+            chi[t][d] = h[d];
+        }
+    });
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int t = 0; t < nch; ++t)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::fmin(lo[d], clo[t][d]);
+            hi[d] = std::fmax(hi[d], chi[t][d]);
         }
     double half = 0.0, center[3];
     for (int d = 0; d < 3; ++d) {
@@ -384,28 +468,45 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
     thread_local std::vector<uint64_t> key;
     cell.resize((size_t)N * 3);
     key.resize((size_t)N);
-    for (int64_t i = 0; i < N; ++i) {
-        for (int d = 0; d < 3; ++d) {
-            long long idx = (long long)std::floor((c0[3 * i + d] - origin[d]) / leaf_size);
-            idx = std::max(0ll, std::min((long long)ncell - 1, idx));
-            cell[3 * i + d] = (uint32_t)idx;
+    uint32_t* const cel = cell.data();
+    uint64_t* const kys = key.data();
+    parallel_chunks(N, kChunk, [&](int, int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            for (int d = 0; d < 3; ++d) {
+                long long idx = (long long)std::floor((cen[3 * i + d] - origin[d]) / leaf_size);
+                idx = std::max(0ll, std::min((long long)ncell - 1, idx));
+                cel[3 * i + d] = (uint32_t)idx;
+            }
+            kys[i] = morton(cel[3 * i], cel[3 * i + 1], cel[3 * i + 2]);
         }
-        key[i] = morton(cell[3 * i], cell[3 * i + 1], cell[3 * i + 2]);
-    }
+    });
+    // leaf order: stable by key.  Up to depth 12 the key takes 36 bits, so
+    // (key << 28 | caller index) sorts plainly into the same order (a merge
+    // sort: bridge panels arrive in long runs of rising keys).
     p.perm.resize(N);
-    std::iota(p.perm.begin(), p.perm.end(), 0);
-    std::stable_sort(p.perm.begin(), p.perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    if (depth <= 12 && N < (int64_t(1) << 28)) {
+        thread_local std::vector<uint64_t> packed;
+        packed.resize((size_t)N);
+        for (int64_t i = 0; i < N; ++i) packed[i] = key[i] << 28 | (uint64_t)i;
+        std::stable_sort(packed.begin(), packed.end());
+        for (int64_t s = 0; s < N; ++s) p.perm[s] = (int32_t)(packed[s] & ((uint64_t(1) << 28) - 1));
+    } else {
+        std::iota(p.perm.begin(), p.perm.end(), 0);
+        std::stable_sort(p.perm.begin(), p.perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    }
     p.verts.resize((size_t)N * 12);
     p.cent.resize((size_t)N * 3);
     p.area.resize(N);
     p.cond.resize(N);
-    for (int64_t s = 0; s < N; ++s) {
-        int64_t i = p.perm[s];
-        std::copy(verts + 12 * i, verts + 12 * i + 12, &p.verts[12 * s]);
-        std::copy(&c0[3 * i], &c0[3 * i] + 3, &p.cent[3 * s]);
-        p.area[s] = a0[i];
-        p.cond[s] = cond ? cond[i] : 0;
-    }
+    parallel_chunks(N, kChunk, [&](int, int64_t b, int64_t e) {
+        for (int64_t s = b; s < e; ++s) {
+            int64_t i = p.perm[s];
+            std::copy(verts + 12 * i, verts + 12 * i + 12, &p.verts[12 * s]);
+            std::copy(&cen[3 * i], &cen[3 * i] + 3, &p.cent[3 * s]);
+            p.area[s] = are[i];
+            p.cond[s] = cond ? cond[i] : 0;
+        }
+    });
     // levels: leaf boxes in Morton order, then parents
     std::vector<std::vector<std::array<uint32_t, 3>>> cells(depth + 1);
     p.leaf_begin.clear();
@@ -458,16 +559,18 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
         for (int64_t s = p.leaf_begin[k]; s < p.leaf_begin[k + 1]; ++s) p.leaf_of[s] = (int32_t)k;
     // 1-D Chebyshev weights of each panel in its leaf (bbfmm.rs:53-59).
     std::vector<double> roots = cheb_roots(order);
+    const std::vector<double> troots = cheb_root_table(order, roots.data());
     p.w1d.resize((size_t)N * 3 * order);
     const double hl = p.lvl_half[depth];
-    for (int64_t k = 0; k + 1 < (int64_t)p.leaf_begin.size(); ++k) {
-        int32_t b = p.lvl_off[depth] + (int32_t)k;
-        double ctr[3];
-        for (int d = 0; d < 3; ++d) ctr[d] = origin[d] + ((double)p.box_cell[3 * b + d] + 0.5) * 2.0 * hl;
-        for (int64_t s = p.leaf_begin[k]; s < p.leaf_begin[k + 1]; ++s)
-            for (int d = 0; d < 3; ++d)
-                cheb_weights((p.cent[3 * s + d] - ctr[d]) / hl, order, roots.data(), &p.w1d[(s * 3 + d) * order]);
-    }
+    parallel_chunks(N, kChunk, [&](int, int64_t b, int64_t e) {
+        for (int64_t s = b; s < e; ++s) {
+            const int32_t bx = p.lvl_off[depth] + p.leaf_of[s];
+            for (int d = 0; d < 3; ++d) {
+                const double ctr = origin[d] + ((double)p.box_cell[3 * bx + d] + 0.5) * 2.0 * hl;
+                cheb_weights_tab((p.cent[3 * s + d] - ctr) / hl, order, troots.data(), &p.w1d[(s * 3 + d) * order]);
+            }
+        }
+    });
     // near blocks: self leaf first, then neighbours in dx,dy,dz order
     const int64_t nl = p.nleaf();
     p.near_off.assign(nl + 1, 0);
@@ -507,35 +610,53 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
         }
     // interaction lists (fmm/tree.rs:188-209): children of the parent's
     // neighbourhood that are not neighbours of the box.
+    // Boxes of level >= 2 are visited parent by parent: the parent's
+    // existing neighbours are looked up once, and each neighbour's children
+    // are taken by octant from its contiguous child range.
     p.m2l_off.assign(nb + 1, 0);
     p.m2l_src.clear();
     p.m2l_slot.clear();
-    for (int64_t b = 0; b < nb; ++b) {
-        int l = 0;
-        while (b >= p.lvl_off[l + 1]) ++l;
-        if (l >= 2) {
-            const int32_t* c = &p.box_cell[3 * b];
-            int64_t pc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
-            const int64_t npc = 1ll << (l - 1);
+    const int64_t first2 = depth >= 2 ? p.lvl_off[2] : nb;
+    for (int64_t b = 0; b < first2; ++b) p.m2l_off[b + 1] = 0;
+    int64_t next = first2;
+    for (int l = 2; l <= depth; ++l) {
+        const int64_t npc = 1ll << (l - 1);
+        for (int32_t pb = p.lvl_off[l - 1]; pb < p.lvl_off[l]; ++pb) {
+            const int32_t* pcell = &p.box_cell[3 * pb];
+            int32_t nbr_child[27][8];
+            int nn = 0;
             for (int dx = -1; dx <= 1; ++dx)
                 for (int dy = -1; dy <= 1; ++dy)
                     for (int dz = -1; dz <= 1; ++dz) {
-                        int64_t q[3] = {pc[0] + dx, pc[1] + dy, pc[2] + dz};
+                        int64_t q[3] = {pcell[0] + dx, pcell[1] + dy, pcell[2] + dz};
                         if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= npc || q[1] >= npc || q[2] >= npc) continue;
-                        if (!idx[l - 1].count(cell_key(q[0], q[1], q[2]))) continue;
-                        for (int o = 0; o < 8; ++o) {
-                            int64_t ch[3] = {2 * q[0] + (o & 1), 2 * q[1] + ((o >> 1) & 1), 2 * q[2] + ((o >> 2) & 1)};
-                            auto it = idx[l].find(cell_key(ch[0], ch[1], ch[2]));
-                            if (it == idx[l].end()) continue;
-                            int64_t ox = ch[0] - c[0], oy = ch[1] - c[1], oz = ch[2] - c[2];
-                            if (std::max(std::llabs(ox), std::max(std::llabs(oy), std::llabs(oz))) <= 1) continue;
-                            p.m2l_src.push_back(it->second);
-                            p.m2l_slot.push_back((int32_t)(((ox + 3) * 7 + oy + 3) * 7 + oz + 3));
-                        }
+                        auto it = idx[l - 1].find(cell_key(q[0], q[1], q[2]));
+                        if (it == idx[l - 1].end()) continue;
+                        int32_t* slot = nbr_child[nn++];
+                        for (int o = 0; o < 8; ++o) slot[o] = -1;
+                        const int32_t qb = it->second;
+                        for (int32_t ch = p.child_first[qb]; ch < p.child_first[qb] + p.child_count[qb]; ++ch)
+                            slot[p.box_octant[ch]] = ch;
                     }
+            for (int32_t b = p.child_first[pb]; b < p.child_first[pb] + p.child_count[pb]; ++b) {
+                if (b != next) throw Error(GPX_ERR_INTERNAL, "octree children out of order");
+                const int32_t* c = &p.box_cell[3 * b];
+                for (int k = 0; k < nn; ++k)
+                    for (int o = 0; o < 8; ++o) {
+                        const int32_t src = nbr_child[k][o];
+                        if (src < 0) continue;
+                        const int32_t* ch = &p.box_cell[3 * src];
+                        int64_t ox = ch[0] - c[0], oy = ch[1] - c[1], oz = ch[2] - c[2];
+                        if (std::max(std::llabs(ox), std::max(std::llabs(oy), std::llabs(oz))) <= 1) continue;
+                        p.m2l_src.push_back(src);
+                        p.m2l_slot.push_back((int32_t)(((ox + 3) * 7 + oy + 3) * 7 + oz + 3));
+                    }
+                p.m2l_off[b + 1] = (int64_t)p.m2l_src.size();
+                ++next;
+            }
         }
-        p.m2l_off[b + 1] = (int64_t)p.m2l_src.size();
     }
+    if (next != nb) throw Error(GPX_ERR_INTERNAL, "octree boxes without a parent");
     // tensor-product M2M operators (bbfmm.rs:89-112)
     p.m2m1d.assign((size_t)24 * order * order, 0.0);
     std::vector<double> w(order);
