@@ -317,7 +317,7 @@ gpx_status gpx_cap_solve_groups(gpx_ctx* ctx, const gpx_volume_group* groups, in
         *n_nets = 0;
         if (n_groups == 0) return;
         auto gs = groups_from_abi(groups, n_groups, rects);
-        PanelizeResult pr;
+        thread_local PanelizeResult pr;  // buffers kept between calls of this thread
         const double t0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
         panelize_groups(gs, xy_scale_m, o.mesh_max_edge, o.max_panels, pr);
         const double t1 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -353,7 +353,7 @@ gpx_status gpx_extract_quasistatic(gpx_ctx* ctx, const gpx_geometry_store* store
             // substrate right-hand side is skipped unless asked for.
             if (!opts) o.skip_ground_rhs = 1;
             *n_out = 0;
-            PanelizeResult pr;
+            thread_local PanelizeResult pr;  // buffers kept between calls of this thread
             const double t0 =
                 std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
             panelize_store(*store, *deck, net_of_poly, n_nop, o.mesh_max_edge, o.max_panels, pr);
@@ -390,7 +390,7 @@ gpx_status gpx_bridge_panelize(gpx_ctx* ctx, const gpx_geometry_store* store, co
         nullptr,
         [&] {
             Opts o = normalize(opts);
-            PanelizeResult pr;
+            thread_local PanelizeResult pr;  // buffers kept between calls of this thread
             panelize_store(*store, *deck, net_of_poly, n_nop, o.mesh_max_edge, o.max_panels, pr);
             *n_panels = pr.panels.size();
             *n_nets = (int64_t)pr.nets.size();

@@ -209,8 +209,14 @@ void decompose_ring(const int32_t* xs, const int32_t* ys, size_t n, uint32_t pol
 void panelize_groups(const std::vector<VolumeGroup>& groups, double xy, double me, int64_t max_panels_opt,
                      PanelizeResult& res) {
     const int64_t max_panels = max_panels_opt == 0 ? kRefMaxPanels : (max_panels_opt < 0 ? INT64_MAX : max_panels_opt);
-    res.panels = PanelBuffer();
+    // cleared, not released: a result kept by the caller between calls keeps
+    // its capacity (no fresh pages, no regrowth)
+    res.panels.verts.clear();
+    res.panels.cond.clear();
+    res.panels.eps.clear();
     res.nets.clear();
+    res.homogeneous = true;
+    res.first_eps = 1.0;
     if (groups.empty()) return;
     std::set<uint32_t> netset;
     for (const auto& g : groups) netset.insert(g.net);

@@ -343,6 +343,9 @@ typedef struct { /* analytical/mod.rs:354-357 NetParasitics */
 } gpx_net_parasitics;
 
 /* Replaces bridge.rs:73-147 `extract_quasistatic` for C (and fixed via R).
+ * This call, gpx_cap_solve_groups and gpx_bridge_panelize keep their panel
+ * buffers per calling thread between calls (capacity of the largest layout
+ * panelised so far), so repeated calls make no fresh host allocations.
  * On GPX_ERR_UNSUPPORTED_GEOMETRY *err_polygon is the polygon index (else
  * UINT32_MAX), as lib.rs:111-123 maps it into the diagnostic. */
 gpx_status gpx_extract_quasistatic(gpx_ctx* ctx, const gpx_geometry_store* store, const gpx_deck* deck,
