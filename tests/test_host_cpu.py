@@ -229,3 +229,25 @@ def test_plan_matches_pinned_checksums():
         assert st == gold[name], name
         seen.add(name)
     assert seen == set(gold)
+
+
+def test_concurrent_host_calls_match_serial():
+    """Panelisation keeps its buffers per calling thread and the plan builder
+    spreads its panel loops over helper threads: calls from several threads
+    at once (ctypes releases the GIL) give exactly the serial results."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    # 18k to 40k panels: the plan builder's panel loops run on 2 to 4 helper threads
+    lays = [layouts.routing_window(24, 25.0, seed=s) for s in (4, 5)] + [layouts.routing_window(40, 32.0, seed=6),
+                                                                      layouts.bus_crossing(), layouts.two_wires()]
+
+    def one(lay):
+        p = _lib.bridge_panelize(lay.store.arrays(), lay.deck.layer_table(), 1.0, lay.net_of_poly,
+                                 mesh_max_edge_m=0.3e-6, max_panels=-1)
+        return p["verts"], p["cond"], _lib.plan_check(p["verts"], 5, 4)["checksum"]
+
+    serial = [one(lay) for lay in lays]
+    with ThreadPoolExecutor(4) as ex:
+        for _ in range(3):
+            for (v, c, h), (v0, c0, h0) in zip(ex.map(one, lays), serial):
+                assert np.array_equal(v, v0) and np.array_equal(c, c0) and h == h0
