@@ -2,7 +2,9 @@
 pairs, the plan statistics and the 64-bit checksum of every plan array
 (gpx_plan_check) as the builder produced them when this file was written.
 A faster builder must reproduce each checksum bit for bit, so the device
-kernels see the same plan.
+kernels see the same plan.  The cases from ``one_panel_o5_d4`` on were added
+with the threaded builder, after its plan arrays had been compared equal to
+those of the serial builder on the same inputs.
 
     python tests/golden/make_plan_checksums.py   # rewrites plan_checksums.json
 """
@@ -52,6 +54,15 @@ def cases():
     yield "bus_crossing_o6_d4", bridge(layouts.bus_crossing()), 6, 4
     yield "random_o5_d7", random_panels(20000, 11), 5, 7
     yield "random_o2_d3", random_panels(3000, 12), 2, 3
+    # sizes around the plan builder's 8192-panel chunks, one panel, depth 12,
+    # and panels that all share one centroid (a zero-size bounding box)
+    yield "one_panel_o5_d4", random_panels(1, 21), 5, 4
+    yield "random8193_o6_d7", random_panels(8193, 25), 6, 7
+    yield "random16385_o3_d12", random_panels(16385, 26), 3, 12
+    yield "random40000_o5_d4", random_panels(40000, 27), 5, 4
+    same = random_panels(500, 28).reshape(-1, 4, 3)
+    same[:] = same[0]
+    yield "one_centroid_o5_d4", same.reshape(-1, 12), 5, 4
 
 
 def generate():
