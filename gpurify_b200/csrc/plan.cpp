@@ -185,12 +185,14 @@ inline void cheb_weights_tab(double x, int n, const double* tab, double* out) {
     }
 }
 
+constexpr unsigned kMaxChunks = 16;  // threads of one parallel_chunks call, the caller's included
+
 // fn(chunk, begin, end) over [0, n) in contiguous chunks of at least
-// min_chunk items, on up to 16 threads (the caller's among them).  Returns
-// the number of chunks.  Chunks are independent; fn must not throw.
+// min_chunk items, on up to kMaxChunks threads (the caller's among them).
+// Returns the number of chunks.  Chunks are independent; fn must not throw.
 template <class F>
 int parallel_chunks(int64_t n, int64_t min_chunk, F&& fn) {
-    const int64_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const int64_t hw = std::max(1u, std::min(kMaxChunks, std::thread::hardware_concurrency()));
     const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(hw, n / std::max<int64_t>(1, min_chunk)));
     const int64_t per = (n + nt - 1) / nt;
     std::vector<std::thread> th;
@@ -431,7 +433,7 @@ void build_plan(Plan& p, int64_t N, const double* verts, const int32_t* cond, in
     // cubic bounding box (fmm/tree.rs:43-62), per chunk then combined (the
     // extremes of finite values do not depend on the order)
     constexpr int64_t kChunk = 8192;
-    double clo[16][3], chi[16][3];
+    double clo[kMaxChunks][3], chi[kMaxChunks][3];
     const int nch = parallel_chunks(N, kChunk, [&](int t, int64_t b, int64_t e) {
         double l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int64_t i = b; i < e; ++i) {
